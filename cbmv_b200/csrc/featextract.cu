@@ -1,0 +1,462 @@
+// Feature extraction: the reference's layout helpers and confidence
+// measures (cpp/featextract/featextract.cpp) and the fused 20-feature kernel
+// that replaces Testing.__extract_features_lr (test.py:521-595).
+//
+// Every confidence is computed in float64 with the reference's operation
+// order, so the features equal the reference's float64 values (and so their
+// float32 roundings, which is what the random forest compares).  The one
+// freedom taken is the order of the likelihood denominator's sum over d,
+// which only moves it by an ulp of float64.
+#include "common.cuh"
+#include "rf.cuh"
+
+namespace cbmv {
+namespace {
+
+constexpr int kBlock = 256;
+
+#define GRID_STRIDE(i, n) \
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+__global__ void swap_axes_kernel(const double* __restrict__ in, int64_t D, int64_t HW,
+                                 double* __restrict__ out) {
+  GRID_STRIDE(t, D * HW) {
+    const int64_t p = t / D, d = t - p * D;
+    out[t] = in[d * HW + p];
+  }
+}
+
+__global__ void swap_axes_back_kernel(const double* __restrict__ in, int64_t HW, int64_t D,
+                                      double* __restrict__ out) {
+  GRID_STRIDE(t, D * HW) {
+    const int64_t d = t / HW, p = t - d * HW;
+    out[t] = in[p * D + d];
+  }
+}
+
+__global__ void get_cost_kernel(const double* __restrict__ in, int64_t n, int64_t K,
+                                double* __restrict__ out) {
+  GRID_STRIDE(t, n) out[t] = in[t * K];
+}
+
+// dir = +1: R[i,j,d] = C[i,j+d,d] for j < W-d (featextract.cpp:136-145)
+// dir = -1: L[i,j,d] = R[i,j-d,d] for j >= d (featextract.cpp:473-481)
+// otherwise the volume's first element (:130, :467).
+__global__ void shift_kernel(const double* __restrict__ in, int64_t H, int64_t W, int64_t D,
+                             int dir, double* __restrict__ out) {
+  const double fill = in[0];
+  GRID_STRIDE(t, H * W * D) {
+    const int64_t d = t % D;
+    const int64_t p = t / D;
+    const int64_t j = p % W;
+    const int64_t js = j + dir * d;
+    out[t] = (js >= 0 && js < W) ? in[(p + dir * d) * D + d] : fill;
+  }
+}
+
+// Row minimum as featextract.cpp:322-329 (start at RAND_MAX, strict <),
+// one warp per row.
+__device__ __forceinline__ double warp_row_min(const double* r, int64_t D) {
+  double m = kRandMax;
+  for (int64_t k = threadIdx.x & 31; k < D; k += 32) m = fmin(m, r[k]);
+  for (int o = 16; o; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+  return m;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double lik_term(double c, double m, double sigma) {
+  const double num = c - m;
+  return exp(-(num * num) / sigma);  // featextract.cpp:433-434
+}
+
+__global__ void ratio_kernel(const double* __restrict__ v, int64_t N, int64_t D, double e,
+                             double* __restrict__ out) {
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; i < N; i += warps) {
+    const double* r = v + i * D;
+    const double m = warp_row_min(r, D);
+    for (int64_t k = threadIdx.x & 31; k < D; k += 32)
+      out[i * D + k] = (m == kRandMax) ? 0.0 : (m + e) / (r[k] + e);
+  }
+}
+
+__global__ void likelihood_kernel(const double* __restrict__ v, int64_t N, int64_t D, double sigma,
+                                  double* __restrict__ out) {
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; i < N; i += warps) {
+    const double* r = v + i * D;
+    const double m = warp_row_min(r, D);
+    double den = 0.0;
+    for (int64_t k = threadIdx.x & 31; k < D; k += 32) den += lik_term(r[k], m, sigma);
+    den = warp_sum(den);
+    for (int64_t k = threadIdx.x & 31; k < D; k += 32) {
+      const double t = r[k] - m;
+      out[i * D + k] = (m == kRandMax) ? 0.0 : exp(-((t * t) / sigma)) / den;
+    }
+  }
+}
+
+__global__ void ratio_samples_kernel(const double* __restrict__ v, int64_t N, int64_t D,
+                                     const int32_t* __restrict__ s, double e,
+                                     double* __restrict__ out) {
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; i < N; i += warps) {
+    const double* r = v + i * D;
+    const double m = warp_row_min(r, D);
+    const int k = threadIdx.x & 31;
+    if (k < 3) out[3 * i + k] = (m == kRandMax) ? 0.0 : (m + e) / (r[s[3 * i + k]] + e);
+  }
+}
+
+__global__ void likelihood_samples_kernel(const double* __restrict__ v, int64_t N, int64_t D,
+                                          const int32_t* __restrict__ s, double sigma,
+                                          double* __restrict__ out) {
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; i < N; i += warps) {
+    const double* r = v + i * D;
+    const double m = warp_row_min(r, D);
+    double den = 0.0;
+    for (int64_t k = threadIdx.x & 31; k < D; k += 32) den += lik_term(r[k], m, sigma);
+    den = warp_sum(den);
+    const int k = threadIdx.x & 31;
+    if (k < 3) {
+      const double t = r[s[3 * i + k]] - m;
+      out[3 * i + k] = (m == kRandMax) ? 0.0 : exp(-((t * t) / sigma)) / den;
+    }
+  }
+}
+
+__global__ void get_samples_kernel(const double* __restrict__ v, int64_t N, int64_t D,
+                                   const int32_t* __restrict__ s, double* __restrict__ out) {
+  GRID_STRIDE(t, 3 * N) out[t] = v[(t / 3) * D + s[t]];
+}
+
+__global__ void labels_kernel(int64_t N, int32_t* __restrict__ out) {
+  GRID_STRIDE(t, 3 * N) out[t] = (t % 3) == 0 ? 1 : 0;
+}
+
+__device__ __forceinline__ uint32_t draw(uint64_t seed, int64_t s, int slot, uint32_t n) {
+  uint64_t z = seed * 0x9E3779B97F4A7C15ull + (uint64_t)s * 3ull + (uint64_t)slot + 1;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return (uint32_t)(z % n);
+}
+
+__global__ void d_indices_kernel(const int32_t* __restrict__ gt, int64_t N, int maxd, int thr,
+                                 uint64_t seed, int32_t* __restrict__ out, int* __restrict__ bad) {
+  GRID_STRIDE(s, N) {
+    const int g = gt[s];
+    const bool low = !(g - thr <= 0), high = !(g + thr >= maxd);
+    const int lo_n = g - thr, hi_n = maxd - (g + thr + 1);
+    int d1 = 0, d2 = 0;
+    bool ok = g >= 0 && g <= maxd;
+    if (low) d1 = (int)draw(seed, s, 0, (uint32_t)lo_n);
+    else if (hi_n > 0) d1 = (int)draw(seed, s, 0, (uint32_t)hi_n) + (g + thr + 1);
+    else ok = false;
+    if (high && hi_n > 0) d2 = (int)draw(seed, s, 1, (uint32_t)hi_n) + (g + thr + 1);
+    else if (!high && lo_n > 0) d2 = (int)draw(seed, s, 1, (uint32_t)lo_n);
+    else ok = false;
+    out[3 * s] = g;
+    out[3 * s + 1] = d1;
+    out[3 * s + 2] = d2;
+    if (!ok) atomicExch(bad, 1);
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------ fused features
+// Per-matcher constants of the reference's feature extraction:
+// ratio epsilon (test.py:548-551) and likelihood sigma (test.py:71-73).
+__constant__ double kEps[4] = {0.01, 1.01, 0.01, 0.01};
+__constant__ double kSigma[4] = {2.0 * 8 * 8, 0.02, 2.0 * 100 * 100, 2.0 * 100 * 100};
+static const double hSigma[4] = {2.0 * 8 * 8, 0.02, 2.0 * 100 * 100, 2.0 * 100 * 100};
+
+// Per-pixel statistics of one matcher volume for both reference views:
+// stats[((m*2 + view)*HW + p)*2 + {0,1}] = {row minimum, likelihood
+// denominator}; view 0 = left reference (row p of the volume), view 1 =
+// right reference (right pixel p: entries C[p + d, d], RAND_MAX when
+// x + d >= W, featextract.cpp:115-152).  One warp per (pixel, view).
+__global__ void feature_stats_kernel(const double* __restrict__ vol, int m, int64_t H, int64_t W,
+                                     int D, double sigma, double* __restrict__ stats) {
+  const int64_t HW = H * W;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x / 32);
+  const int lane = threadIdx.x & 31;
+  for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; t < 2 * HW; t += nwarps) {
+    const int view = (int)(t / HW);
+    const int64_t p = t - view * HW;
+    const int64_t x = p % W;
+    const double fill = vol[0];  // get_right_cost's fill, featextract.cpp:130
+    double mn = kRandMax;
+    if (view == 0) {
+      const double* r = vol + p * D;
+      for (int d = lane; d < D; d += 32) mn = fmin(mn, r[d]);
+    } else {
+      for (int d = lane; d < D; d += 32) mn = fmin(mn, x + d < W ? vol[(p + d) * D + d] : fill);
+    }
+    for (int o = 16; o; o >>= 1) mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    double den = 0.0;
+    if (view == 0) {
+      const double* r = vol + p * D;
+      for (int d = lane; d < D; d += 32) den += lik_term(r[d], mn, sigma);
+    } else {
+      for (int d = lane; d < D; d += 32)
+        den += lik_term(x + d < W ? vol[(p + d) * D + d] : fill, mn, sigma);
+    }
+    den = warp_sum(den);
+    if (lane == 0) {
+      double* o = stats + ((int64_t)(m * 2 + view) * HW + p) * 2;
+      o[0] = mn;
+      o[1] = den;
+    }
+  }
+}
+
+// ratio / likelihood of cost c against the statistics (min, den) of its row
+// (featextract.cpp:333, :440).
+__device__ __forceinline__ void confidences(double c, double mn, double den, double e, double sigma,
+                                            float* ratio, float* lik) {
+  if (mn == kRandMax) {
+    *ratio = 0.0f;
+    *lik = 0.0f;
+  } else {
+    *ratio = (float)((mn + e) / (c + e));
+    const double t = c - mn;
+    *lik = (float)(exp(-((t * t) / sigma)) / den);
+  }
+}
+
+// The 20 features of (p, d) in the reference's column order.  The right-
+// reference confidences at left (x, d) are those of right pixel x - d at
+// disparity d, whose cost is C[p, d] itself; for x < d get_left_cost fills
+// with the first element of the right-view feature volume, which is 0 (the
+// right view's pixel (row, 0) has only sentinel costs).
+__device__ __forceinline__ void features_at(const double* const* vols, const double* stats,
+                                            int64_t HW, int64_t W, int D, int64_t p, int64_t x,
+                                            int d, float* f) {
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    const double c = vols[m][p * D + d];
+    f[m] = (float)c;
+    const double* sl = stats + ((int64_t)(m * 2 + 0) * HW + p) * 2;
+    confidences(c, sl[0], sl[1], kEps[m], kSigma[m], &f[4 + m], &f[8 + m]);
+    if (x >= d) {
+      const double* sr = stats + ((int64_t)(m * 2 + 1) * HW + (p - d)) * 2;
+      confidences(c, sr[0], sr[1], kEps[m], kSigma[m], &f[12 + m], &f[16 + m]);
+    } else {
+      f[12 + m] = 0.0f;
+      f[16 + m] = 0.0f;
+    }
+  }
+}
+
+struct FeatVols {
+  const double* v[4];
+};
+
+__global__ void features_kernel(FeatVols fv, const double* __restrict__ stats, int64_t H, int64_t W,
+                                int D, float* __restrict__ out) {
+  const int64_t HW = H * W;
+  GRID_STRIDE(t, HW * D) {
+    const int64_t p = t / D;
+    const int d = (int)(t - p * D);
+    float f[20];
+    features_at(fv.v, stats, HW, W, D, p, p % W, d, f);
+#pragma unroll
+    for (int k = 0; k < 20; k++) out[t * 20 + k] = f[k];
+  }
+}
+
+// Features and random forest fused: each thread builds the 20 features of
+// its (pixel, d) in a private column of shared memory (feature k of thread t
+// at [k][t], so the walk's data-dependent reads never conflict on a bank)
+// and walks every tree; the [H*W*D, 20] feature matrix never reaches HBM.
+// prob0 receives P(class 0) = the matching cost fed to the post-processing.
+__global__ void __launch_bounds__(128) features_rf_kernel(FeatVols fv,
+                                                          const double* __restrict__ stats,
+                                                          int64_t H, int64_t W, int D, RfView f,
+                                                          float* __restrict__ prob0) {
+  extern __shared__ float xs[];
+  const int64_t HW = H * W;
+  const int tid = threadIdx.x;
+  const int B = blockDim.x;
+  GRID_STRIDE(t, HW * D) {
+    const int64_t p = t / D;
+    const int d = (int)(t - p * D);
+    float fe[20];
+    features_at(fv.v, stats, HW, W, D, p, p % W, d, fe);
+#pragma unroll
+    for (int k = 0; k < 20; k++) xs[k * B + tid] = fe[k];
+    double acc = 0.0;
+    for (int tr = 0; tr < f.n_trees; tr++) {
+      uint32_t idx = (uint32_t)__ldg(f.offsets + tr);
+      uint2 node = __ldg(f.nodes + idx);
+      while (!(node.y & kLeafFlag)) {
+        const float x = xs[(node.y & 31u) * B + tid];
+        idx = ((node.y >> 5) & kChildMask) + (x <= __uint_as_float(node.x) ? 0u : 1u);
+        node = __ldg(f.nodes + idx);
+      }
+      acc += __ldg(f.leaf_value + (node.y & ~kLeafFlag)).x;
+    }
+    prob0[t] = (float)(acc / f.n_trees);
+  }
+}
+
+int launch_features_rf(const double* const* vols, const double* stats, int64_t H, int64_t W,
+                       int D, const RfView& f, float* prob0, cudaStream_t st) {
+  FeatVols fv = {{vols[0], vols[1], vols[2], vols[3]}};
+  const int block = 128;
+  features_rf_kernel<<<grid_for(H * W * D, block), block, 20 * block * sizeof(float), st>>>(
+      fv, stats, H, W, D, f, prob0);
+  return check_launch("features_rf");
+}
+
+int launch_feature_stats(const double* const* vols, int64_t H, int64_t W, int D, double* stats,
+                         cudaStream_t st) {
+  const int64_t warps = 2 * H * W;
+  for (int m = 0; m < 4; m++)
+    feature_stats_kernel<<<grid_for(warps * 32, kBlock), kBlock, 0, st>>>(vols[m], m, H, W, D,
+                                                                          hSigma[m], stats);
+  return check_launch("feature_stats");
+}
+
+}  // namespace cbmv
+
+using namespace cbmv;
+
+#define CHECK_VOL(p, q) CBMV_REQUIRE((p) && (q), CBMV_EINVAL, "null pointer argument")
+
+extern "C" int cbmv_swap_axes(const double* in, int64_t D, int64_t H, int64_t W, double* out,
+                              void* stream) {
+  CHECK_VOL(in, out);
+  CBMV_REQUIRE(D > 0 && H > 0 && W > 0, CBMV_EINVAL, "bad size");
+  swap_axes_kernel<<<grid_for(D * H * W, kBlock), kBlock, 0, as_stream(stream)>>>(in, D, H * W, out);
+  return check_launch("swap_axes");
+}
+
+extern "C" int cbmv_swap_axes_back(const double* in, int64_t H, int64_t W, int64_t D, double* out,
+                                   void* stream) {
+  CHECK_VOL(in, out);
+  CBMV_REQUIRE(D > 0 && H > 0 && W > 0, CBMV_EINVAL, "bad size");
+  swap_axes_back_kernel<<<grid_for(D * H * W, kBlock), kBlock, 0, as_stream(stream)>>>(in, H * W, D,
+                                                                                      out);
+  return check_launch("swap_axes_back");
+}
+
+extern "C" int cbmv_get_cost(const double* in, int64_t H, int64_t W, int64_t D, int64_t K,
+                             double* out, void* stream) {
+  CHECK_VOL(in, out);
+  CBMV_REQUIRE(D > 0 && H > 0 && W > 0 && K > 0, CBMV_EINVAL, "bad size");
+  get_cost_kernel<<<grid_for(H * W * D, kBlock), kBlock, 0, as_stream(stream)>>>(in, H * W * D, K, out);
+  return check_launch("get_cost");
+}
+
+extern "C" int cbmv_get_right_cost(const double* C, int64_t H, int64_t W, int64_t D, double* out,
+                                   void* stream) {
+  CHECK_VOL(C, out);
+  CBMV_REQUIRE(D > 0 && H > 0 && W > 0 && C != out, CBMV_EINVAL, "bad size or in-place call");
+  shift_kernel<<<grid_for(H * W * D, kBlock), kBlock, 0, as_stream(stream)>>>(C, H, W, D, 1, out);
+  return check_launch("get_right_cost");
+}
+
+extern "C" int cbmv_get_left_cost(const double* Rv, int64_t H, int64_t W, int64_t D, double* out,
+                                  void* stream) {
+  CHECK_VOL(Rv, out);
+  CBMV_REQUIRE(D > 0 && H > 0 && W > 0 && Rv != out, CBMV_EINVAL, "bad size or in-place call");
+  shift_kernel<<<grid_for(H * W * D, kBlock), kBlock, 0, as_stream(stream)>>>(Rv, H, W, D, -1, out);
+  return check_launch("get_left_cost");
+}
+
+extern "C" int cbmv_extract_ratio(const double* vol, int64_t N, int64_t D, double e, double* out,
+                                  void* stream) {
+  CHECK_VOL(vol, out);
+  CBMV_REQUIRE(N > 0 && D > 0, CBMV_EINVAL, "bad size");
+  ratio_kernel<<<grid_for(N * 32, kBlock), kBlock, 0, as_stream(stream)>>>(vol, N, D, e, out);
+  return check_launch("extract_ratio");
+}
+
+extern "C" int cbmv_extract_likelihood(const double* vol, int64_t N, int64_t D, double sigma,
+                                       double* out, void* stream) {
+  CHECK_VOL(vol, out);
+  CBMV_REQUIRE(N > 0 && D > 0 && sigma > 0, CBMV_EINVAL, "bad size or sigma");
+  likelihood_kernel<<<grid_for(N * 32, kBlock), kBlock, 0, as_stream(stream)>>>(vol, N, D, sigma, out);
+  return check_launch("extract_likelihood");
+}
+
+extern "C" int cbmv_extract_ratio_samples(const double* vol, int64_t N, int64_t D,
+                                          const int32_t* samples, double e, double* out,
+                                          void* stream) {
+  CHECK_VOL(vol, out);
+  CBMV_REQUIRE(samples && N > 0 && D > 0, CBMV_EINVAL, "bad argument");
+  ratio_samples_kernel<<<grid_for(N * 32, kBlock), kBlock, 0, as_stream(stream)>>>(vol, N, D, samples,
+                                                                                  e, out);
+  return check_launch("extract_ratio_samples");
+}
+
+extern "C" int cbmv_extract_likelihood_samples(const double* vol, int64_t N, int64_t D,
+                                               const int32_t* samples, double sigma, double* out,
+                                               void* stream) {
+  CHECK_VOL(vol, out);
+  CBMV_REQUIRE(samples && N > 0 && D > 0 && sigma > 0, CBMV_EINVAL, "bad argument");
+  likelihood_samples_kernel<<<grid_for(N * 32, kBlock), kBlock, 0, as_stream(stream)>>>(
+      vol, N, D, samples, sigma, out);
+  return check_launch("extract_likelihood_samples");
+}
+
+extern "C" int cbmv_get_samples(const double* vol, int64_t N, int64_t D, const int32_t* samples,
+                                double* out, void* stream) {
+  CHECK_VOL(vol, out);
+  CBMV_REQUIRE(samples && N > 0 && D > 0, CBMV_EINVAL, "bad argument");
+  get_samples_kernel<<<grid_for(3 * N, kBlock), kBlock, 0, as_stream(stream)>>>(vol, N, D, samples, out);
+  return check_launch("get_samples");
+}
+
+extern "C" int cbmv_generate_labels(int64_t N, int32_t* out, void* stream) {
+  CBMV_REQUIRE(out && N > 0, CBMV_EINVAL, "bad argument");
+  labels_kernel<<<grid_for(3 * N, kBlock), kBlock, 0, as_stream(stream)>>>(N, out);
+  return check_launch("generate_labels");
+}
+
+extern "C" int cbmv_generate_d_indices(const int32_t* gt, int64_t N, int maxd, int thr,
+                                       uint64_t seed, int32_t* out, void* stream) {
+  CBMV_REQUIRE(gt && out && N > 0 && maxd > 0 && thr >= 0, CBMV_EINVAL, "bad argument");
+  cudaStream_t st = as_stream(stream);
+  int* bad = nullptr;
+  CBMV_CUDA(cudaMallocAsync(&bad, sizeof(int), st));
+  CBMV_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), st));
+  d_indices_kernel<<<grid_for(N, kBlock), kBlock, 0, st>>>(gt, N, maxd, thr, seed, out, bad);
+  int rc = check_launch("generate_d_indices");
+  int hbad = 0;
+  CBMV_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CBMV_CUDA(cudaFreeAsync(bad, st));
+  CBMV_CUDA(cudaStreamSynchronize(st));
+  if (rc) return rc;
+  CBMV_REQUIRE(!hbad, CBMV_EINVAL,
+               "generate_d_indices: a ground-truth value is outside [0, maxd] or leaves an empty "
+               "negative range (gt = maxd - thr - 1)");
+  return CBMV_OK;
+}
+
+extern "C" int cbmv_features(const double* census, const double* ncc, const double* sob,
+                             const double* sad, int64_t H, int64_t W, int D, float* out,
+                             void* stream) {
+  CBMV_REQUIRE(census && ncc && sob && sad && out, CBMV_EINVAL, "null pointer argument");
+  CBMV_REQUIRE(H > 0 && W > 0 && D > 0, CBMV_EINVAL, "bad size");
+  cudaStream_t st = as_stream(stream);
+  double* stats = nullptr;
+  CBMV_CUDA(cudaMallocAsync(&stats, sizeof(double) * 16 * H * W, st));
+  const double* vols[4] = {census, ncc, sob, sad};
+  int rc = launch_feature_stats(vols, H, W, D, stats, st);
+  if (!rc) {
+    FeatVols fv = {{census, ncc, sob, sad}};
+    features_kernel<<<grid_for(H * W * D, kBlock), kBlock, 0, st>>>(fv, stats, H, W, D, out);
+    rc = check_launch("features");
+  }
+  CBMV_CUDA(cudaFreeAsync(stats, st));
+  return rc;
+}

@@ -1,0 +1,301 @@
+// The fused test path for one rectified pair: the work of main.py:53-70
+// (Testing.test_model, test.py:597-626, then Testing.eval_prob with the
+// default `_mem` post-processing, test.py:143-149 and 341-449) as one
+// sequence of device launches on one stream, with every intermediate
+// resident in HBM:
+//
+//   1. per-pixel terms: census descriptors, NCC window sums, ZSAD means,
+//      Sobel responses (both images)
+//   2. the four [H,W,D] float64 cost volumes (census, ncc, sadsob, zsad)
+//   3. per-pixel row minimum and likelihood denominator of every volume, for
+//      the left and the right reference view
+//   4. features + random forest fused -> P(class 0), float32 [H,W,D]
+//   5. post: image normalisation, cross arms, SGM x sgm_i, CBCA x cbca_i2,
+//      winner-take-all + subpixel, median, thresholded Gaussian.
+//
+// The reference's per-row batching of the classifier (test.py:608-623) only
+// bounds its host memory; every feature is row-local, so one launch covers
+// the whole image with identical results.
+#include <math.h>
+#include <string.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "pipeline.cuh"
+#include "post.cuh"
+
+using namespace cbmv;
+
+extern "C" void cbmv_params_default(cbmv_params* p) {
+  // Testing.__init__ defaults, test.py:44-47; SAD-on-Sobel window test.py:131
+  p->censw = 11;
+  p->nccw = 3;
+  p->sadw = 5;
+  p->sobw = 5;
+  p->pi1 = 1.3f;
+  p->pi2 = 10.0f;
+  p->sgm_q1 = 2.2f;
+  p->sgm_q2 = 3.0f;
+  p->alpha1 = 1.4f;
+  p->tau_so = 0.12f;
+  p->sgm_i = 2;
+  p->L1 = 6;
+  p->tau1 = 0.07f;
+  p->cbca_i1 = 0;
+  p->cbca_i2 = 4;
+  p->median_i = 1;
+  p->median_w = 3;
+  p->blur_sigma = 2.2f;
+  p->blur_t = 1.3f;
+  p->direction = -1;  // test.py:501
+}
+
+struct cbmv_ctx {
+  cudaStream_t stream = nullptr;
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  cudaEvent_t ev[6] = {};
+  float ms[5] = {};
+  float* gauss = nullptr;  // device copy of the mean2d kernel
+  int gauss_ks = 0;
+  float gauss_sigma = -1.0f;
+};
+
+namespace {
+
+// Testing.__gaussian, test.py:108-118 (centre offset by one, as written).
+std::vector<float> gaussian_kernel(double sigma, int* ks_out) {
+  const int kr = (int)ceil(sigma * 3);
+  const int ks = kr * 2 + 1;
+  std::vector<float> k((size_t)ks * ks);
+  for (int i = 0; i < ks; i++)
+    for (int j = 0; j < ks; j++) {
+      const double y = (i - 1) - kr, x = (j - 1) - kr;
+      k[(size_t)i * ks + j] = (float)exp(-(x * x + y * y) / (2 * sigma * sigma));
+    }
+  *ks_out = ks;
+  return k;
+}
+
+struct Carve {
+  char* base;
+  size_t off = 0;
+  template <class T>
+  T* take(size_t n) {
+    off = (off + 255) & ~(size_t)255;
+    T* p = (T*)(base ? base + off : nullptr);
+    off += n * sizeof(T);
+    return p;
+  }
+};
+
+struct Work {
+  ulonglong2 *descL, *descR;
+  uint32_t *AL, *AR;
+  double *CL, *CR, *muL, *muR;
+  int32_t *sobL, *sobR;
+  double* vol[4];
+  double* stats;
+  float *volA, *volB;
+  float *imL, *imR, *crossL, *crossR, *dtmp, *dtmp2;
+  double* mom;
+};
+
+Work carve(void* base, int64_t H, int64_t W, int D, size_t* bytes) {
+  Carve c{(char*)base};
+  Work w;
+  const size_t HW = (size_t)H * W, V = HW * (size_t)D;
+  w.descL = c.take<ulonglong2>(HW);
+  w.descR = c.take<ulonglong2>(HW);
+  w.AL = c.take<uint32_t>(HW);
+  w.AR = c.take<uint32_t>(HW);
+  w.CL = c.take<double>(HW);
+  w.CR = c.take<double>(HW);
+  w.muL = c.take<double>(HW);
+  w.muR = c.take<double>(HW);
+  w.sobL = c.take<int32_t>(HW);
+  w.sobR = c.take<int32_t>(HW);
+  for (int m = 0; m < 4; m++) w.vol[m] = c.take<double>(V);
+  w.stats = c.take<double>(16 * HW);
+  w.volA = c.take<float>(V);
+  w.volB = c.take<float>(V);
+  w.imL = c.take<float>(HW);
+  w.imR = c.take<float>(HW);
+  w.crossL = c.take<float>(4 * HW);
+  w.crossR = c.take<float>(4 * HW);
+  w.dtmp = c.take<float>(HW);
+  w.dtmp2 = c.take<float>(HW);
+  w.mom = c.take<double>(4);
+  *bytes = c.off + 256;
+  return w;
+}
+
+int check_params(const cbmv_params* p) {
+  CBMV_REQUIRE(p->censw == 11 && p->nccw >= 1 && p->nccw <= 15 && (p->nccw & 1) && p->sadw >= 1 &&
+                   p->sadw <= 15 && (p->sadw & 1) && p->sobw >= 1 && p->sobw <= 15 && (p->sobw & 1),
+               CBMV_EINVAL, "unsupported matcher windows");
+  CBMV_REQUIRE(p->sgm_i >= 0 && p->cbca_i1 >= 0 && p->cbca_i2 >= 0 && p->median_i >= 0,
+               CBMV_EINVAL, "negative iteration count");
+  CBMV_REQUIRE(p->median_w >= 1 && p->median_w <= 11 && (p->median_w & 1), CBMV_EINVAL,
+               "median window must be odd <= 11");
+  CBMV_REQUIRE(p->blur_sigma > 0 && p->blur_sigma <= 5.0f, CBMV_EINVAL, "blur_sigma not in (0, 5]");
+  CBMV_REQUIRE(p->direction == 1 || p->direction == -1, CBMV_EINVAL, "direction must be +-1");
+  return CBMV_OK;
+}
+
+}  // namespace
+
+extern "C" int cbmv_ctx_create(void* stream, cbmv_ctx** out) {
+  CBMV_REQUIRE(out, CBMV_EINVAL, "null pointer argument");
+  cbmv_ctx* c = new cbmv_ctx();
+  c->stream = as_stream(stream);
+  for (int i = 0; i < 6; i++) {
+    if (cudaEventCreate(&c->ev[i]) != cudaSuccess) {
+      for (int j = 0; j < i; j++) cudaEventDestroy(c->ev[j]);
+      delete c;
+      return set_error(CBMV_ECUDA, "cudaEventCreate failed");
+    }
+  }
+  *out = c;
+  return CBMV_OK;
+}
+
+extern "C" int cbmv_ctx_destroy(cbmv_ctx* c) {
+  if (!c) return CBMV_OK;
+  cudaStreamSynchronize(c->stream);
+  if (c->ws) cudaFree(c->ws);
+  if (c->gauss) cudaFree(c->gauss);
+  for (int i = 0; i < 6; i++) cudaEventDestroy(c->ev[i]);
+  delete c;
+  return CBMV_OK;
+}
+
+extern "C" int cbmv_ctx_timings(cbmv_ctx* c, float* ms5) {
+  CBMV_REQUIRE(c && ms5, CBMV_EINVAL, "null pointer argument");
+  const int pairs[5][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {0, 4}};
+  for (int k = 0; k < 5; k++) CBMV_CUDA(cudaEventElapsedTime(&ms5[k], c->ev[pairs[k][0]], c->ev[pairs[k][1]]));
+  return CBMV_OK;
+}
+
+static int ensure_workspace(cbmv_ctx* c, size_t bytes) {
+  if (c->ws_bytes >= bytes) return CBMV_OK;
+  CBMV_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->ws) cudaFree(c->ws);
+  c->ws = nullptr;
+  c->ws_bytes = 0;
+  cudaError_t e = cudaMalloc(&c->ws, bytes);
+  if (e != cudaSuccess)
+    return set_error(CBMV_ENOMEM, "workspace of %zu bytes: %s", bytes, cudaGetErrorString(e));
+  c->ws_bytes = bytes;
+  return CBMV_OK;
+}
+
+static int ensure_gaussian(cbmv_ctx* c, float sigma) {
+  if (c->gauss && c->gauss_sigma == sigma) return CBMV_OK;
+  int ks = 0;
+  std::vector<float> k = gaussian_kernel(sigma, &ks);
+  if (c->gauss) {
+    CBMV_CUDA(cudaStreamSynchronize(c->stream));
+    cudaFree(c->gauss);
+    c->gauss = nullptr;
+  }
+  CBMV_CUDA(cudaMalloc(&c->gauss, k.size() * sizeof(float)));
+  CBMV_CUDA(cudaMemcpy(c->gauss, k.data(), k.size() * sizeof(float), cudaMemcpyHostToDevice));
+  c->gauss_ks = ks;
+  c->gauss_sigma = sigma;
+  return CBMV_OK;
+}
+
+#define RC(x)                 \
+  do {                        \
+    int rc_ = (x);            \
+    if (rc_) return rc_;      \
+  } while (0)
+
+// Steps 5 of the header comment on the float32 volume in w.volA; the
+// disparity lands in `disp`.
+static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
+                    int64_t H, int64_t W, int D, Work& w, float* disp) {
+  cudaStream_t st = c->stream;
+  const int64_t HW = H * W;
+  RC(ensure_gaussian(c, p->blur_sigma));
+  RC(launch_normalise(L, HW, w.mom, w.imL, st));
+  RC(launch_normalise(R, HW, w.mom + 2, w.imR, st));
+  RC(launch_cross(w.imL, H, W, p->L1, p->tau1, w.crossL, st));
+  RC(launch_cross(w.imR, H, W, p->L1, p->tau1, w.crossR, st));
+  float* cur = w.volA;
+  float* oth = w.volB;
+  for (int i = 0; i < p->cbca_i1; i++) {
+    RC(launch_cbca(w.crossL, w.crossR, cur, H, W, D, CBMV_HWD, p->direction, oth, st));
+    float* t = cur; cur = oth; oth = t;
+  }
+  SgmParams sp{p->pi1, p->pi2, p->tau_so, p->alpha1, p->sgm_q1, p->sgm_q2, p->direction};
+  for (int i = 0; i < p->sgm_i; i++) {
+    // out = ((L0 + L1 + L2) + L3) / 4   (test.py:379-383)
+    RC(launch_sgm_direction(0, w.imL, w.imR, cur, H, W, D, sp, 0, 1.0f, oth, st));
+    RC(launch_sgm_direction(1, w.imL, w.imR, cur, H, W, D, sp, 1, 1.0f, oth, st));
+    RC(launch_sgm_direction(2, w.imL, w.imR, cur, H, W, D, sp, 1, 1.0f, oth, st));
+    RC(launch_sgm_direction(3, w.imL, w.imR, cur, H, W, D, sp, 2, 0.25f, oth, st));
+    float* t = cur; cur = oth; oth = t;
+  }
+  for (int i = 0; i < p->cbca_i2; i++) {
+    RC(launch_cbca(w.crossL, w.crossR, cur, H, W, D, CBMV_HWD, p->direction, oth, st));
+    float* t = cur; cur = oth; oth = t;
+  }
+  float* d0 = w.dtmp;
+  float* d1 = w.dtmp2;
+  RC(launch_wta_subpixel(cur, H, W, D, nullptr, d0, st));
+  for (int i = 0; i < p->median_i; i++) {
+    RC(launch_median(d0, H, W, p->median_w, d1, st));
+    float* t = d0; d0 = d1; d1 = t;
+  }
+  RC(launch_mean2d(d0, H, W, c->gauss, c->gauss_ks, p->blur_t, disp, st));
+  return CBMV_OK;
+}
+
+extern "C" int cbmv_run_rf(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params* p,
+                           const uint8_t* L, const uint8_t* R, int64_t H, int64_t W, int D,
+                           float* disp, float* prob0) {
+  CBMV_REQUIRE(c && f && L && R && disp, CBMV_EINVAL, "null pointer argument");
+  cbmv_params def;
+  if (!p) {
+    cbmv_params_default(&def);
+    p = &def;
+  }
+  RC(check_params(p));
+  CBMV_REQUIRE(H > p->censw && W > p->censw, CBMV_EINVAL, "image %lldx%lld smaller than the census window",
+               (long long)W, (long long)H);
+  CBMV_REQUIRE(H <= 65535 && D >= 1 && D <= 1024, CBMV_ERANGE, "H must be <= 65535 and D in 1..1024");
+  CBMV_REQUIRE(forest_view(f)->n_features == 20, CBMV_EINVAL, "the forest must take the 20 CBMV features");
+  size_t bytes = 0;
+  carve(nullptr, H, W, D, &bytes);
+  RC(ensure_workspace(c, bytes));
+  Work w = carve(c->ws, H, W, D, &bytes);
+  cudaStream_t st = c->stream;
+
+  CBMV_CUDA(cudaEventRecord(c->ev[0], st));
+  RC(launch_census_desc(L, H, W, p->censw, w.descL, st));
+  RC(launch_census_desc(R, H, W, p->censw, w.descR, st));
+  RC(launch_ncc_stats(L, H, W, p->nccw, w.AL, w.CL, st));
+  RC(launch_ncc_stats(R, H, W, p->nccw, w.AR, w.CR, st));
+  RC(launch_zsad_means(L, H, W, p->sadw, w.muL, st));
+  RC(launch_zsad_means(R, H, W, p->sadw, w.muR, st));
+  RC(launch_sobel_i32(L, H, W, w.sobL, st));
+  RC(launch_sobel_i32(R, H, W, w.sobR, st));
+  RC(launch_census_cost<double>(w.descL, w.descR, H, W, D, p->censw, CBMV_HWD, w.vol[0], st));
+  RC(launch_ncc_cost<double>(L, R, w.AL, w.AR, w.CL, w.CR, H, W, D, p->nccw, CBMV_HWD, w.vol[1], st));
+  RC(launch_sadsob_cost<double>(w.sobL, w.sobR, H, W, D, p->sobw, CBMV_HWD, w.vol[2], st));
+  RC(launch_zsad_cost<double>(L, R, w.muL, w.muR, H, W, D, p->sadw, CBMV_HWD, w.vol[3], st));
+  CBMV_CUDA(cudaEventRecord(c->ev[1], st));
+  const double* vols[4] = {w.vol[0], w.vol[1], w.vol[2], w.vol[3]};
+  RC(launch_feature_stats(vols, H, W, D, w.stats, st));
+  CBMV_CUDA(cudaEventRecord(c->ev[2], st));
+  RC(launch_features_rf(vols, w.stats, H, W, D, *forest_view(f), w.volA, st));
+  if (prob0)
+    CBMV_CUDA(cudaMemcpyAsync(prob0, w.volA, sizeof(float) * H * W * D, cudaMemcpyDeviceToDevice, st));
+  CBMV_CUDA(cudaEventRecord(c->ev[3], st));
+  RC(run_post(c, p, L, R, H, W, D, w, disp));
+  CBMV_CUDA(cudaEventRecord(c->ev[4], st));
+  return CBMV_OK;
+}

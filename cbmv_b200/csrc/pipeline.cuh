@@ -1,0 +1,35 @@
+// Launch helpers shared by the fused pipeline (pipeline.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rf.cuh"
+
+namespace cbmv {
+
+int launch_census_desc(const uint8_t* img, int64_t H, int64_t W, int w, ulonglong2* desc,
+                       cudaStream_t st);
+template <class T>
+int launch_census_cost(const ulonglong2* dl, const ulonglong2* dr, int64_t H, int64_t W, int D,
+                       int w, int layout, T* out, cudaStream_t st);
+int launch_ncc_stats(const uint8_t* img, int64_t H, int64_t W, int w, uint32_t* A, double* C,
+                     cudaStream_t st);
+template <class T>
+int launch_ncc_cost(const uint8_t* L, const uint8_t* R, const uint32_t* Al, const uint32_t* Ar,
+                    const double* Cl, const double* Cr, int64_t H, int64_t W, int D, int w,
+                    int layout, T* out, cudaStream_t st);
+int launch_sobel_i32(const uint8_t* img, int64_t H, int64_t W, int32_t* out, cudaStream_t st);
+template <class T>
+int launch_sadsob_cost(const int32_t* SL, const int32_t* SR, int64_t H, int64_t W, int D, int w,
+                       int layout, T* out, cudaStream_t st);
+int launch_zsad_means(const uint8_t* img, int64_t H, int64_t W, int w, double* mean,
+                      cudaStream_t st);
+template <class T>
+int launch_zsad_cost(const uint8_t* L, const uint8_t* R, const double* ml, const double* mr,
+                     int64_t H, int64_t W, int D, int w, int layout, T* out, cudaStream_t st);
+int launch_feature_stats(const double* const* vols, int64_t H, int64_t W, int D, double* stats,
+                         cudaStream_t st);
+int launch_features_rf(const double* const* vols, const double* stats, int64_t H, int64_t W,
+                       int D, const RfView& f, float* prob0, cudaStream_t st);
+
+}  // namespace cbmv

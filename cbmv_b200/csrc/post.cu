@@ -1,0 +1,681 @@
+// MC-CNN cost optimisation ("post", cpp/post/post.cu), float32 on the device.
+//
+// The reference keeps its volumes in float64 and does most arithmetic in
+// float32; these kernels keep the volumes in float32 and do the same float32
+// arithmetic as the reference kernels (comparisons, arm bounds, transition
+// penalties, CBCA summation order, subpixel parabola, median, thresholded
+// Gaussian).  Where the reference accumulates in float64 (the SGM path
+// values and their sum over the four directions) the sums here are float32.
+//
+// SGM runs one scan direction per launch with one warp per scan line and the
+// scan inside the kernel (the reference launches one kernel per scan step,
+// 2(W+H) launches per call, post.cu:273-330); each lane holds D/32 path
+// values in registers, the minimum over d is a warp-shuffle reduction, and
+// the next step's costs are loaded one step ahead.
+#include "common.cuh"
+#include "post.cuh"
+
+namespace cbmv {
+namespace {
+
+constexpr int kBlock = 128;
+
+#define GRID_STRIDE(i, n) \
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+__device__ __forceinline__ void decode(int layout, int64_t t, int64_t H, int64_t W, int64_t D,
+                                       int64_t* y, int64_t* x, int64_t* d) {
+  if (layout == CBMV_HWD) {
+    *d = t % D;
+    const int64_t p = t / D;
+    *x = p % W;
+    *y = p / W;
+  } else {
+    *x = t % W;
+    const int64_t q = t / W;
+    *y = q % H;
+    *d = q / H;
+  }
+}
+
+// cross (post.cu:336-396)
+__global__ void cross_kernel(const float* __restrict__ x0, int64_t H, int64_t W, int L1, float tau1,
+                             float* __restrict__ out) {
+  GRID_STRIDE(id, 4 * H * W) {
+    const int64_t x = id % W, y = (id / W) % H;
+    const int dir = (int)(id / (W * H));
+    const int dx = dir == 0 ? -1 : dir == 1 ? 1 : 0;
+    const int dy = dir == 2 ? -1 : dir == 3 ? 1 : 0;
+    const float c = x0[y * W + x];
+    int64_t xx = x + dx, yy = y + dy;
+    for (;; xx += dx, yy += dy) {
+      if (xx < 0 || xx >= W || yy < 0 || yy >= H) break;
+      const int64_t dist = max(llabs(xx - x), llabs(yy - y));
+      if (dist == 1) continue;
+      if (fabsf(c - x0[yy * W + xx]) >= tau1) break;  // rule 1
+      if (dist >= L1) break;                          // rule 2
+    }
+    out[id] = (float)(dir <= 1 ? xx : yy);
+  }
+}
+
+// One scan direction of sgm2 (post.cu:178-261) per launch; warp = scan line.
+// mode 0: out = L; mode 1: out += L; mode 2: out = (out + L) * scale.
+template <int DIR, int KPL>
+__global__ void __launch_bounds__(128) sgm_kernel(const float* __restrict__ x0,
+                                                  const float* __restrict__ x1,
+                                                  const float* __restrict__ in, int H, int W, int D,
+                                                  SgmParams sp, int mode, float scale,
+                                                  float* __restrict__ out) {
+  const int line = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  const int nlines = DIR <= 1 ? H : W;
+  if (line >= nlines) return;
+  const int nsteps = DIR <= 1 ? W : H;
+  const int dx = DIR == 0 ? 1 : DIR == 1 ? -1 : 0;
+  const int dy = DIR == 2 ? 1 : DIR == 3 ? -1 : 0;
+  const float inf = __int_as_float(0x7f800000);
+  // penalties of post.cu:239-248 and the alpha1 split of :252/:255
+  const float p1a = sp.pi1, p2a = sp.pi2;
+  const float p1b = sp.pi1 / (sp.q1 * sp.q2), p2b = sp.pi2 / (sp.q1 * sp.q2);
+  const float p1c = sp.pi1 / sp.q1, p2c = sp.pi2 / sp.q1;
+
+  float prev[KPL], nxt[KPL];
+  auto coords = [&](int step, int& x, int& y) {
+    if (DIR == 0) { x = step; y = line; }
+    else if (DIR == 1) { x = W - 1 - step; y = line; }
+    else if (DIR == 2) { x = line; y = step; }
+    else { x = line; y = H - 1 - step; }
+  };
+  auto load = [&](int step, float* v) {
+    int x, y;
+    coords(step, x, y);
+    const float* src = in + ((int64_t)y * W + x) * D;
+#pragma unroll
+    for (int k = 0; k < KPL; k++) {
+      const int d = lane + 32 * k;
+      v[k] = d < D ? src[d] : inf;
+    }
+  };
+  load(0, nxt);
+  for (int step = 0; step < nsteps; step++) {
+    float cur[KPL];
+#pragma unroll
+    for (int k = 0; k < KPL; k++) cur[k] = nxt[k];
+    if (step + 1 < nsteps) load(step + 1, nxt);
+    int x, y;
+    coords(step, x, y);
+    float L[KPL];
+    if (step == 0) {
+#pragma unroll
+      for (int k = 0; k < KPL; k++) L[k] = cur[k];
+    } else {
+      float mn = prev[0];
+#pragma unroll
+      for (int k = 1; k < KPL; k++) mn = fminf(mn, prev[k]);
+#pragma unroll
+      for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+      const int64_t ind2 = (int64_t)y * W + x;
+      const int64_t indp = ind2 - (int64_t)dy * W - dx;
+      const float D1 = fabsf(x0[ind2] - x0[indp]);
+#pragma unroll
+      for (int k = 0; k < KPL; k++) {
+        const int d = lane + 32 * k;
+        // neighbours d-1 and d+1 of the previous step
+        float lo = __shfl_up_sync(0xffffffffu, prev[k], 1);
+        float hi = __shfl_down_sync(0xffffffffu, prev[k], 1);
+        const float lo_w = __shfl_sync(0xffffffffu, prev[k > 0 ? k - 1 : 0], 31);
+        const float hi_w = __shfl_sync(0xffffffffu, prev[k + 1 < KPL ? k + 1 : k], 0);
+        if (lane == 0) lo = lo_w;
+        if (lane == 31) hi = hi_w;
+        if (d < D) {
+          const int xx = x + d * sp.direction;
+          float D2;
+          if (xx < 0 || xx >= W || xx - dx < 0 || xx - dx >= W)
+            D2 = 10.0f;
+          else
+            D2 = fabsf(x1[ind2 + d * sp.direction] - x1[indp + d * sp.direction]);
+          float P1, P2;
+          if (D1 < sp.tau_so && D2 < sp.tau_so) { P1 = p1a; P2 = p2a; }
+          else if (D1 > sp.tau_so && D2 > sp.tau_so) { P1 = p1b; P2 = p2b; }
+          else { P1 = p1c; P2 = p2c; }
+          float cost = fminf(prev[k], mn + P2);
+          if (d - 1 >= 0) cost = fminf(cost, lo + (DIR == 2 ? P1 / sp.alpha1 : P1));
+          if (d + 1 < D) cost = fminf(cost, hi + (DIR == 3 ? P1 / sp.alpha1 : P1));
+          L[k] = cur[k] + cost - mn;
+        } else {
+          L[k] = inf;
+        }
+      }
+    }
+    float* dst = out + ((int64_t)y * W + x) * D;
+#pragma unroll
+    for (int k = 0; k < KPL; k++) {
+      const int d = lane + 32 * k;
+      if (d < D) {
+        if (mode == 0) dst[d] = L[k];
+        else if (mode == 1) dst[d] += L[k];
+        else dst[d] = (dst[d] + L[k]) * scale;
+      }
+      prev[k] = L[k];
+    }
+  }
+}
+
+// cbca (post.cu:399-450), any layout.
+__global__ void cbca_kernel(const float* __restrict__ lc, const float* __restrict__ rc,
+                            const float* __restrict__ in, int64_t H, int64_t W, int64_t D,
+                            int layout, int direction, float* __restrict__ out) {
+  GRID_STRIDE(id, H * W * D) {
+    int64_t y, x, d;
+    decode(layout, id, H, W, D, &y, &x, &d);
+    const int64_t xm = x + d * direction;
+    if (xm < 0 || xm >= W) {
+      out[id] = in[id];
+      continue;
+    }
+    const int yy_s = (int)fmaxf(lc[(2 * H + y) * W + x], rc[(2 * H + y) * W + xm]);
+    const int yy_t = (int)fminf(lc[(3 * H + y) * W + x], rc[(3 * H + y) * W + xm]);
+    const float dd = (float)(d * direction);
+    float sum = 0.0f;
+    int cnt = 0;
+    for (int yy = yy_s + 1; yy < yy_t; yy++) {
+      const int xx_s = (int)fmaxf(lc[(0 * H + yy) * W + x], rc[(0 * H + yy) * W + xm] - dd);
+      const int xx_t = (int)fminf(lc[(1 * H + yy) * W + x], rc[(1 * H + yy) * W + xm] - dd);
+      for (int xx = xx_s + 1; xx < xx_t; xx++) {
+        sum += in[vol_index(layout, yy, xx, d, H, W, D)];
+        cnt++;
+      }
+    }
+    out[id] = sum / (float)cnt;
+  }
+}
+
+// Winner-take-all (first minimum, as np.argmin) and the subpixel parabola
+// (post.cu:453-483).  One warp per pixel on [H,W,D] volumes.
+__global__ void wta_subpixel_hwd_kernel(const float* __restrict__ c, int64_t HW, int D,
+                                        float* __restrict__ disp_int, float* __restrict__ disp) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < HW; p += nw) {
+    const float* r = c + p * D;
+    float bv = __int_as_float(0x7f800000);
+    int bd = 0x7fffffff;
+    for (int d = lane; d < D; d += 32) {
+      const float v = r[d];
+      if (v < bv) { bv = v; bd = d; }
+    }
+    for (int o = 16; o; o >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int od = __shfl_xor_sync(0xffffffffu, bd, o);
+      if (ov < bv || (ov == bv && od < bd)) { bv = ov; bd = od; }
+    }
+    if (bd == 0x7fffffff) bd = 0;  // all NaN: np.argmin would return 0 for a NaN at 0
+    if (lane == 0) {
+      if (disp_int) disp_int[p] = (float)bd;
+      if (disp) {
+        float o = (float)bd;
+        if (1 <= bd && bd < D - 1) {
+          const float cn = r[bd - 1], cz = r[bd], cp = r[bd + 1];
+          const float denom = 2 * (cp + cn - 2 * cz);
+          if (denom > 1e-5) {
+            const double q = (double)((cp - cn) / denom);
+            o = (float)(bd - fmin(1.0, fmax(-1.0, q)));
+          }
+        }
+        disp[p] = o;
+      }
+    }
+  }
+}
+
+__global__ void wta_dhw_kernel(const float* __restrict__ c, int64_t HW, int D,
+                               float* __restrict__ disp) {
+  GRID_STRIDE(p, HW) {
+    float bv = c[p];
+    int bd = 0;
+    for (int d = 1; d < D; d++) {
+      const float v = c[(int64_t)d * HW + p];
+      if (v < bv) { bv = v; bd = d; }
+    }
+    disp[p] = (float)bd;
+  }
+}
+
+__global__ void subpixel_kernel(const float* __restrict__ d0, const float* __restrict__ c,
+                                int64_t H, int64_t W, int D, int layout, float* __restrict__ out) {
+  GRID_STRIDE(id, H * W) {
+    const int d = (int)d0[id];
+    float o = (float)d;
+    if (1 <= d && d < D - 1) {
+      const int64_t y = id / W, x = id - y * W;
+      const float cn = c[vol_index(layout, y, x, d - 1, H, W, D)];
+      const float cz = c[vol_index(layout, y, x, d, H, W, D)];
+      const float cp = c[vol_index(layout, y, x, d + 1, H, W, D)];
+      const float denom = 2 * (cp + cn - 2 * cz);
+      if (denom > 1e-5) {
+        const double q = (double)((cp - cn) / denom);
+        o = (float)(d - fmin(1.0, fmax(-1.0, q)));
+      }
+    }
+    out[id] = o;
+  }
+}
+
+__device__ void sort_small(float* x, int n) {
+  for (int i = 0; i < n - 1; i++) {
+    int mn = i;
+    for (int j = i + 1; j < n; j++)
+      if (x[j] < x[mn]) mn = j;
+    const float t = x[mn];
+    x[mn] = x[i];
+    x[i] = t;
+  }
+}
+
+// median2d (post.cu:486-518)
+__global__ void median_kernel(const float* __restrict__ img, int64_t H, int64_t W, int r,
+                              float* __restrict__ out) {
+  GRID_STRIDE(id, H * W) {
+    const int64_t x = id % W, y = id / W;
+    float xs[11 * 11];
+    int n = 0;
+    for (int64_t xx = x - r; xx <= x + r; xx++)
+      for (int64_t yy = y - r; yy <= y + r; yy++)
+        if (0 <= xx && xx < W && 0 <= yy && yy < H) xs[n++] = img[yy * W + xx];
+    sort_small(xs, n);
+    out[id] = xs[n / 2];
+  }
+}
+
+// mean2d (post.cu:520-566): kernel indexed xx-major as the reference.
+__global__ void mean2d_kernel(const float* __restrict__ img, int64_t H, int64_t W,
+                              const float* __restrict__ kernel, int r, float alpha2,
+                              float* __restrict__ out) {
+  GRID_STRIDE(id, H * W) {
+    const int64_t x = id % W, y = id / W;
+    const float c = img[id];
+    float sum = 0.0f, cnt = 0.0f;
+    int i = 0;
+    for (int64_t xx = x - r; xx <= x + r; xx++)
+      for (int64_t yy = y - r; yy <= y + r; yy++, i++)
+        if (0 <= xx && xx < W && 0 <= yy && yy < H) {
+          const float v = img[yy * W + xx];
+          if (fabsf(v - c) < alpha2) {
+            sum = fmaf(v, kernel[i], sum);
+            cnt += kernel[i];
+          }
+        }
+    out[id] = sum / cnt;
+  }
+}
+
+// outlier_detection (post.cu:717-754)
+__global__ void outlier_kernel(const float* __restrict__ d0, const float* __restrict__ d1,
+                               int64_t H, int64_t W, int disp_max, float* __restrict__ out) {
+  GRID_STRIDE(id, H * W) {
+    const int64_t x = id % W;
+    const int d0i = (int)d0[id];
+    float o;
+    if (x - d0i < 0 || x - d0i >= W) {  // (>= W only for negative input, where the reference reads out of bounds)
+      o = 1;
+    } else if (fabsf(d0[id] - d1[id - d0i]) < 1.1) {
+      o = 0;
+    } else {
+      o = 1;
+      for (int d = 0; d < disp_max; d++)
+        if (x - d >= 0 && fabsf((float)d - d1[id - d]) < 1.1) {
+          o = 2;
+          break;
+        }
+    }
+    out[id] = o;
+  }
+}
+
+// interpolate_mismatch (post.cu:757-827).  Where every direction leaves the
+// image before meeting a non-mismatch pixel the reference asserts; here the
+// pixel keeps its disparity.
+__global__ void mismatch_kernel(const float* __restrict__ d0, const float* __restrict__ outlier,
+                                int64_t H, int64_t W, float* __restrict__ out) {
+  const float dir[32] = {0, 1, -0.5f, 1, -1, 1, -1, 0.5f, -1, 0, -1, -0.5f, -1, -1, -0.5f, -1,
+                         0, -1, 0.5f, -1, 1, -1, 1, -0.5f, 1, 0, 1, 0.5f, 1, 1, 0.5f, 1};
+  GRID_STRIDE(id, H * W) {
+    if (outlier[id] != 2) {
+      out[id] = d0[id];
+      continue;
+    }
+    float vals[16];
+    int n = 0;
+    const int64_t x = id % W, y = id / W;
+    for (int k = 0; k < 16; k++) {
+      const float dx = dir[2 * k], dy = dir[2 * k + 1];
+      float xx = (float)x, yy = (float)y;
+      int64_t xi = (int64_t)roundf(xx), yi = (int64_t)roundf(yy);
+      while (0 <= yi && yi < H && 0 <= xi && xi < W && outlier[yi * W + xi] == 2) {
+        xx += dx;
+        yy += dy;
+        xi = (int64_t)roundf(xx);
+        yi = (int64_t)roundf(yy);
+      }
+      if (0 <= yi && yi < H && 0 <= xi && xi < W) vals[n++] = d0[yi * W + xi];
+    }
+    if (n == 0) {
+      out[id] = d0[id];
+      continue;
+    }
+    sort_small(vals, n);
+    out[id] = vals[n / 2];
+  }
+}
+
+// interpolate_occlusion (post.cu:829-869)
+__global__ void occlusion_kernel(const float* __restrict__ d0, const float* __restrict__ outlier,
+                                 int64_t H, int64_t W, float* __restrict__ out) {
+  GRID_STRIDE(id, H * W) {
+    if (outlier[id] != 1) {
+      out[id] = d0[id];
+      continue;
+    }
+    const int64_t x = id % W;
+    int64_t dx = 0;
+    while (x + dx >= 0 && outlier[id + dx] != 0) dx--;
+    if (x + dx < 0) {
+      dx = 0;
+      while (x + dx < W && outlier[id + dx] != 0) dx++;
+    }
+    out[id] = (x + dx < W) ? d0[id + dx] : d0[id];
+  }
+}
+
+// [H*W, D] <-> [D, H*W] tiled transpose of float32.
+__global__ void transpose_kernel(const float* __restrict__ in, int64_t rows, int64_t cols,
+                                 float* __restrict__ out) {
+  __shared__ float tile[32][33];
+  const int64_t c0 = (int64_t)blockIdx.x * 32, r0 = (int64_t)blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int64_t r = r0 + k, c = c0 + threadIdx.x;
+    if (r < rows && c < cols) tile[k][threadIdx.x] = in[r * cols + c];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int64_t c = c0 + k, r = r0 + threadIdx.x;
+    if (r < rows && c < cols) out[c * rows + r] = tile[threadIdx.x][k];
+  }
+}
+
+__global__ void scale_kernel(float* a, int64_t n, float mul) {
+  GRID_STRIDE(i, n) a[i] *= mul;
+}
+
+__global__ void f64_to_f32_kernel(const double* __restrict__ in, int64_t n, float* __restrict__ out) {
+  GRID_STRIDE(i, n) out[i] = (float)in[i];
+}
+
+__global__ void f32_to_f64_kernel(const float* __restrict__ in, int64_t n, double* __restrict__ out) {
+  GRID_STRIDE(i, n) out[i] = (double)in[i];
+}
+
+// Sums of an image and of its squares in float64 (one block).
+__global__ void moments_kernel(const uint8_t* __restrict__ img, int64_t n, double* __restrict__ mom) {
+  __shared__ double s1[32], s2[32];
+  double a = 0.0, b = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const double v = img[i];
+    a += v;
+    b += v * v;
+  }
+  for (int o = 16; o; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    s1[threadIdx.x >> 5] = a;
+    s2[threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double A = 0.0, B = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
+      A += s1[k];
+      B += s2[k];
+    }
+    mom[0] = A;
+    mom[1] = B;
+  }
+}
+
+// (I - mean) / std in float32 with float32 mean and population std, as
+// test.py:489-492 does with numpy on the float32 image.
+__global__ void normalise_kernel(const uint8_t* __restrict__ img, int64_t n,
+                                 const double* __restrict__ mom, float* __restrict__ out) {
+  const double mean = mom[0] / (double)n;
+  const double var = fmax(mom[1] / (double)n - mean * mean, 0.0);
+  const float m = (float)mean, s = (float)sqrt(var);
+  GRID_STRIDE(i, n) out[i] = ((float)img[i] - m) / s;
+}
+
+}  // namespace
+
+int launch_cross(const float* img, int64_t H, int64_t W, int L1, float tau1, float* out,
+                 cudaStream_t st) {
+  cross_kernel<<<grid_for(4 * H * W, kBlock), kBlock, 0, st>>>(img, H, W, L1, tau1, out);
+  return check_launch("cross");
+}
+
+template <int DIR, int KPL>
+static void sgm_launch(const float* x0, const float* x1, const float* in, int H, int W, int D,
+                       const SgmParams& sp, int mode, float scale, float* out, cudaStream_t st) {
+  const int nlines = DIR <= 1 ? H : W;
+  const int blocks = (nlines * 32 + 127) / 128;
+  sgm_kernel<DIR, KPL><<<blocks, 128, 0, st>>>(x0, x1, in, H, W, D, sp, mode, scale, out);
+}
+
+template <int KPL>
+static void sgm_dir(int dir, const float* x0, const float* x1, const float* in, int H, int W, int D,
+                    const SgmParams& sp, int mode, float scale, float* out, cudaStream_t st) {
+  switch (dir) {
+    case 0: sgm_launch<0, KPL>(x0, x1, in, H, W, D, sp, mode, scale, out, st); break;
+    case 1: sgm_launch<1, KPL>(x0, x1, in, H, W, D, sp, mode, scale, out, st); break;
+    case 2: sgm_launch<2, KPL>(x0, x1, in, H, W, D, sp, mode, scale, out, st); break;
+    default: sgm_launch<3, KPL>(x0, x1, in, H, W, D, sp, mode, scale, out, st); break;
+  }
+}
+
+int launch_sgm_direction(int dir, const float* x0, const float* x1, const float* in, int64_t H,
+                         int64_t W, int D, const SgmParams& sp, int mode, float scale, float* out,
+                         cudaStream_t st) {
+  const int kpl = (D + 31) / 32;
+  const int h = (int)H, w = (int)W;
+  if (kpl <= 1) sgm_dir<1>(dir, x0, x1, in, h, w, D, sp, mode, scale, out, st);
+  else if (kpl <= 2) sgm_dir<2>(dir, x0, x1, in, h, w, D, sp, mode, scale, out, st);
+  else if (kpl <= 4) sgm_dir<4>(dir, x0, x1, in, h, w, D, sp, mode, scale, out, st);
+  else if (kpl <= 8) sgm_dir<8>(dir, x0, x1, in, h, w, D, sp, mode, scale, out, st);
+  else if (kpl <= 16) sgm_dir<16>(dir, x0, x1, in, h, w, D, sp, mode, scale, out, st);
+  else sgm_dir<32>(dir, x0, x1, in, h, w, D, sp, mode, scale, out, st);
+  return check_launch("sgm");
+}
+
+int launch_cbca(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
+                int layout, int direction, float* out, cudaStream_t st) {
+  cbca_kernel<<<grid_for(H * W * D, kBlock), kBlock, 0, st>>>(lc, rc, in, H, W, D, layout, direction,
+                                                             out);
+  return check_launch("cbca");
+}
+
+int launch_wta_subpixel(const float* cost, int64_t H, int64_t W, int D, float* disp_int,
+                        float* disp, cudaStream_t st) {
+  wta_subpixel_hwd_kernel<<<grid_for(H * W * 32, 256), 256, 0, st>>>(cost, H * W, D, disp_int, disp);
+  return check_launch("wta_subpixel");
+}
+
+int launch_median(const float* in, int64_t H, int64_t W, int k, float* out, cudaStream_t st) {
+  median_kernel<<<grid_for(H * W, kBlock), kBlock, 0, st>>>(in, H, W, k / 2, out);
+  return check_launch("median2d");
+}
+
+int launch_mean2d(const float* in, int64_t H, int64_t W, const float* kernel, int ks, float alpha2,
+                  float* out, cudaStream_t st) {
+  mean2d_kernel<<<grid_for(H * W, kBlock), kBlock, 0, st>>>(in, H, W, kernel, ks / 2, alpha2, out);
+  return check_launch("mean2d");
+}
+
+int launch_normalise(const uint8_t* img, int64_t n, double* mom, float* out, cudaStream_t st) {
+  moments_kernel<<<1, 1024, 0, st>>>(img, n, mom);
+  normalise_kernel<<<grid_for(n, 256), 256, 0, st>>>(img, n, mom, out);
+  return check_launch("normalise");
+}
+
+int launch_outlier(const float* d0, const float* d1, int64_t H, int64_t W, int disp_max, float* out,
+                   cudaStream_t st) {
+  outlier_kernel<<<grid_for(H * W, kBlock), kBlock, 0, st>>>(d0, d1, H, W, disp_max, out);
+  return check_launch("outlier_detection");
+}
+
+int launch_mismatch(const float* d0, const float* o, int64_t H, int64_t W, float* out,
+                    cudaStream_t st) {
+  mismatch_kernel<<<grid_for(H * W, kBlock), kBlock, 0, st>>>(d0, o, H, W, out);
+  return check_launch("interpolate_mismatch");
+}
+
+int launch_occlusion(const float* d0, const float* o, int64_t H, int64_t W, float* out,
+                     cudaStream_t st) {
+  occlusion_kernel<<<grid_for(H * W, kBlock), kBlock, 0, st>>>(d0, o, H, W, out);
+  return check_launch("interpolate_occlusion");
+}
+
+}  // namespace cbmv
+
+using namespace cbmv;
+
+#define REQ_PTR(...) CBMV_REQUIRE(__VA_ARGS__, CBMV_EINVAL, "null pointer argument")
+#define REQ_HW(H, W) \
+  CBMV_REQUIRE((H) > 0 && (W) > 0 && (H) <= (1 << 30) && (W) <= (1 << 30), CBMV_EINVAL, "bad size")
+
+extern "C" int cbmv_cross(const float* img, int64_t H, int64_t W, int L1, float tau1, float* out,
+                          void* stream) {
+  REQ_PTR(img && out);
+  REQ_HW(H, W);
+  return launch_cross(img, H, W, L1, tau1, out, as_stream(stream));
+}
+
+extern "C" int cbmv_sgm(const float* imL, const float* imR, const float* in, int64_t H, int64_t W,
+                        int D, float pi1, float pi2, float tau_so, float alpha1, float q1, float q2,
+                        int direction, float* out, void* stream) {
+  REQ_PTR(imL && imR && in && out);
+  REQ_HW(H, W);
+  CBMV_REQUIRE(D > 0 && D <= 1024, CBMV_ERANGE, "D=%d not in 1..1024", D);
+  CBMV_REQUIRE(in != out, CBMV_EINVAL, "sgm: in and out must differ");
+  SgmParams sp{pi1, pi2, tau_so, alpha1, q1, q2, direction};
+  for (int dir = 0; dir < 4; dir++) {
+    int rc = launch_sgm_direction(dir, imL, imR, in, H, W, D, sp, 1, 1.0f, out, as_stream(stream));
+    if (rc) return rc;
+  }
+  return CBMV_OK;
+}
+
+extern "C" int cbmv_cbca(const float* crossL, const float* crossR, const float* in, int64_t H,
+                         int64_t W, int D, int layout, int direction, float* out, void* stream) {
+  REQ_PTR(crossL && crossR && in && out);
+  REQ_HW(H, W);
+  CBMV_REQUIRE(D > 0, CBMV_EINVAL, "bad D");
+  CBMV_REQUIRE(in != out, CBMV_EINVAL, "cbca: in and out must differ");
+  CBMV_REQUIRE(direction == 1 || direction == -1, CBMV_EINVAL, "direction must be +-1");
+  CBMV_REQUIRE(layout == CBMV_HWD || layout == CBMV_DHW, CBMV_EINVAL, "bad layout");
+  return launch_cbca(crossL, crossR, in, H, W, D, layout, direction, out, as_stream(stream));
+}
+
+extern "C" int cbmv_wta(const float* cost, int64_t H, int64_t W, int D, int layout, float* disp,
+                        void* stream) {
+  REQ_PTR(cost && disp);
+  REQ_HW(H, W);
+  CBMV_REQUIRE(D > 0, CBMV_EINVAL, "bad D");
+  if (layout == CBMV_HWD) return launch_wta_subpixel(cost, H, W, D, disp, nullptr, as_stream(stream));
+  wta_dhw_kernel<<<grid_for(H * W, kBlock), kBlock, 0, as_stream(stream)>>>(cost, H * W, D, disp);
+  return check_launch("wta");
+}
+
+extern "C" int cbmv_subpixel(const float* disp, const float* cost, int64_t H, int64_t W, int D,
+                             int layout, float* out, void* stream) {
+  REQ_PTR(disp && cost && out);
+  REQ_HW(H, W);
+  CBMV_REQUIRE(D > 0, CBMV_EINVAL, "bad D");
+  subpixel_kernel<<<grid_for(H * W, kBlock), kBlock, 0, as_stream(stream)>>>(disp, cost, H, W, D, layout,
+                                                                            out);
+  return check_launch("subpixel");
+}
+
+extern "C" int cbmv_median2d(const float* in, int64_t H, int64_t W, int k, float* out,
+                             void* stream) {
+  REQ_PTR(in && out);
+  REQ_HW(H, W);
+  CBMV_REQUIRE(k >= 1 && k <= 11 && (k & 1), CBMV_EINVAL, "median window %d must be odd <= 11", k);
+  CBMV_REQUIRE(in != out, CBMV_EINVAL, "median2d: in and out must differ");
+  return launch_median(in, H, W, k, out, as_stream(stream));
+}
+
+extern "C" int cbmv_mean2d(const float* in, int64_t H, int64_t W, const float* kernel, int ks,
+                           float alpha2, float* out, void* stream) {
+  REQ_PTR(in && out && kernel);
+  REQ_HW(H, W);
+  CBMV_REQUIRE(ks >= 1 && ks <= 31 && (ks & 1), CBMV_EINVAL, "kernel size %d must be odd <= 31", ks);
+  CBMV_REQUIRE(in != out, CBMV_EINVAL, "mean2d: in and out must differ");
+  return launch_mean2d(in, H, W, kernel, ks, alpha2, out, as_stream(stream));
+}
+
+extern "C" int cbmv_outlier_detection(const float* d0, const float* d1, int64_t H, int64_t W,
+                                      int disp_max, float* out, void* stream) {
+  REQ_PTR(d0 && d1 && out);
+  REQ_HW(H, W);
+  return launch_outlier(d0, d1, H, W, disp_max, out, as_stream(stream));
+}
+
+extern "C" int cbmv_interpolate_mismatch(const float* d0, const float* outlier, int64_t H,
+                                         int64_t W, float* out, void* stream) {
+  REQ_PTR(d0 && outlier && out);
+  REQ_HW(H, W);
+  CBMV_REQUIRE(d0 != out, CBMV_EINVAL, "in and out must differ");
+  return launch_mismatch(d0, outlier, H, W, out, as_stream(stream));
+}
+
+extern "C" int cbmv_interpolate_occlusion(const float* d0, const float* outlier, int64_t H,
+                                          int64_t W, float* out, void* stream) {
+  REQ_PTR(d0 && outlier && out);
+  REQ_HW(H, W);
+  CBMV_REQUIRE(d0 != out, CBMV_EINVAL, "in and out must differ");
+  return launch_occlusion(d0, outlier, H, W, out, as_stream(stream));
+}
+
+extern "C" int cbmv_transpose_f32(const float* in, int64_t H, int64_t W, int64_t D, int to_layout,
+                                  float* out, void* stream) {
+  REQ_PTR(in && out);
+  CBMV_REQUIRE(H > 0 && W > 0 && D > 0 && in != out, CBMV_EINVAL, "bad argument");
+  const int64_t rows = to_layout == CBMV_DHW ? H * W : D;
+  const int64_t cols = to_layout == CBMV_DHW ? D : H * W;
+  CBMV_REQUIRE((rows + 31) / 32 <= 65535, CBMV_ERANGE, "volume too large for the transpose grid");
+  dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
+  transpose_kernel<<<grid, dim3(32, 8), 0, as_stream(stream)>>>(in, rows, cols, out);
+  return check_launch("transpose");
+}
+
+extern "C" int cbmv_scale_f32(float* a, int64_t n, float mul, void* stream) {
+  REQ_PTR(a);
+  CBMV_REQUIRE(n >= 0, CBMV_EINVAL, "bad size");
+  if (n == 0) return CBMV_OK;
+  scale_kernel<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(a, n, mul);
+  return check_launch("scale");
+}
+
+extern "C" int cbmv_f64_to_f32(const double* in, int64_t n, float* out, void* stream) {
+  REQ_PTR(in && out);
+  if (n <= 0) return n == 0 ? CBMV_OK : set_error(CBMV_EINVAL, "bad size");
+  f64_to_f32_kernel<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(in, n, out);
+  return check_launch("f64_to_f32");
+}
+
+extern "C" int cbmv_f32_to_f64(const float* in, int64_t n, double* out, void* stream) {
+  REQ_PTR(in && out);
+  if (n <= 0) return n == 0 ? CBMV_OK : set_error(CBMV_EINVAL, "bad size");
+  f32_to_f64_kernel<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(in, n, out);
+  return check_launch("f32_to_f64");
+}

@@ -1,0 +1,34 @@
+// Launch helpers of the cost-optimisation kernels (post.cu), shared with the
+// fused pipeline.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cbmv {
+
+struct SgmParams {
+  float pi1, pi2, tau_so, alpha1, q1, q2;
+  int direction;
+};
+
+int launch_cross(const float* img, int64_t H, int64_t W, int L1, float tau1, float* out,
+                 cudaStream_t st);
+int launch_sgm_direction(int dir, const float* x0, const float* x1, const float* in, int64_t H,
+                         int64_t W, int D, const SgmParams& sp, int mode, float scale, float* out,
+                         cudaStream_t st);
+int launch_cbca(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
+                int layout, int direction, float* out, cudaStream_t st);
+int launch_wta_subpixel(const float* cost, int64_t H, int64_t W, int D, float* disp_int,
+                        float* disp, cudaStream_t st);
+int launch_median(const float* in, int64_t H, int64_t W, int k, float* out, cudaStream_t st);
+int launch_mean2d(const float* in, int64_t H, int64_t W, const float* kernel, int ks, float alpha2,
+                  float* out, cudaStream_t st);
+int launch_normalise(const uint8_t* img, int64_t n, double* mom, float* out, cudaStream_t st);
+int launch_outlier(const float* d0, const float* d1, int64_t H, int64_t W, int disp_max, float* out,
+                   cudaStream_t st);
+int launch_mismatch(const float* d0, const float* o, int64_t H, int64_t W, float* out,
+                    cudaStream_t st);
+int launch_occlusion(const float* d0, const float* o, int64_t H, int64_t W, float* out,
+                     cudaStream_t st);
+
+}  // namespace cbmv

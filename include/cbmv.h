@@ -1,0 +1,255 @@
+/*
+ * cbmv.h -- C ABI of libcbmv, the B200 (sm_100a) implementation of CBMV's
+ * cost-volume path: matchers, feature extraction, random-forest classifier
+ * and the MC-CNN cost optimisation ("post").
+ *
+ * The reference exposes this path as three boost.python modules imported by
+ * its Python drivers (test.py:30-35, train.py:25-28):
+ *   libmatchers    cpp/matchers/matchers.cpp:568-582
+ *   libfeatextract cpp/featextract/featextract.cpp:519-540
+ *   post           cpp/post/post.cu:905-933
+ * plus scikit-learn's RandomForestClassifier.predict_proba (test.py:620).
+ * Each entry point below names the reference function it replaces.  The
+ * Python package cbmv_b200 binds these with ctypes under the reference's own
+ * module and function names (cbmv_b200.libmatchers, .libfeatextract, .post).
+ *
+ * Conventions
+ *  - Every pointer argument is DEVICE memory unless the comment says
+ *    otherwise; the caller owns it.  Every call is asynchronous on `stream`
+ *    (a cudaStream_t; NULL = the legacy default stream).
+ *  - Every function returns 0 on success or a negative CBMV_E* code; the
+ *    message of the last failure on the calling thread is cbmv_last_error().
+ *    Invalid arguments are rejected on the host before anything is launched.
+ *  - Volumes are dense and row-major.  CBMV_HWD = [H,W,D] (d fastest, the
+ *    reference's census layout and the pipeline's internal layout);
+ *    CBMV_DHW = [D,H,W] (the reference's nccNister/sadsob/zsad layout).
+ *  - Invalid (border) cost entries hold the reference's sentinel RAND_MAX =
+ *    2147483647 (2147483648.0f when stored as float32).
+ *  - Sizes are int64; H*W*D may exceed 2^31.
+ */
+#ifndef CBMV_H_
+#define CBMV_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum cbmv_status {
+  CBMV_OK = 0,
+  CBMV_EINVAL = -1,  /* bad argument (null pointer, size, window, dtype ...) */
+  CBMV_ECUDA = -2,   /* a CUDA runtime call failed                          */
+  CBMV_ENOMEM = -3,  /* device allocation failed                            */
+  CBMV_ERANGE = -4,  /* size beyond a documented limit                      */
+  CBMV_ESTATE = -5   /* object used in the wrong state                       */
+};
+
+enum cbmv_dtype { CBMV_F32 = 0, CBMV_F64 = 1 };
+enum cbmv_layout { CBMV_HWD = 0, CBMV_DHW = 1 };
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* cbmv_last_error(void);
+/* Library version, e.g. "cbmv-b200 0.1". */
+const char* cbmv_version(void);
+/* Waits for all work on `stream`. */
+int cbmv_sync(void* stream);
+
+/* ------------------------------------------------------------------ */
+/* matchers -- libmatchers                                            */
+/* ------------------------------------------------------------------ */
+
+/* census (matchers.cpp:209-350): 121-bit (wsize^2) census descriptors,
+ * Hamming cost for d <= column index of the window.  L, R: uint8 [H,W].
+ * out: [H,W,D] or [D,H,W] of float32/float64.  wsize odd, wsize^2 <= 128. */
+int cbmv_census(const uint8_t* L, const uint8_t* R, int64_t H, int64_t W, int D, int wsize,
+                void* out, int dtype, int layout, void* stream);
+
+/* nccNister (matchers.cpp:24-205): normalised cross-correlation cost
+ * -(w^2 S - A_L A_R) C_L C_R, 1 on flat windows.  wsize odd, <= 15. */
+int cbmv_ncc(const uint8_t* L, const uint8_t* R, int64_t H, int64_t W, int D, int wsize,
+             void* out, int dtype, int layout, void* stream);
+
+/* sobel (matchers.cpp:515-555): horizontal Sobel response written at
+ * (i+1, j+1) for i < H-3, j < W-3, zero elsewhere.  out [H,W] f32/f64. */
+int cbmv_sobel(const uint8_t* img, int64_t H, int64_t W, void* out, int dtype, void* stream);
+
+/* sadsob (matchers.cpp:353-436): box sum of |SL - SR(j-d)| over Sobel
+ * responses SL, SR ([H,W], dtype sob_dtype, integer-valued).  wsize odd <= 15. */
+int cbmv_sadsob(const void* SL, const void* SR, int sob_dtype, int64_t H, int64_t W, int D,
+                int wsize, void* out, int dtype, int layout, void* stream);
+
+/* zsad (matchers.cpp:440-512): zero-mean SAD.  wsize odd <= 15. */
+int cbmv_zsad(const uint8_t* L, const uint8_t* R, int64_t H, int64_t W, int D, int wsize,
+              void* out, int dtype, int layout, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* feature extraction -- libfeatextract (float64 volumes, as the      */
+/* reference's)                                                       */
+/* ------------------------------------------------------------------ */
+
+/* swap_axes (featextract.cpp:24-53): [D,H,W] -> [H,W,D]. */
+int cbmv_swap_axes(const double* in, int64_t D, int64_t H, int64_t W, double* out, void* stream);
+/* swap_axes_back (featextract.cpp:55-83): [H,W,D] -> [D,H,W]. */
+int cbmv_swap_axes_back(const double* in, int64_t H, int64_t W, int64_t D, double* out,
+                        void* stream);
+/* get_cost (featextract.cpp:85-113): [H,W,D,K] -> [H,W,D], k = 0. */
+int cbmv_get_cost(const double* in, int64_t H, int64_t W, int64_t D, int64_t K, double* out,
+                  void* stream);
+/* get_right_cost (featextract.cpp:115-152): R[i,j,d] = C[i,j+d,d], else C[0,0,0]. */
+int cbmv_get_right_cost(const double* C, int64_t H, int64_t W, int64_t D, double* out,
+                        void* stream);
+/* get_left_cost (featextract.cpp:452-488): L[i,j,d] = R[i,j-d,d], else R[0,0,0]. */
+int cbmv_get_left_cost(const double* Rv, int64_t H, int64_t W, int64_t D, double* out,
+                       void* stream);
+/* extract_ratio, test form (featextract.cpp:303-342): rows of [N,D]. */
+int cbmv_extract_ratio(const double* vol, int64_t N, int64_t D, double e, double* out,
+                       void* stream);
+/* extract_likelihood, test form (featextract.cpp:402-450). */
+int cbmv_extract_likelihood(const double* vol, int64_t N, int64_t D, double sigma, double* out,
+                            void* stream);
+/* extract_ratio, training form (featextract.cpp:254-300): samples int32 [N,3]; out [3N]. */
+int cbmv_extract_ratio_samples(const double* vol, int64_t N, int64_t D, const int32_t* samples,
+                               double e, double* out, void* stream);
+/* extract_likelihood, training form (featextract.cpp:345-399). */
+int cbmv_extract_likelihood_samples(const double* vol, int64_t N, int64_t D,
+                                    const int32_t* samples, double sigma, double* out,
+                                    void* stream);
+/* get_samples (featextract.cpp:217-252). */
+int cbmv_get_samples(const double* vol, int64_t N, int64_t D, const int32_t* samples,
+                     double* out, void* stream);
+/* generate_labels (featextract.cpp:490-516): [1,0,0] per sample; out int32 [3N]. */
+int cbmv_generate_labels(int64_t N, int32_t* out, void* stream);
+/* generate_d_indices (featextract.cpp:154-215): one positive (gt) and two
+ * negatives per sample drawn |d - gt| > thr from a counter-based generator
+ * keyed by `seed` (the reference's rand() under OpenMP is not reproducible).
+ * gt int32 [N] with 0 <= gt <= maxd; out int32 [N,3].  CBMV_EINVAL when a
+ * sample's range is empty (where the reference divides by zero). */
+int cbmv_generate_d_indices(const int32_t* gt, int64_t N, int maxd, int thr, uint64_t seed,
+                            int32_t* out, void* stream);
+
+/* Fused features (test.py:521-595, Testing.__extract_features_lr): the 20
+ * CBMV features per (pixel, d) from the four [H,W,D] float64 cost volumes
+ * (census, ncc, sadsob, zsad, in that order), column order as the reference:
+ * 0-3 costs, 4-7 ratio, 8-11 likelihood, 12-15 right-reference ratio warped
+ * to the left view, 16-19 the same for likelihood.  Computed in float64 as
+ * the reference and stored as float32 (what the random forest reads).
+ * out float32 [H*W*D, 20]. */
+int cbmv_features(const double* census, const double* ncc, const double* sob, const double* sad,
+                  int64_t H, int64_t W, int D, float* out, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* random forest -- sklearn RandomForestClassifier.predict_proba      */
+/* ------------------------------------------------------------------ */
+
+typedef struct cbmv_forest cbmv_forest;
+
+/* Uploads a packed forest (HOST pointers; layout in cbmv_b200/forest.py):
+ * nodes uint32 [n_nodes,2] = {float32 threshold bits, word}, leaf_value
+ * float64 [n_leaves,2] (class-0 and class-1 fractions), tree_offsets int32
+ * [n_trees+1].  Replaces unpickling the sklearn model (test.py:603-604). */
+int cbmv_forest_create(const uint32_t* nodes, int64_t n_nodes, const double* leaf_value,
+                       int64_t n_leaves, const int32_t* tree_offsets, int n_trees,
+                       int n_features, cbmv_forest** out);
+/* Device pointers of an uploaded forest (for fused kernels and tests). */
+int cbmv_forest_info(const cbmv_forest* f, int* n_trees, int64_t* n_nodes, int64_t* n_leaves);
+int cbmv_forest_destroy(cbmv_forest* f);
+
+/* predict_proba (sklearn/ensemble/_forest.py ForestClassifier.predict_proba,
+ * called at test.py:620): X float32 [N,F]; proba float64 [N,2] (may be
+ * NULL): column k = sum over trees, in tree order, of the leaf's class-k
+ * fraction, / n_trees.  leaves int32 [N,n_trees] (may be NULL): the leaf
+ * reached in each tree as its tree-local index in the packed breadth-first
+ * numbering (FlatForest.pack returns the map back to sklearn's node ids). */
+int cbmv_forest_predict(const cbmv_forest* f, const float* X, int64_t N, double* proba,
+                        int32_t* leaves, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* cost optimisation -- post (post.cu), float32 on the device          */
+/* ------------------------------------------------------------------ */
+
+/* cross (post.cu:336-396): out float32 [4,H,W] arm end coordinates. */
+int cbmv_cross(const float* img, int64_t H, int64_t W, int L1, float tau1, float* out,
+               void* stream);
+/* sgm_w (post.cu:263-333): out += sum over the 4 scan directions of the
+ * path costs of `in` ([H,W,D] float32).  `out` is NOT cleared (the reference
+ * zeroes it first, test.py:379).  D <= 1024. */
+int cbmv_sgm(const float* imL, const float* imR, const float* in, int64_t H, int64_t W, int D,
+             float pi1, float pi2, float tau_so, float alpha1, float q1, float q2, int direction,
+             float* out, void* stream);
+/* cbca (post.cu:399-450) on a volume of layout `layout`; in != out. */
+int cbmv_cbca(const float* crossL, const float* crossR, const float* in, int64_t H, int64_t W,
+              int D, int layout, int direction, float* out, void* stream);
+/* np.argmin over d (test.py:408-409), first minimum; disp float32 [H,W]. */
+int cbmv_wta(const float* cost, int64_t H, int64_t W, int D, int layout, float* disp,
+             void* stream);
+/* subpixel_enchancement (post.cu:453-483). */
+int cbmv_subpixel(const float* disp, const float* cost, int64_t H, int64_t W, int D, int layout,
+                  float* out, void* stream);
+/* median2d (post.cu:486-518), k odd <= 11. */
+int cbmv_median2d(const float* in, int64_t H, int64_t W, int k, float* out, void* stream);
+/* mean2d (post.cu:520-566): kernel float32 [ks,ks] in DEVICE memory, ks odd <= 31. */
+int cbmv_mean2d(const float* in, int64_t H, int64_t W, const float* kernel, int ks, float alpha2,
+                float* out, void* stream);
+/* outlier_detection (post.cu:717-754). */
+int cbmv_outlier_detection(const float* d0, const float* d1, int64_t H, int64_t W, int disp_max,
+                           float* out, void* stream);
+/* interpolate_mismatch (post.cu:757-827). */
+int cbmv_interpolate_mismatch(const float* d0, const float* outlier, int64_t H, int64_t W,
+                              float* out, void* stream);
+/* interpolate_occlusion (post.cu:829-869). */
+int cbmv_interpolate_occlusion(const float* d0, const float* outlier, int64_t H, int64_t W,
+                               float* out, void* stream);
+/* Volume helpers replacing post.swap_axis / swap_axis_back / CUDA_divide_double
+ * (post.cu:569-684) on float32 volumes. */
+int cbmv_transpose_f32(const float* in, int64_t H, int64_t W, int64_t D, int to_layout,
+                       float* out, void* stream);
+int cbmv_scale_f32(float* a, int64_t n, float mul, void* stream);
+/* float64 <-> float32 conversion of n elements. */
+int cbmv_f64_to_f32(const double* in, int64_t n, float* out, void* stream);
+int cbmv_f32_to_f64(const float* in, int64_t n, double* out, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* end-to-end pipeline                                                 */
+/* ------------------------------------------------------------------ */
+
+/* Parameters of Testing.__init__ (test.py:44-73) and the feature constants
+ * (test.py:71-73, 548-551); cbmv_params_default fills the reference's
+ * defaults. */
+typedef struct cbmv_params {
+  int censw, nccw, sadw, sobw;
+  float pi1, pi2, sgm_q1, sgm_q2, alpha1, tau_so;
+  int sgm_i;
+  int L1;
+  float tau1;
+  int cbca_i1, cbca_i2, median_i, median_w;
+  float blur_sigma, blur_t;
+  int direction;
+} cbmv_params;
+void cbmv_params_default(cbmv_params* p);
+
+typedef struct cbmv_ctx cbmv_ctx;
+
+/* A context owns the device workspaces of one pair shape and one stream;
+ * it grows them on demand.  Not thread-safe: one context per host thread. */
+int cbmv_ctx_create(void* stream, cbmv_ctx** out);
+int cbmv_ctx_destroy(cbmv_ctx* c);
+
+/* The reference's test path for one rectified pair (main.py:53-70 with
+ * interpolate=False): matchers -> features -> random forest -> P(class 0)
+ * -> post (_mem chain, test.py:341-449) -> disparity.  L, R uint8 [H,W],
+ * disp float32 [H,W], all device memory.  prob0 (optional, may be NULL)
+ * receives the float32 [H,W,D] matching-cost volume P(class 0). */
+int cbmv_run_rf(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params* p, const uint8_t* L,
+                const uint8_t* R, int64_t H, int64_t W, int D, float* disp, float* prob0);
+
+/* Stage timings of the last cbmv_run_* call in milliseconds (CUDA events):
+ * [0] matchers, [1] feature statistics, [2] features+classifier, [3] post,
+ * [4] total.  Valid after the stream has been synchronised. */
+int cbmv_ctx_timings(cbmv_ctx* c, float* ms5);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CBMV_H_ */

@@ -1,0 +1,70 @@
+"""The fused pipeline (images -> disparity on the device) against the
+reference's test path restated over the oracle (matchers, features, random
+forest, eval_prob with the _mem post-processing)."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_forest(oracle_cpu):
+    from sklearn.ensemble import RandomForestClassifier
+    from oracle import glue
+    from cbmv_b200 import synth
+    from cbmv_b200.forest import FlatForest
+    S = []
+    for seed in (31, 32):
+        L, R, gt, _ = synth.make_pair(seed=seed, width=120, height=72, ndisp=24, planes=5, dmin=2, dmax=20)
+        S.append(glue.create_samples_mem(oracle_cpu.mtc, oracle_cpu.fte, L, R, gt, 24,
+                                         lambda g, nd: oracle_cpu.fte.generate_d_indices(g, nd, 1, seed=seed)))
+    S = np.concatenate(S).astype(np.float32)
+    rf = RandomForestClassifier(n_estimators=10, min_samples_leaf=50, max_depth=20, random_state=0,
+                                n_jobs=4).fit(S[:, :20], S[:, 20])
+    return FlatForest.from_sklearn(rf)
+
+
+@pytest.fixture(scope="module")
+def forest(oracle_cpu):
+    return _small_forest(oracle_cpu)
+
+
+def test_pipeline_matches_reference_path(gpu, oracle_cpu, small_pair, forest):
+    from oracle import glue
+    from cbmv_b200.forest_gpu import GpuForest
+    from cbmv_b200.pipeline import StereoPipeline
+    L, R, gt, nonocc = small_pair
+    D = 24
+    H, W = L.shape
+    # reference path, restated over the oracle
+    proba = glue.test_model(oracle_cpu.mtc, oracle_cpu.fte,
+                            lambda X: np.stack([oracle_cpu.rf_predict(forest, X),
+                                                1 - oracle_cpu.rf_predict(forest, X)], 1), L, R, D)
+    p0_ref = proba[:, 0].reshape(H, W, D)
+    disp_ref = glue.eval_prob(oracle_cpu.post, oracle_cpu.fte, proba, L, R, D)
+    # fused GPU path
+    gf = GpuForest(forest)
+    pipe = StereoPipeline(gf)
+    prob = torch.empty((H, W, D), device="cuda")
+    disp = pipe.run_rf(L, R, D, prob_out=prob)
+    torch.cuda.synchronize()
+    p0 = prob.cpu().numpy()
+    # identical features -> identical leaves -> P0 equal to float32 rounding
+    same = np.mean(p0 == p0_ref.astype(np.float32))
+    assert same > 0.9999, same
+    close = np.mean(np.abs(disp - disp_ref) <= 0.5)
+    assert close >= 0.995, close
+    t = pipe.timings()
+    assert t["total"] > 0
+
+
+def test_pipeline_repeatable_and_device_io(gpu, small_pair, forest):
+    from cbmv_b200.forest_gpu import GpuForest
+    from cbmv_b200.pipeline import StereoPipeline
+    L, R, _, _ = small_pair
+    pipe = StereoPipeline(GpuForest(forest))
+    a = pipe.run_rf(L, R, 24)
+    l, r = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
+    b = pipe.run_rf(l, r, 24)
+    assert isinstance(b, torch.Tensor) and b.is_cuda
+    assert np.array_equal(a, b.cpu().numpy())  # deterministic
