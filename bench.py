@@ -1,0 +1,355 @@
+"""Benchmark: pixel·disparities per second of the CBMV test path on B200.
+
+Workload: one synthetic rectified pair at 694x554, D=128 (seeded, the
+reference's README-scale Middlebury size), 49,212,928 (pixel, d) units.  A
+step is the whole test path for that pair: four matchers, 20 features,
+random forest (50 trees, depth <= 20, trained on 30 seeded pairs, see
+tests/golden/make_forest.py), then the MC-CNN `_mem` post-processing to the
+disparity map.  With N GPUs (torchrun), every rank processes its own pair
+(seed = rank): weak scaling by independent pairs, no collective on the data
+path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cbmv|reference]
+
+`value` is device time with the images resident in HBM and L2 flushed
+between steps; `e2e` is the same metric through the public call with pinned
+host buffers (H2D of both images and D2H of the disparity inside the timed
+region).  `--impl reference` times the reference's own implementation of the
+path: its C++ matchers and feature extraction compiled unmodified
+(oracle/_ref), scikit-learn's predict_proba on the same forest, and its
+post.cu on the GPU (as shipped; the CPU restatement when that build is
+absent).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FOREST = os.path.join(ROOT, "tests", "golden", "forest_694x554.npz")
+W0, H0, D0 = 694, 554, 128
+UNITS = W0 * H0 * D0
+METRIC = "pixel·disparities/s end-to-end at 694×554, D=128 (RF classifier)"
+BYTES_PER_UNIT_FUSED = 4.0  # algorithmic HBM bytes of matchers+features+classifier per (p,d)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                self.out, _ = self.p.communicate()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def reduce_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    import torch
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def run_cbmv(a, ws, rank, local):
+    import torch
+    from cbmv_b200 import synth
+    from cbmv_b200.forest import FlatForest
+    from cbmv_b200.forest_gpu import GpuForest
+    from cbmv_b200.pipeline import StereoPipeline
+
+    if not os.path.exists(a.forest):
+        raise SystemExit("forest fixture missing: run `python tests/golden/make_forest.py` (%s)" % a.forest)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    L, R, gt, nonocc = synth.pair_694x554(seed=rank)
+    if a.height != H0:
+        L, R, gt, nonocc = (v[:a.height].copy() for v in (L, R, gt, nonocc))
+    units = L.shape[0] * W0 * D0
+    flat = FlatForest.load(a.forest)
+    gf = GpuForest(flat)
+    pipe = StereoPipeline(gf)
+    l = torch.from_numpy(L).to(dev)
+    r = torch.from_numpy(R).to(dev)
+    disp = torch.empty(L.shape, dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > L2
+    st = torch.cuda.current_stream()
+
+    for _ in range(a.warmup):
+        pipe.run_rf(l, r, D0, disp_out=disp)
+    barrier(ws)
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    stage = {"matchers": 0.0, "stats": 0.0, "classify": 0.0, "post": 0.0, "total": 0.0}
+    with Clocks(local) as clk:
+        for k in range(a.steps):
+            flush.fill_(float(k))
+            ev0[k].record(st)
+            pipe.run_rf(l, r, D0, disp_out=disp)
+            ev1[k].record(st)
+            st.synchronize()
+            for kk, v in pipe.timings().items():
+                stage[kk] += v
+        barrier(ws)
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1)) / a.steps
+    ms = reduce_max(ms, ws)
+    stage = {k: v / a.steps for k, v in stage.items()}
+    value = units * ws / (ms / 1e3)
+    # kernel launches per step (pipeline.cu): 8 per-pixel terms, 4 cost volumes,
+    # 4 feature statistics, 1 features+forest, post: 4 normalisation, 2 cross,
+    # 4 x sgm_i SGM directions, cbca_i2 CBCA, WTA+subpixel, median, mean2d
+    launches = 8 + 4 + 4 + 1 + 4 + 2 + 4 * 2 + 4 + 3
+
+    # end to end through the public call with pinned host buffers
+    Lh = torch.from_numpy(L).pin_memory()
+    Rh = torch.from_numpy(R).pin_memory()
+    for _ in range(2):
+        pipe.run_rf(Lh, Rh, D0)
+    barrier(ws)
+    e2e_ms = 0.0
+    for k in range(a.steps):
+        flush.fill_(float(k))
+        st.synchronize()
+        t0 = time.perf_counter()
+        out = pipe.run_rf(Lh, Rh, D0)  # H2D of both images, the whole path, D2H of the map
+        e2e_ms += (time.perf_counter() - t0) * 1e3
+        assert out.shape == L.shape
+    e2e_ms = reduce_max(e2e_ms / a.steps, ws)
+
+    # accuracy of this pair (bad-2.0 on non-occluded pixels)
+    d = disp.cpu().numpy()
+    bad2 = float(np.mean(np.abs(d[nonocc] - gt[nonocc]) > 2.0))
+
+    peak, peak_kind = peaks()
+    t_cls = stage["classify"]
+    achieved = BYTES_PER_UNIT_FUSED * units / (t_cls / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get("features_rf_kernel")
+    line = {
+        "metric": METRIC, "value": value, "unit": "pixel·disparities/s", "n_gpus": ws,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32",
+        "data": "synthetic (seeded 694x554 pair per rank; L2 flushed between steps)",
+        "config": {"workload": "694x554 D=128 test path: 4 matchers, 20 features, RF 50 trees "
+                               "depth<=20, MC-CNN _mem post", "width": W0, "height": int(L.shape[0]), "ndisp": D0,
+                   "units_per_pair": units, "classifier": "random_forest",
+                   "forest_nodes": int(flat.n_nodes), "l2": "flushed (256 MB write) between steps",
+                   "parallelism": "replica per GPU, one pair per rank"},
+        "stage_ms": stage,
+        "bad2_nonocc": bad2,
+        "gpu_launches": launches * a.steps,
+        "e2e": {"value": units * ws / (e2e_ms / 1e3), "unit": "pixel·disparities/s",
+                "ms_per_step": e2e_ms, "h2d_bytes_per_step": 2 * L.size,
+                "d2h_bytes_per_step": 4 * L.size},
+        "roofline": {"bound": "hbm", "kernel": "features_rf_kernel", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_kind": peak_kind, "bytes_per_unit": BYTES_PER_UNIT_FUSED,
+                     "note": "dominant kernel is the forest walk, bound by node-visit gathers, "
+                             "not HBM"},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(flat, L, R, a)
+    return line
+
+
+def _cpu_stage_band(ref, skl, L, R, rows, cores):
+    """The reference's CPU stages (test.py:122-138, 521-595, 597-626) on the
+    first `rows` image rows: the matchers run on a band with a 10-row margin
+    (every matcher is row-local within +-5 rows, so the kept rows equal the
+    full-image ones), then the feature assembly and predict_proba on those
+    rows.  Returns seconds."""
+    from oracle import glue
+    ref.set_threads(cores)
+    band_l, band_r = L[:rows + 10], R[:rows + 10]
+    t0 = time.perf_counter()
+    glue.test_model(ref.mtc, ref.fte, skl.predict_proba, band_l, band_r, D0, rows=rows)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(flat, L, R, a):
+    """The reference's own CPU stages, timed on this host (bounded sample)."""
+    from oracle import ref, skforest
+    cores = len(os.sched_getaffinity(0))
+    if not ref.cpu_available():
+        return {"value": None, "unit": "pixel·disparities/s", "cores": cores, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    skl = skforest.to_sklearn(flat, n_jobs=cores)
+    rows = a.cpu_rows
+    _cpu_stage_band(ref, skl, L, R, 8, cores)  # warm-up (thread pools, page-in)
+    t = _cpu_stage_band(ref, skl, L, R, rows, cores)
+    units = rows * W0 * D0
+    return {"value": units / t, "unit": "pixel·disparities/s", "cores": cores, "kind": "reference",
+            "sample": "first %d rows of the 694x554 D=128 pair: reference matchers (on a %d-row band) + "
+                      "feature assembly + sklearn predict_proba (n_jobs=%d); post excluded (the "
+                      "reference runs it on the GPU); %.1f s" % (rows, rows + 10, cores, t)}
+
+
+def run_reference(a, ws, rank, local):
+    """--impl reference: the reference's implementation of the path."""
+    if rank != 0:
+        return None
+    import torch
+    from cbmv_b200 import synth
+    from cbmv_b200.forest import FlatForest
+    from oracle import cpu, glue, ref, skforest
+
+    cores = len(os.sched_getaffinity(0))
+    if not ref.cpu_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref (the reference compiled from its sources) "
+                                                  "is not built"}
+    if not os.path.exists(a.forest):
+        return {"impl": "reference", "unavailable": "forest fixture missing (tests/golden/make_forest.py)"}
+    flat = FlatForest.load(a.forest)
+    skl = skforest.to_sklearn(flat, n_jobs=cores)
+    L, R, gt, nonocc = synth.pair_694x554(seed=0)
+    post_kind = "reference post.cu on the GPU (as shipped)" if ref.post_available() and \
+        torch.cuda.is_available() else "oracle CPU restatement of post.cu"
+    post_mod = ref.post if "post.cu" in post_kind else cpu.post
+    rows = a.cpu_rows
+    rng = np.random.default_rng(0)
+    prob_full = rng.random((H0, W0, D0, 2))  # the post stage's input: a [H,W,D] cost volume
+    prob_full = prob_full.reshape(-1, 2)
+    times = []
+    for k in range(a.warmup + a.steps):
+        t_cpu = _cpu_stage_band(ref, skl, L, R, rows, cores)
+        t0 = time.perf_counter()
+        glue.eval_prob(post_mod, ref.fte, prob_full, L, R, D0)
+        if post_mod is ref.post:
+            ref.post.sync()
+        t_post = time.perf_counter() - t0
+        if k >= a.warmup:
+            times.append((t_cpu, t_post))
+    t_cpu = float(np.mean([t for t, _ in times]))
+    t_post = float(np.mean([t for _, t in times]))
+    t_pair = t_cpu * (H0 / rows) + t_post  # a whole pair: CPU stages scaled from the band
+    value = UNITS / t_pair
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "pixel·disparities/s",
+        "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_pair * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded 694x554 pair)",
+        "config": {"workload": "694x554 D=128 test path: 4 matchers, 20 features, RF 50 trees "
+                               "depth<=20, MC-CNN _mem post", "width": W0, "height": H0, "ndisp": D0},
+        "cpu_baseline": {"value": value, "unit": "pixel·disparities/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": "per step: reference CPU stages (matchers, feature assembly, sklearn "
+                                   "predict_proba) on the first %d rows, scaled to the %d rows of the "
+                                   "pair (%.2f s -> %.2f s), plus the full-pair post (%s, %.2f s incl. "
+                                   "its host copies and host argmin)"
+                                   % (rows, H0, t_cpu, t_cpu * H0 / rows, post_kind, t_post)},
+        "e2e": {"value": value, "unit": "pixel·disparities/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["cbmv", "reference"], default="cbmv")
+    ap.add_argument("--forest", default=FOREST)
+    ap.add_argument("--cpu-rows", type=int, default=48)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--height", type=int, default=H0,
+                    help="rows of the pair (smaller cases for profiler captures; default 554)")
+    a = ap.parse_args()
+    ws, rank, local = dist_init()
+    if a.impl == "reference":
+        if a.steps > 3:  # each reference step is seconds of CPU work; keep the run within minutes
+            a.steps = 3
+        a.warmup = min(a.warmup, 1)
+        line = run_reference(a, ws, rank, local)
+    else:
+        line = run_cbmv(a, ws, rank, local)
+    if rank == 0 and line is not None:
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -8,7 +8,7 @@
 // freedom taken is the order of the likelihood denominator's sum over d,
 // which only moves it by an ulp of float64.
 #include "common.cuh"
-#include "rf.cuh"
+#include "features.cuh"
 
 namespace cbmv {
 namespace {
@@ -171,12 +171,6 @@ __global__ void d_indices_kernel(const int32_t* __restrict__ gt, int64_t N, int 
 }  // namespace
 
 // ------------------------------------------------------ fused features
-// Per-matcher constants of the reference's feature extraction:
-// ratio epsilon (test.py:548-551) and likelihood sigma (test.py:71-73).
-__constant__ double kEps[4] = {0.01, 1.01, 0.01, 0.01};
-__constant__ double kSigma[4] = {2.0 * 8 * 8, 0.02, 2.0 * 100 * 100, 2.0 * 100 * 100};
-static const double hSigma[4] = {2.0 * 8 * 8, 0.02, 2.0 * 100 * 100, 2.0 * 100 * 100};
-
 // Per-pixel statistics of one matcher volume for both reference views:
 // stats[((m*2 + view)*HW + p)*2 + {0,1}] = {row minimum, likelihood
 // denominator}; view 0 = left reference (row p of the volume), view 1 =
@@ -217,48 +211,6 @@ __global__ void feature_stats_kernel(const double* __restrict__ vol, int m, int6
   }
 }
 
-// ratio / likelihood of cost c against the statistics (min, den) of its row
-// (featextract.cpp:333, :440).
-__device__ __forceinline__ void confidences(double c, double mn, double den, double e, double sigma,
-                                            float* ratio, float* lik) {
-  if (mn == kRandMax) {
-    *ratio = 0.0f;
-    *lik = 0.0f;
-  } else {
-    *ratio = (float)((mn + e) / (c + e));
-    const double t = c - mn;
-    *lik = (float)(exp(-((t * t) / sigma)) / den);
-  }
-}
-
-// The 20 features of (p, d) in the reference's column order.  The right-
-// reference confidences at left (x, d) are those of right pixel x - d at
-// disparity d, whose cost is C[p, d] itself; for x < d get_left_cost fills
-// with the first element of the right-view feature volume, which is 0 (the
-// right view's pixel (row, 0) has only sentinel costs).
-__device__ __forceinline__ void features_at(const double* const* vols, const double* stats,
-                                            int64_t HW, int64_t W, int D, int64_t p, int64_t x,
-                                            int d, float* f) {
-#pragma unroll
-  for (int m = 0; m < 4; m++) {
-    const double c = vols[m][p * D + d];
-    f[m] = (float)c;
-    const double* sl = stats + ((int64_t)(m * 2 + 0) * HW + p) * 2;
-    confidences(c, sl[0], sl[1], kEps[m], kSigma[m], &f[4 + m], &f[8 + m]);
-    if (x >= d) {
-      const double* sr = stats + ((int64_t)(m * 2 + 1) * HW + (p - d)) * 2;
-      confidences(c, sr[0], sr[1], kEps[m], kSigma[m], &f[12 + m], &f[16 + m]);
-    } else {
-      f[12 + m] = 0.0f;
-      f[16 + m] = 0.0f;
-    }
-  }
-}
-
-struct FeatVols {
-  const double* v[4];
-};
-
 __global__ void features_kernel(FeatVols fv, const double* __restrict__ stats, int64_t H, int64_t W,
                                 int D, float* __restrict__ out) {
   const int64_t HW = H * W;
@@ -270,50 +222,6 @@ __global__ void features_kernel(FeatVols fv, const double* __restrict__ stats, i
 #pragma unroll
     for (int k = 0; k < 20; k++) out[t * 20 + k] = f[k];
   }
-}
-
-// Features and random forest fused: each thread builds the 20 features of
-// its (pixel, d) in a private column of shared memory (feature k of thread t
-// at [k][t], so the walk's data-dependent reads never conflict on a bank)
-// and walks every tree; the [H*W*D, 20] feature matrix never reaches HBM.
-// prob0 receives P(class 0) = the matching cost fed to the post-processing.
-__global__ void __launch_bounds__(128) features_rf_kernel(FeatVols fv,
-                                                          const double* __restrict__ stats,
-                                                          int64_t H, int64_t W, int D, RfView f,
-                                                          float* __restrict__ prob0) {
-  extern __shared__ float xs[];
-  const int64_t HW = H * W;
-  const int tid = threadIdx.x;
-  const int B = blockDim.x;
-  GRID_STRIDE(t, HW * D) {
-    const int64_t p = t / D;
-    const int d = (int)(t - p * D);
-    float fe[20];
-    features_at(fv.v, stats, HW, W, D, p, p % W, d, fe);
-#pragma unroll
-    for (int k = 0; k < 20; k++) xs[k * B + tid] = fe[k];
-    double acc = 0.0;
-    for (int tr = 0; tr < f.n_trees; tr++) {
-      uint32_t idx = (uint32_t)__ldg(f.offsets + tr);
-      uint2 node = __ldg(f.nodes + idx);
-      while (!(node.y & kLeafFlag)) {
-        const float x = xs[(node.y & 31u) * B + tid];
-        idx = ((node.y >> 5) & kChildMask) + (x <= __uint_as_float(node.x) ? 0u : 1u);
-        node = __ldg(f.nodes + idx);
-      }
-      acc += __ldg(f.leaf_value + (node.y & ~kLeafFlag)).x;
-    }
-    prob0[t] = (float)(acc / f.n_trees);
-  }
-}
-
-int launch_features_rf(const double* const* vols, const double* stats, int64_t H, int64_t W,
-                       int D, const RfView& f, float* prob0, cudaStream_t st) {
-  FeatVols fv = {{vols[0], vols[1], vols[2], vols[3]}};
-  const int block = 128;
-  features_rf_kernel<<<grid_for(H * W * D, block), block, 20 * block * sizeof(float), st>>>(
-      fv, stats, H, W, D, f, prob0);
-  return check_launch("features_rf");
 }
 
 int launch_feature_stats(const double* const* vols, int64_t H, int64_t W, int D, double* stats,

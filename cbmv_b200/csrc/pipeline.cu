@@ -227,7 +227,7 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
   float* cur = w.volA;
   float* oth = w.volB;
   for (int i = 0; i < p->cbca_i1; i++) {
-    RC(launch_cbca(w.crossL, w.crossR, cur, H, W, D, CBMV_HWD, p->direction, oth, st));
+    RC(launch_cbca(w.crossL, w.crossR, cur, H, W, D, CBMV_HWD, p->direction, oth, st, p->L1 - 1));
     float* t = cur; cur = oth; oth = t;
   }
   SgmParams sp{p->pi1, p->pi2, p->tau_so, p->alpha1, p->sgm_q1, p->sgm_q2, p->direction};
@@ -240,7 +240,7 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
     float* t = cur; cur = oth; oth = t;
   }
   for (int i = 0; i < p->cbca_i2; i++) {
-    RC(launch_cbca(w.crossL, w.crossR, cur, H, W, D, CBMV_HWD, p->direction, oth, st));
+    RC(launch_cbca(w.crossL, w.crossR, cur, H, W, D, CBMV_HWD, p->direction, oth, st, p->L1 - 1));
     float* t = cur; cur = oth; oth = t;
   }
   float* d0 = w.dtmp;
@@ -291,7 +291,7 @@ extern "C" int cbmv_run_rf(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params*
   const double* vols[4] = {w.vol[0], w.vol[1], w.vol[2], w.vol[3]};
   RC(launch_feature_stats(vols, H, W, D, w.stats, st));
   CBMV_CUDA(cudaEventRecord(c->ev[2], st));
-  RC(launch_features_rf(vols, w.stats, H, W, D, *forest_view(f), w.volA, st));
+  RC(launch_features_rf(vols, w.stats, H, W, D, f, w.volA, st));
   if (prob0)
     CBMV_CUDA(cudaMemcpyAsync(prob0, w.volA, sizeof(float) * H * W * D, cudaMemcpyDeviceToDevice, st));
   CBMV_CUDA(cudaEventRecord(c->ev[3], st));

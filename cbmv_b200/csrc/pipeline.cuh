@@ -30,6 +30,6 @@ int launch_zsad_cost(const uint8_t* L, const uint8_t* R, const double* ml, const
 int launch_feature_stats(const double* const* vols, int64_t H, int64_t W, int D, double* stats,
                          cudaStream_t st);
 int launch_features_rf(const double* const* vols, const double* stats, int64_t H, int64_t W,
-                       int D, const RfView& f, float* prob0, cudaStream_t st);
+                       int D, const cbmv_forest* forest, float* prob0, cudaStream_t st);
 
 }  // namespace cbmv

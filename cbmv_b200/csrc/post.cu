@@ -80,44 +80,61 @@ __global__ void __launch_bounds__(128) sgm_kernel(const float* __restrict__ x0,
   const float p1b = sp.pi1 / (sp.q1 * sp.q2), p2b = sp.pi2 / (sp.q1 * sp.q2);
   const float p1c = sp.pi1 / sp.q1, p2c = sp.pi2 / sp.q1;
 
-  float prev[KPL], nxt[KPL];
+  // Everything a step reads that does not depend on the recursion -- the
+  // step's costs, the output it accumulates into, and the image differences
+  // D1 (left image) and D2 (right image, per d) -- is loaded one step ahead.
+  struct Step {
+    float cost[KPL], acc[KPL], d2[KPL];
+    float d1;
+  };
   auto coords = [&](int step, int& x, int& y) {
     if (DIR == 0) { x = step; y = line; }
     else if (DIR == 1) { x = W - 1 - step; y = line; }
     else if (DIR == 2) { x = line; y = step; }
     else { x = line; y = H - 1 - step; }
   };
-  auto load = [&](int step, float* v) {
+  auto load = [&](int step, Step& s) {
     int x, y;
     coords(step, x, y);
-    const float* src = in + ((int64_t)y * W + x) * D;
+    const int64_t ind2 = (int64_t)y * W + x;
+    const float* src = in + ind2 * D;
+    const float* acc = out + ind2 * D;
+    const bool first = step == 0;  // no previous pixel: D1/D2 unused
+    const int64_t indp = first ? ind2 : ind2 - (int64_t)dy * W - dx;
+    s.d1 = first ? 0.0f : fabsf(x0[ind2] - x0[indp]);
 #pragma unroll
     for (int k = 0; k < KPL; k++) {
       const int d = lane + 32 * k;
-      v[k] = d < D ? src[d] : inf;
+      s.cost[k] = d < D ? src[d] : inf;
+      s.acc[k] = (mode != 0 && d < D) ? acc[d] : 0.0f;
+      const int xx = x + d * sp.direction;
+      // post.cu:232-237: D2 = 10 when the matching pixel or its predecessor
+      // leaves the image
+      if (first || d >= D || xx < 0 || xx >= W || xx - dx < 0 || xx - dx >= W)
+        s.d2[k] = 10.0f;
+      else
+        s.d2[k] = fabsf(x1[ind2 + d * sp.direction] - x1[indp + d * sp.direction]);
     }
   };
+  float prev[KPL];
+  Step nxt;
   load(0, nxt);
   for (int step = 0; step < nsteps; step++) {
-    float cur[KPL];
-#pragma unroll
-    for (int k = 0; k < KPL; k++) cur[k] = nxt[k];
+    const Step cur = nxt;
     if (step + 1 < nsteps) load(step + 1, nxt);
     int x, y;
     coords(step, x, y);
     float L[KPL];
     if (step == 0) {
 #pragma unroll
-      for (int k = 0; k < KPL; k++) L[k] = cur[k];
+      for (int k = 0; k < KPL; k++) L[k] = cur.cost[k];
     } else {
       float mn = prev[0];
 #pragma unroll
       for (int k = 1; k < KPL; k++) mn = fminf(mn, prev[k]);
 #pragma unroll
       for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-      const int64_t ind2 = (int64_t)y * W + x;
-      const int64_t indp = ind2 - (int64_t)dy * W - dx;
-      const float D1 = fabsf(x0[ind2] - x0[indp]);
+      const float D1 = cur.d1;
 #pragma unroll
       for (int k = 0; k < KPL; k++) {
         const int d = lane + 32 * k;
@@ -129,12 +146,7 @@ __global__ void __launch_bounds__(128) sgm_kernel(const float* __restrict__ x0,
         if (lane == 0) lo = lo_w;
         if (lane == 31) hi = hi_w;
         if (d < D) {
-          const int xx = x + d * sp.direction;
-          float D2;
-          if (xx < 0 || xx >= W || xx - dx < 0 || xx - dx >= W)
-            D2 = 10.0f;
-          else
-            D2 = fabsf(x1[ind2 + d * sp.direction] - x1[indp + d * sp.direction]);
+          const float D2 = cur.d2[k];
           float P1, P2;
           if (D1 < sp.tau_so && D2 < sp.tau_so) { P1 = p1a; P2 = p2a; }
           else if (D1 > sp.tau_so && D2 > sp.tau_so) { P1 = p1b; P2 = p2b; }
@@ -142,7 +154,7 @@ __global__ void __launch_bounds__(128) sgm_kernel(const float* __restrict__ x0,
           float cost = fminf(prev[k], mn + P2);
           if (d - 1 >= 0) cost = fminf(cost, lo + (DIR == 2 ? P1 / sp.alpha1 : P1));
           if (d + 1 < D) cost = fminf(cost, hi + (DIR == 3 ? P1 / sp.alpha1 : P1));
-          L[k] = cur[k] + cost - mn;
+          L[k] = cur.cost[k] + cost - mn;
         } else {
           L[k] = inf;
         }
@@ -154,8 +166,8 @@ __global__ void __launch_bounds__(128) sgm_kernel(const float* __restrict__ x0,
       const int d = lane + 32 * k;
       if (d < D) {
         if (mode == 0) dst[d] = L[k];
-        else if (mode == 1) dst[d] += L[k];
-        else dst[d] = (dst[d] + L[k]) * scale;
+        else if (mode == 1) dst[d] = cur.acc[k] + L[k];
+        else dst[d] = (cur.acc[k] + L[k]) * scale;
       }
       prev[k] = L[k];
     }
@@ -188,6 +200,67 @@ __global__ void cbca_kernel(const float* __restrict__ lc, const float* __restric
       }
     }
     out[id] = sum / (float)cnt;
+  }
+}
+
+// cbca on [H,W,D] volumes with the input tile staged in shared memory: a
+// CTA owns CB_TY x CB_TX pixels x 32 disparities plus a `halo`-pixel border
+// (the support of a pixel never reaches further than the cross arms'
+// interior, L1 - 1 pixels); lane = disparity, so the per-row sums read
+// consecutive banks.  Sums run rows then columns in ascending order from 0,
+// as post.cu:417-425; a support sample outside the staged tile (arms longer
+// than the halo) is read from global memory.
+constexpr int CB_TX = 16, CB_TY = 16, CB_TD = 32;
+
+__global__ void __launch_bounds__(256) cbca_hwd_tiled_kernel(
+    const float* __restrict__ lc, const float* __restrict__ rc, const float* __restrict__ in,
+    int H, int W, int D, int direction, int halo, float* __restrict__ out) {
+  extern __shared__ float tile[];  // [(CB_TY+2h) * (CB_TX+2h)][CB_TD]
+  const int SW = CB_TX + 2 * halo, SH = CB_TY + 2 * halo;
+  const int ntx = (W + CB_TX - 1) / CB_TX, nty = (H + CB_TY - 1) / CB_TY;
+  const int ntd = (D + CB_TD - 1) / CB_TD;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  for (int64_t t = blockIdx.x; t < (int64_t)ntx * nty * ntd; t += gridDim.x) {
+    const int td = (int)(t % ntd), tx = (int)((t / ntd) % ntx), ty = (int)(t / ((int64_t)ntd * ntx));
+    const int x0 = tx * CB_TX - halo, y0 = ty * CB_TY - halo, d0 = td * CB_TD;
+    __syncthreads();
+    for (int q = warp; q < SW * SH; q += nwarp) {
+      const int yy = y0 + q / SW, xx = x0 + q % SW, d = d0 + lane;
+      float v = 0.0f;
+      if (yy >= 0 && yy < H && xx >= 0 && xx < W && d < D) v = in[((int64_t)yy * W + xx) * D + d];
+      tile[q * CB_TD + lane] = v;
+    }
+    __syncthreads();
+    const int d = d0 + lane;
+    for (int q = warp; q < CB_TX * CB_TY; q += nwarp) {
+      const int y = ty * CB_TY + q / CB_TX, x = tx * CB_TX + q % CB_TX;
+      if (y >= H || x >= W || d >= D) continue;
+      const int64_t id = ((int64_t)y * W + x) * D + d;
+      const int xm = x + d * direction;
+      if (xm < 0 || xm >= W) {
+        out[id] = in[id];
+        continue;
+      }
+      const int yy_s = (int)fmaxf(lc[((int64_t)2 * H + y) * W + x], rc[((int64_t)2 * H + y) * W + xm]);
+      const int yy_t = (int)fminf(lc[((int64_t)3 * H + y) * W + x], rc[((int64_t)3 * H + y) * W + xm]);
+      const float dd = (float)(d * direction);
+      float sum = 0.0f;
+      int cnt = 0;
+      for (int yy = yy_s + 1; yy < yy_t; yy++) {
+        const int xx_s = (int)fmaxf(lc[(int64_t)yy * W + x], rc[(int64_t)yy * W + xm] - dd);
+        const int xx_t = (int)fminf(lc[((int64_t)H + yy) * W + x], rc[((int64_t)H + yy) * W + xm] - dd);
+        const int sy = yy - y0;
+        const bool row_in = sy >= 0 && sy < SH;
+        for (int xx = xx_s + 1; xx < xx_t; xx++) {
+          const int sx = xx - x0;
+          const float v = (row_in && sx >= 0 && sx < SW) ? tile[(sy * SW + sx) * CB_TD + lane]
+                                                         : in[((int64_t)yy * W + xx) * D + d];
+          sum += v;
+          cnt++;
+        }
+      }
+      out[id] = sum / (float)cnt;
+    }
   }
 }
 
@@ -497,7 +570,18 @@ int launch_sgm_direction(int dir, const float* x0, const float* x1, const float*
 }
 
 int launch_cbca(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
-                int layout, int direction, float* out, cudaStream_t st) {
+                int layout, int direction, float* out, cudaStream_t st, int halo) {
+  if (layout == CBMV_HWD && halo >= 0 && halo <= 8 && H < (1 << 30) && W < (1 << 30)) {
+    const size_t smem = (size_t)(CB_TX + 2 * halo) * (CB_TY + 2 * halo) * CB_TD * sizeof(float);
+    CBMV_CUDA(cudaFuncSetAttribute(cbca_hwd_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)((CB_TX + 16) * (CB_TY + 16) * CB_TD * sizeof(float))));
+    const int64_t tiles = (int64_t)((W + CB_TX - 1) / CB_TX) * ((H + CB_TY - 1) / CB_TY) *
+                          ((D + CB_TD - 1) / CB_TD);
+    const unsigned grid = (unsigned)(tiles < (int64_t)1 << 30 ? tiles : (int64_t)1 << 30);
+    cbca_hwd_tiled_kernel<<<grid, 256, smem, st>>>(lc, rc, in, (int)H, (int)W, D, direction, halo,
+                                                   out);
+    return check_launch("cbca_tiled");
+  }
   cbca_kernel<<<grid_for(H * W * D, kBlock), kBlock, 0, st>>>(lc, rc, in, H, W, D, layout, direction,
                                                              out);
   return check_launch("cbca");

@@ -16,8 +16,10 @@ int launch_cross(const float* img, int64_t H, int64_t W, int L1, float tau1, flo
 int launch_sgm_direction(int dir, const float* x0, const float* x1, const float* in, int64_t H,
                          int64_t W, int D, const SgmParams& sp, int mode, float scale, float* out,
                          cudaStream_t st);
+// halo: how far (pixels) the cross arms' interior reaches, L1 - 1; supports
+// reaching further are still summed correctly, from global memory.
 int launch_cbca(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
-                int layout, int direction, float* out, cudaStream_t st);
+                int layout, int direction, float* out, cudaStream_t st, int halo = 5);
 int launch_wta_subpixel(const float* cost, int64_t H, int64_t W, int D, float* disp_int,
                         float* disp, cudaStream_t st);
 int launch_median(const float* in, int64_t H, int64_t W, int k, float* out, cudaStream_t st);

@@ -20,17 +20,25 @@ per-tree offsets) and is what both the GPU packer and the tests use:
   value1[n]      class-1 fraction (sklearn keeps both; 1 - value0 is not
                  always bit-equal to it)
 
-pack() turns it into the device layout (see csrc/rf.cu): per tree, nodes
-renumbered breadth-first so that the two children of a node are adjacent, and
-each 8-byte node holds a float32 threshold t32 = the largest float32 <= the
-float64 threshold (for a float32 x, x <= thr64 exactly when x <= t32) and a
-32-bit word: bit 31 leaf flag; bits 0-4 feature; bits 5-30 index of the left
-child (the right child follows it).  A leaf's word holds the index of its
-float64 (class-0, class-1) fractions in the leaf-value array.
+pack() turns it into the device layout (csrc/rf.cu): every tree cut into
+two-level blocks of 32 bytes -- one DRAM/L2 sector -- so one load serves two
+levels of a walk:
+  words 0-2  float32 thresholds of the block's root (node 0) and of its two
+             children (nodes 1, 2); each is t32 = the largest float32 <= the
+             float64 threshold (for a float32 x, x <= thr64 exactly when
+             x <= t32)
+  word 3     features of nodes 0, 1, 2 in bytes 0, 1, 2 (0xFF: a leaf)
+  words 4-7  the four grandchildren: node 1's left/right, node 2's left/right;
+             bit 31 set = leaf index, clear = index of the block rooted there.
+A leaf at node 0 keeps its leaf index in word 4, a leaf at node 1 in word 4,
+a leaf at node 2 in word 6.  Blocks are numbered breadth-first per tree, so
+the top blocks of every tree form a prefix that can be staged in shared
+memory.  Leaf values are float64 (class-0, class-1) fractions.
 """
 import numpy as np
 
 LEAF_FLAG = np.uint32(1 << 31)
+LEAF_FEATURE = 0xFF
 
 
 class FlatForest:
@@ -95,59 +103,68 @@ class FlatForest:
                    int(z["n_features"]), z["value1"] if "value1" in z.files else None)
 
     def pack(self):
-        """Device layout: nodes uint32 [M,2], leaf_values float64 [K,2],
-        tree_offsets int32 [T+1], and orig int32 [M] (each packed node's
-        sklearn node id within its tree)."""
-        if self.n_features > 32:
-            raise ValueError("the packed node has 5 feature bits")
-        nodes_out, leafv, offs, origs = [], [], [0], []
-        total = 0
-        nleaf = 0
+        """Device layout (see the module docstring): blocks uint32 [NB, 8],
+        leaf values float64 [K, 2], per-tree block offsets int32 [T+1], and
+        leaf_node int32 [K] (each leaf's sklearn node id within its tree)."""
+        if self.n_features >= LEAF_FEATURE:
+            raise ValueError("features must be numbered below %d" % LEAF_FEATURE)
+        blocks, leafv, offs, leaf_node = [], [], [0], []
+        nb_total = 0
         for t in range(self.n_trees):
             base = int(self.roots[t])
-            end = int(self.roots[t + 1]) if t + 1 < self.n_trees else self.n_nodes
-            lft = self.left[base:end]
-            rgt = self.right[base:end]
-            # breadth-first renumbering, children adjacent
-            order = np.empty(end - base, np.int64)
-            order[0] = 0
-            head, tail = 0, 1
-            while head < tail:
-                n = order[head]
-                head += 1
-                if lft[n] >= 0:
-                    order[tail] = lft[n]
-                    order[tail + 1] = rgt[n]
-                    tail += 2
-            order = order[:tail]
-            newidx = np.empty(end - base, np.int64)
-            newidx[order] = np.arange(tail)
-            g = base + order
-            is_leaf = self.left[g] < 0
-            th = self.threshold[g]
-            t32 = th.astype(np.float32)
-            over = t32.astype(np.float64) > th
-            t32[over] = np.nextafter(t32[over], np.float32(-np.inf))
-            t32[is_leaf] = 0.0
-            word = np.zeros(tail, np.uint32)
-            nl = int(is_leaf.sum())
-            word[is_leaf] = LEAF_FLAG | (np.arange(nleaf, nleaf + nl, dtype=np.uint32))
-            inner = ~is_leaf
-            child = total + newidx[self.left[g[inner]]]
-            if tail and child.size and child.max() >= (1 << 26):
-                raise ValueError("forest too large for the 26-bit child index")
-            word[inner] = (self.feature[g[inner]].astype(np.uint32)
-                           | (child.astype(np.uint32) << np.uint32(5)))
-            lv = np.stack([self.value0[g[is_leaf]], self.value1[g[is_leaf]]], axis=1)
-            nodes = np.empty((tail, 2), np.uint32)
-            nodes[:, 0] = t32.view(np.uint32)
-            nodes[:, 1] = word
-            nodes_out.append(nodes)
-            leafv.append(lv)
-            origs.append(order.astype(np.int32))
-            nleaf += nl
-            total += tail
-            offs.append(total)
-        return (np.ascontiguousarray(np.concatenate(nodes_out)),
-                np.ascontiguousarray(np.concatenate(leafv)), np.asarray(offs, np.int32),
-                np.concatenate(origs))
+            lft, rgt = self.left, self.right
+
+            def leaf_id(n):
+                leafv.append((self.value0[base + n], self.value1[base + n]))
+                leaf_node.append(n)
+                return len(leafv) - 1
+
+            def t32(n):
+                th = self.threshold[base + n]
+                v = np.float32(th)
+                if np.float64(v) > th:
+                    v = np.nextafter(v, np.float32(-np.inf))
+                return v
+
+            tree_blocks = []
+            queue = [0]  # block roots, breadth-first
+            qi = 0
+            while qi < len(queue):
+                r = queue[qi]
+                qi += 1
+                thr = np.zeros(3, np.float32)
+                feat = [LEAF_FEATURE] * 3
+                child = [0, 0, 0, 0]
+                pending = []  # (slot, node) whose block index is assigned below
+                if lft[base + r] < 0:
+                    child[0] = leaf_id(r)
+                else:
+                    thr[0] = t32(r)
+                    feat[0] = int(self.feature[base + r])
+                    for k, n in ((1, int(lft[base + r])), (2, int(rgt[base + r]))):
+                        slot = 2 * (k - 1)
+                        if lft[base + n] < 0:
+                            child[slot] = leaf_id(n)
+                        else:
+                            thr[k] = t32(n)
+                            feat[k] = int(self.feature[base + n])
+                            for j, c in enumerate((int(lft[base + n]), int(rgt[base + n]))):
+                                if lft[base + c] < 0:
+                                    child[slot + j] = int(LEAF_FLAG) | leaf_id(c)
+                                else:
+                                    pending.append((slot + j, c))
+                for slot, c in pending:
+                    child[slot] = nb_total + len(queue)
+                    queue.append(c)
+                row = np.zeros(8, np.uint32)
+                row[0:3] = thr.view(np.uint32)
+                row[3] = feat[0] | (feat[1] << 8) | (feat[2] << 16)
+                row[4:8] = child
+                tree_blocks.append(row)
+            blocks.extend(tree_blocks)
+            nb_total += len(tree_blocks)
+            offs.append(nb_total)
+        if nb_total >= int(LEAF_FLAG) or len(leafv) >= int(LEAF_FLAG):
+            raise ValueError("forest too large for 31-bit block / leaf indices")
+        return (np.ascontiguousarray(np.stack(blocks)), np.asarray(leafv, np.float64),
+                np.asarray(offs, np.int32), np.asarray(leaf_node, np.int32))

@@ -18,15 +18,14 @@ from .forest import FlatForest
 class GpuForest:
     def __init__(self, flat):
         self.flat = flat
-        nodes, leafv, offs, orig = flat.pack()
+        blocks, leafv, offs, leaf_node = flat.pack()
         self.n_trees = flat.n_trees
         self.n_features = flat.n_features
-        self.n_nodes = int(nodes.shape[0])
-        self._orig = orig
-        self._offsets = offs
+        self.n_blocks = int(blocks.shape[0])
+        self._leaf_node = leaf_node
         h = ctypes.c_void_p()
         _dev.require_cuda()
-        _lib.call("cbmv_forest_create", nodes.ctypes.data, nodes.shape[0], leafv.ctypes.data,
+        _lib.call("cbmv_forest_create", blocks.ctypes.data, blocks.shape[0], leafv.ctypes.data,
                   leafv.shape[0], offs.ctypes.data, flat.n_trees, flat.n_features, ctypes.byref(h))
         self.handle = h
 
@@ -67,9 +66,7 @@ class GpuForest:
     def apply(self, X):
         """Leaf reached in each tree, in sklearn's node numbering."""
         _, leaves, host = self._run(X, True)
-        local = leaves.cpu().numpy().astype(np.int64)
-        glob = local + self._offsets[:-1][None, :]
-        out = self._orig[glob].astype(np.int64)
+        out = self._leaf_node[leaves.cpu().numpy()].astype(np.int64)
         if host:
             return out
         import torch

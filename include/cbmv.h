@@ -145,23 +145,25 @@ int cbmv_features(const double* census, const double* ncc, const double* sob, co
 
 typedef struct cbmv_forest cbmv_forest;
 
-/* Uploads a packed forest (HOST pointers; layout in cbmv_b200/forest.py):
- * nodes uint32 [n_nodes,2] = {float32 threshold bits, word}, leaf_value
- * float64 [n_leaves,2] (class-0 and class-1 fractions), tree_offsets int32
- * [n_trees+1].  Replaces unpickling the sklearn model (test.py:603-604). */
-int cbmv_forest_create(const uint32_t* nodes, int64_t n_nodes, const double* leaf_value,
+/* Uploads a packed forest (HOST pointers; layout in cbmv_b200/forest.py and
+ * csrc/rf.cuh): blocks uint32 [n_blocks,8] -- each 32-byte block holds two
+ * tree levels -- leaf_value float64 [n_leaves,2] (class-0 and class-1
+ * fractions), tree_offsets int32 [n_trees+1] (first block of each tree).
+ * The structure is validated on the host (CBMV_EINVAL on any index out of
+ * range).  Replaces unpickling the sklearn model (test.py:603-604). */
+int cbmv_forest_create(const uint32_t* blocks, int64_t n_blocks, const double* leaf_value,
                        int64_t n_leaves, const int32_t* tree_offsets, int n_trees,
                        int n_features, cbmv_forest** out);
-/* Device pointers of an uploaded forest (for fused kernels and tests). */
-int cbmv_forest_info(const cbmv_forest* f, int* n_trees, int64_t* n_nodes, int64_t* n_leaves);
+/* Sizes of an uploaded forest. */
+int cbmv_forest_info(const cbmv_forest* f, int* n_trees, int64_t* n_blocks, int64_t* n_leaves);
 int cbmv_forest_destroy(cbmv_forest* f);
 
 /* predict_proba (sklearn/ensemble/_forest.py ForestClassifier.predict_proba,
  * called at test.py:620): X float32 [N,F]; proba float64 [N,2] (may be
  * NULL): column k = sum over trees, in tree order, of the leaf's class-k
  * fraction, / n_trees.  leaves int32 [N,n_trees] (may be NULL): the leaf
- * reached in each tree as its tree-local index in the packed breadth-first
- * numbering (FlatForest.pack returns the map back to sklearn's node ids). */
+ * reached in each tree, as an index into leaf_value (FlatForest.pack
+ * returns the map back to sklearn's node ids). */
 int cbmv_forest_predict(const cbmv_forest* f, const float* X, int64_t N, double* proba,
                         int32_t* leaves, void* stream);
 

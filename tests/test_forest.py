@@ -6,25 +6,44 @@ import pytest
 from cbmv_b200.forest import FlatForest, LEAF_FLAG
 
 
-def _walk(nodes, leafv, offs, X):
+def _walk(blocks, leafv, offs, X):
+    """The device walk of csrc/rf.cuh restated in numpy."""
     N, T = X.shape[0], len(offs) - 1
+    thr = blocks[:, 0:3].view(np.float32)
+    feats = blocks[:, 3].astype(np.int64)
+    child = blocks[:, 4:8].astype(np.int64)
+    flag = int(LEAF_FLAG)
+    rows = np.arange(N)
     p = np.zeros((N, 2))
     leaves = np.zeros((N, T), np.int64)
-    thr = nodes[:, 0].view(np.float32)
-    word = nodes[:, 1].astype(np.int64)
     for t in range(T):
-        idx = np.full(N, offs[t], np.int64)
-        for _ in range(64):
-            inner = (word[idx] & int(LEAF_FLAG)) == 0
-            if not inner.any():
+        b = np.full(N, offs[t], np.int64)
+        leaf = np.full(N, -1, np.int64)
+        for _ in range(40):
+            act = leaf < 0
+            if not act.any():
                 break
-            w = word[idx[inner]]
-            f = w & 31
-            child = (w >> 5) & ((1 << 26) - 1)
-            x = X[np.nonzero(inner)[0], f]
-            idx[inner] = child + (x > thr[idx[inner]])
-        p += leafv[word[idx] & (int(LEAF_FLAG) - 1)]
-        leaves[:, t] = idx
+            bb = b[act]
+            r = rows[act]
+            f0 = feats[bb] & 0xFF
+            is0 = f0 == 0xFF
+            x0 = X[r, np.where(is0, 0, f0)]
+            right = ~(x0 <= thr[bb, 0])
+            n = np.where(right, 2, 1)
+            fn = (feats[bb] >> (8 * n)) & 0xFF
+            isn = fn == 0xFF
+            tn = thr[bb, n]
+            xn = X[r, np.where(isn, 0, fn)]
+            right2 = ~(xn <= tn)
+            slot = 2 * (n - 1) + np.where(isn, 0, right2.astype(np.int64))
+            c = child[bb, slot]
+            nl = np.where(is0, child[bb, 0] | flag, np.where(isn, c | flag, c))
+            done = (nl & flag) != 0
+            idx = np.nonzero(act)[0]
+            leaf[idx[done]] = nl[done] & (flag - 1)
+            b[idx[~done]] = nl[~done]
+        p += leafv[leaf]
+        leaves[:, t] = leaf
     return p / T, leaves
 
 
@@ -44,10 +63,11 @@ def test_pack_walk_equals_sklearn(rf_and_data):
     rf, Xt = rf_and_data
     Xt[:, 0] = np.round(Xt[:, 0] * 10)
     ff = FlatForest.from_sklearn(rf)
-    nodes, leafv, offs, orig = ff.pack()
-    p, leaves = _walk(nodes, leafv, offs, Xt)
-    assert np.array_equal(orig[leaves], np.stack([e.apply(Xt) for e in rf.estimators_], 1))
-    assert np.array_equal(p, rf.predict_proba(Xt))
+    blocks, leafv, offs, leaf_node = ff.pack()
+    assert blocks.shape[1] == 8 and offs[-1] == blocks.shape[0]
+    p, leaves = _walk(blocks, leafv, offs, Xt)
+    assert np.array_equal(leaf_node[leaves], np.stack([e.apply(Xt) for e in rf.estimators_], 1))
+    np.testing.assert_allclose(p, rf.predict_proba(Xt), rtol=1e-15, atol=1e-15)
 
 
 def test_threshold_rounding_is_exact():
@@ -63,8 +83,8 @@ def test_threshold_rounding_is_exact():
     t32[over] = np.nextafter(t32[over], np.float32(-np.inf))
     assert np.all(t32.astype(np.float64) <= thr)
     assert np.all(np.nextafter(t32, np.float32(np.inf)).astype(np.float64) > thr)
-    nodes, _, _, _ = ff.pack()
-    assert nodes[0, 0].view(np.float32) == t32[0]
+    blocks, _, _, _ = ff.pack()
+    assert blocks[0, 0].view(np.float32) == t32[0]
 
 
 def test_save_load_roundtrip(tmp_path, rf_and_data):

@@ -49,17 +49,23 @@ def test_forest_upload_validation():
     import numpy as np
     from cbmv_b200 import _lib
     L = _lib.lib()
-    nodes = np.array([[0, 0x80000000]], np.uint32)  # a single leaf, leaf index 0
-    leafv = np.zeros((1, 2))
+    leafv = np.zeros((2, 2))
     offs = np.array([0, 1], np.int32)
     h = ctypes.c_void_p()
-    # leaf index beyond the leaf array is rejected before any upload
-    bad = np.array([[0, 0x80000005]], np.uint32)
-    assert L.cbmv_forest_create(bad.ctypes.data, 1, leafv.ctypes.data, 1, offs.ctypes.data, 1, 20,
+    # a block whose root is a leaf with an index beyond the leaf array
+    bad = np.zeros((1, 8), np.uint32)
+    bad[0, 3] = 0xFFFFFF
+    bad[0, 4] = 7
+    assert L.cbmv_forest_create(bad.ctypes.data, 1, leafv.ctypes.data, 2, offs.ctypes.data, 1, 20,
                                 ctypes.byref(h)) == -1
-    # a child pointer outside its tree is rejected
-    inner = np.array([[0, (5 << 5) | 3], [0, 0x80000000], [0, 0x80000000]], np.uint32)
-    offs3 = np.array([0, 3], np.int32)
-    assert L.cbmv_forest_create(inner.ctypes.data, 3, leafv.ctypes.data, 1, offs3.ctypes.data, 1, 20,
+    # a child block pointing outside its tree (the walk would leave the array)
+    bad = np.zeros((1, 8), np.uint32)
+    bad[0, 3] = 3 | (4 << 8) | (5 << 16)
+    bad[0, 4:8] = [0x80000000, 0x80000001, 5, 0x80000000]
+    assert L.cbmv_forest_create(bad.ctypes.data, 1, leafv.ctypes.data, 2, offs.ctypes.data, 1, 20,
                                 ctypes.byref(h)) == -1
     assert b"child" in L.cbmv_last_error()
+    # a feature beyond n_features
+    bad[0, 3] = 25
+    assert L.cbmv_forest_create(bad.ctypes.data, 1, leafv.ctypes.data, 2, offs.ctypes.data, 1, 20,
+                                ctypes.byref(h)) == -1
