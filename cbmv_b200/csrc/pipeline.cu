@@ -99,6 +99,7 @@ struct Work {
   double* stats;
   float *volA, *volB;
   float *imL, *imR, *crossL, *crossR, *dtmp, *dtmp2;
+  float* grad;  // SGM neighbour differences: left h/v, right h/v
   double* mom;
 };
 
@@ -126,6 +127,7 @@ Work carve(void* base, int64_t H, int64_t W, int D, size_t* bytes) {
   w.crossR = c.take<float>(4 * HW);
   w.dtmp = c.take<float>(HW);
   w.dtmp2 = c.take<float>(HW);
+  w.grad = c.take<float>(4 * HW);
   w.mom = c.take<double>(4);
   *bytes = c.off + 256;
   return w;
@@ -231,12 +233,15 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
     float* t = cur; cur = oth; oth = t;
   }
   SgmParams sp{p->pi1, p->pi2, p->tau_so, p->alpha1, p->sgm_q1, p->sgm_q2, p->direction};
+  SgmGrad g{w.grad, w.grad + HW, w.grad + 2 * HW, w.grad + 3 * HW};
+  // the four direction volumes reuse the float64 cost volumes, dead by now
+  const int64_t V = HW * D;
+  SgmOut so{{(float*)w.vol[0], (float*)w.vol[0] + V, (float*)w.vol[1], (float*)w.vol[1] + V}};
+  if (p->sgm_i > 0) RC(launch_sgm_grad(w.imL, w.imR, H, W, &g, st));
   for (int i = 0; i < p->sgm_i; i++) {
     // out = ((L0 + L1 + L2) + L3) / 4   (test.py:379-383)
-    RC(launch_sgm_direction(0, w.imL, w.imR, cur, H, W, D, sp, 0, 1.0f, oth, st));
-    RC(launch_sgm_direction(1, w.imL, w.imR, cur, H, W, D, sp, 1, 1.0f, oth, st));
-    RC(launch_sgm_direction(2, w.imL, w.imR, cur, H, W, D, sp, 1, 1.0f, oth, st));
-    RC(launch_sgm_direction(3, w.imL, w.imR, cur, H, W, D, sp, 2, 0.25f, oth, st));
+    RC(launch_sgm4(g, cur, H, W, D, sp, so, st));
+    RC(launch_sgm_combine(so, V, nullptr, 0.25f, oth, st));
     float* t = cur; cur = oth; oth = t;
   }
   for (int i = 0; i < p->cbca_i2; i++) {

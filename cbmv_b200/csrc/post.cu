@@ -59,118 +59,148 @@ __global__ void cross_kernel(const float* __restrict__ x0, int64_t H, int64_t W,
   }
 }
 
-// One scan direction of sgm2 (post.cu:178-261) per launch; warp = scan line.
-// mode 0: out = L; mode 1: out += L; mode 2: out = (out + L) * scale.
-template <int DIR, int KPL>
-__global__ void __launch_bounds__(128) sgm_kernel(const float* __restrict__ x0,
-                                                  const float* __restrict__ x1,
-                                                  const float* __restrict__ in, int H, int W, int D,
-                                                  SgmParams sp, int mode, float scale,
-                                                  float* __restrict__ out) {
-  const int line = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+// Absolute differences of neighbouring pixels of a normalised image:
+// gh[y][x] = |I[y][x] - I[y][x-1]|, gv[y][x] = |I[y][x] - I[y-1][x]| (0 on
+// the first column / row).  SGM's image terms D1 and D2 (post.cu:230-237)
+// are exactly these values (|a - b| == |b - a| in IEEE arithmetic).
+__global__ void grad_kernel(const float* __restrict__ img, int64_t H, int64_t W,
+                            float* __restrict__ gh, float* __restrict__ gv) {
+  GRID_STRIDE(p, H * W) {
+    const int64_t y = p / W, x = p - y * W;
+    const float c = img[p];
+    gh[p] = x > 0 ? fabsf(c - img[p - 1]) : 0.0f;
+    gv[p] = y > 0 ? fabsf(c - img[p - W]) : 0.0f;
+  }
+}
+
+// sgm2 (post.cu:178-261) for all four scan directions in one launch: one
+// warp per scan line (the 2H horizontal and 2W vertical lines run
+// concurrently, each direction writing its path costs to its own volume),
+// lane = d (mod 32), KPL disparities per lane.  The scan runs inside the
+// kernel; the step's costs, D1 and the per-d D2 do not depend on the
+// recursion and are loaded PF steps ahead from a register ring.
+template <int DIR, int KPL, int PF>
+__device__ __forceinline__ void sgm_scan(const SgmGrad& g, const float* __restrict__ in, int H, int W,
+                                         int D, const SgmParams& sp, int line,
+                                         float* __restrict__ out) {
   const int lane = threadIdx.x & 31;
-  const int nlines = DIR <= 1 ? H : W;
-  if (line >= nlines) return;
   const int nsteps = DIR <= 1 ? W : H;
   const int dx = DIR == 0 ? 1 : DIR == 1 ? -1 : 0;
-  const int dy = DIR == 2 ? 1 : DIR == 3 ? -1 : 0;
   const float inf = __int_as_float(0x7f800000);
-  // penalties of post.cu:239-248 and the alpha1 split of :252/:255
-  const float p1a = sp.pi1, p2a = sp.pi2;
-  const float p1b = sp.pi1 / (sp.q1 * sp.q2), p2b = sp.pi2 / (sp.q1 * sp.q2);
-  const float p1c = sp.pi1 / sp.q1, p2c = sp.pi2 / sp.q1;
+  // penalties of post.cu:239-248; the alpha1 split of :252/:255 applies to
+  // the d-1 term in direction 2 and to the d+1 term in direction 3
+  const float p1[3] = {sp.pi1, sp.pi1 / (sp.q1 * sp.q2), sp.pi1 / sp.q1};
+  const float p2[3] = {sp.pi2, sp.pi2 / (sp.q1 * sp.q2), sp.pi2 / sp.q1};
+  float p1lo[3], p1hi[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    p1lo[c] = DIR == 2 ? p1[c] / sp.alpha1 : p1[c];
+    p1hi[c] = DIR == 3 ? p1[c] / sp.alpha1 : p1[c];
+  }
+  const float* gl = DIR <= 1 ? g.lh : g.lv;
+  const float* gr = DIR <= 1 ? g.rh : g.rv;
+  // the difference to the previous pixel of the scan sits at the later of
+  // the two pixels in the neighbour-difference images
+  const int gshift = DIR == 1 ? 1 : DIR == 3 ? W : 0;
 
-  // Everything a step reads that does not depend on the recursion -- the
-  // step's costs, the output it accumulates into, and the image differences
-  // D1 (left image) and D2 (right image, per d) -- is loaded one step ahead.
   struct Step {
-    float cost[KPL], acc[KPL], d2[KPL];
+    float cost[KPL], d2[KPL];
     float d1;
   };
-  auto coords = [&](int step, int& x, int& y) {
-    if (DIR == 0) { x = step; y = line; }
-    else if (DIR == 1) { x = W - 1 - step; y = line; }
-    else if (DIR == 2) { x = line; y = step; }
-    else { x = line; y = H - 1 - step; }
+  auto pix = [&](int step) -> int64_t {
+    if (DIR == 0) return (int64_t)line * W + step;
+    if (DIR == 1) return (int64_t)line * W + (W - 1 - step);
+    if (DIR == 2) return (int64_t)step * W + line;
+    return (int64_t)(H - 1 - step) * W + line;
   };
   auto load = [&](int step, Step& s) {
-    int x, y;
-    coords(step, x, y);
-    const int64_t ind2 = (int64_t)y * W + x;
+    const int64_t ind2 = pix(step);
+    const int x = DIR <= 1 ? (DIR == 0 ? step : W - 1 - step) : line;
     const float* src = in + ind2 * D;
-    const float* acc = out + ind2 * D;
-    const bool first = step == 0;  // no previous pixel: D1/D2 unused
-    const int64_t indp = first ? ind2 : ind2 - (int64_t)dy * W - dx;
-    s.d1 = first ? 0.0f : fabsf(x0[ind2] - x0[indp]);
+    s.d1 = step > 0 ? gl[ind2 + gshift] : 0.0f;
 #pragma unroll
     for (int k = 0; k < KPL; k++) {
       const int d = lane + 32 * k;
       s.cost[k] = d < D ? src[d] : inf;
-      s.acc[k] = (mode != 0 && d < D) ? acc[d] : 0.0f;
       const int xx = x + d * sp.direction;
       // post.cu:232-237: D2 = 10 when the matching pixel or its predecessor
       // leaves the image
-      if (first || d >= D || xx < 0 || xx >= W || xx - dx < 0 || xx - dx >= W)
+      if (step == 0 || d >= D || xx < 0 || xx >= W || xx - dx < 0 || xx - dx >= W)
         s.d2[k] = 10.0f;
       else
-        s.d2[k] = fabsf(x1[ind2 + d * sp.direction] - x1[indp + d * sp.direction]);
+        s.d2[k] = gr[ind2 + d * sp.direction + gshift];
     }
   };
   float prev[KPL];
-  Step nxt;
-  load(0, nxt);
-  for (int step = 0; step < nsteps; step++) {
-    const Step cur = nxt;
-    if (step + 1 < nsteps) load(step + 1, nxt);
-    int x, y;
-    coords(step, x, y);
-    float L[KPL];
-    if (step == 0) {
+  Step ring[PF];
 #pragma unroll
-      for (int k = 0; k < KPL; k++) L[k] = cur.cost[k];
-    } else {
-      float mn = prev[0];
+  for (int i = 0; i < PF; i++)
+    if (i < nsteps) load(i, ring[i]);
+  for (int s0 = 0; s0 < nsteps; s0 += PF) {
 #pragma unroll
-      for (int k = 1; k < KPL; k++) mn = fminf(mn, prev[k]);
+    for (int i = 0; i < PF; i++) {
+      const int step = s0 + i;
+      if (step >= nsteps) break;
+      const Step cur = ring[i];
+      if (step + PF < nsteps) load(step + PF, ring[i]);
+      float L[KPL];
+      if (step == 0) {
 #pragma unroll
-      for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-      const float D1 = cur.d1;
+        for (int k = 0; k < KPL; k++) L[k] = cur.cost[k];
+      } else {
+        float mn = prev[0];
+#pragma unroll
+        for (int k = 1; k < KPL; k++) mn = fminf(mn, prev[k]);
+#pragma unroll
+        for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        const bool d1lo = cur.d1 < sp.tau_so, d1hi = cur.d1 > sp.tau_so;
+#pragma unroll
+        for (int k = 0; k < KPL; k++) {
+          const int d = lane + 32 * k;
+          // neighbours d-1 and d+1 of the previous step
+          float lo = __shfl_up_sync(0xffffffffu, prev[k], 1);
+          float hi = __shfl_down_sync(0xffffffffu, prev[k], 1);
+          const float lo_w = __shfl_sync(0xffffffffu, prev[k > 0 ? k - 1 : 0], 31);
+          const float hi_w = __shfl_sync(0xffffffffu, prev[k + 1 < KPL ? k + 1 : k], 0);
+          if (lane == 0) lo = lo_w;
+          if (lane == 31) hi = hi_w;
+          const float D2 = cur.d2[k];
+          const int c = (d1lo && D2 < sp.tau_so) ? 0 : (d1hi && D2 > sp.tau_so) ? 1 : 2;
+          float cost = fminf(prev[k], mn + p2[c]);
+          if (d - 1 >= 0) cost = fminf(cost, lo + p1lo[c]);
+          if (d + 1 < D) cost = fminf(cost, hi + p1hi[c]);
+          L[k] = d < D ? cur.cost[k] + cost - mn : inf;
+        }
+      }
+      float* dst = out + pix(step) * D;
 #pragma unroll
       for (int k = 0; k < KPL; k++) {
         const int d = lane + 32 * k;
-        // neighbours d-1 and d+1 of the previous step
-        float lo = __shfl_up_sync(0xffffffffu, prev[k], 1);
-        float hi = __shfl_down_sync(0xffffffffu, prev[k], 1);
-        const float lo_w = __shfl_sync(0xffffffffu, prev[k > 0 ? k - 1 : 0], 31);
-        const float hi_w = __shfl_sync(0xffffffffu, prev[k + 1 < KPL ? k + 1 : k], 0);
-        if (lane == 0) lo = lo_w;
-        if (lane == 31) hi = hi_w;
-        if (d < D) {
-          const float D2 = cur.d2[k];
-          float P1, P2;
-          if (D1 < sp.tau_so && D2 < sp.tau_so) { P1 = p1a; P2 = p2a; }
-          else if (D1 > sp.tau_so && D2 > sp.tau_so) { P1 = p1b; P2 = p2b; }
-          else { P1 = p1c; P2 = p2c; }
-          float cost = fminf(prev[k], mn + P2);
-          if (d - 1 >= 0) cost = fminf(cost, lo + (DIR == 2 ? P1 / sp.alpha1 : P1));
-          if (d + 1 < D) cost = fminf(cost, hi + (DIR == 3 ? P1 / sp.alpha1 : P1));
-          L[k] = cur.cost[k] + cost - mn;
-        } else {
-          L[k] = inf;
-        }
+        if (d < D) dst[d] = L[k];
+        prev[k] = L[k];
       }
     }
-    float* dst = out + ((int64_t)y * W + x) * D;
-#pragma unroll
-    for (int k = 0; k < KPL; k++) {
-      const int d = lane + 32 * k;
-      if (d < D) {
-        if (mode == 0) dst[d] = L[k];
-        else if (mode == 1) dst[d] = cur.acc[k] + L[k];
-        else dst[d] = (cur.acc[k] + L[k]) * scale;
-      }
-      prev[k] = L[k];
-    }
+  }
+}
+
+template <int KPL, int PF>
+__global__ void __launch_bounds__(128) sgm4_kernel(SgmGrad g, const float* __restrict__ in, int H,
+                                                   int W, int D, SgmParams sp, SgmOut o) {
+  const int warp = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (warp < H) sgm_scan<0, KPL, PF>(g, in, H, W, D, sp, warp, o.dir[0]);
+  else if (warp < 2 * H) sgm_scan<1, KPL, PF>(g, in, H, W, D, sp, warp - H, o.dir[1]);
+  else if (warp < 2 * H + W) sgm_scan<2, KPL, PF>(g, in, H, W, D, sp, warp - 2 * H, o.dir[2]);
+  else if (warp < 2 * H + 2 * W) sgm_scan<3, KPL, PF>(g, in, H, W, D, sp, warp - 2 * H - W, o.dir[3]);
+}
+
+// out = base + (((L0 + L1) + L2) + L3) * scale over n elements (base may be
+// out itself, or null for 0): the four directions summed as post.cu
+// sgm_w adds them (directions in order 0..3).
+__global__ void sgm_combine_kernel(SgmOut o, int64_t n, const float* base, float scale,
+                                   float* out) {
+  GRID_STRIDE(i, n) {
+    const float s = ((o.dir[0][i] + o.dir[1][i]) + o.dir[2][i]) + o.dir[3][i];
+    out[i] = base ? base[i] + s * scale : s * scale;
   }
 }
 
@@ -203,61 +233,98 @@ __global__ void cbca_kernel(const float* __restrict__ lc, const float* __restric
   }
 }
 
-// cbca on [H,W,D] volumes with the input tile staged in shared memory: a
-// CTA owns CB_TY x CB_TX pixels x 32 disparities plus a `halo`-pixel border
-// (the support of a pixel never reaches further than the cross arms'
-// interior, L1 - 1 pixels); lane = disparity, so the per-row sums read
-// consecutive banks.  Sums run rows then columns in ascending order from 0,
-// as post.cu:417-425; a support sample outside the staged tile (arms longer
-// than the halo) is read from global memory.
+// cbca on [H,W,D] volumes, tiled: a CTA owns CB_TY x CB_TX pixels x 32
+// disparities.  Shared memory holds the input tile with a `halo`-pixel
+// border (a pixel's support never reaches beyond its cross arms' interior,
+// L1 - 1 pixels) and the tile's cross arms as int16: the left arms of the
+// tile columns, and the right arms of every column x + d*direction the tile
+// matches against.  Lane = disparity, so the running sums read consecutive
+// banks.  Each output is the float sum over its support in the reference's
+// order (rows ascending, then columns ascending, from 0; post.cu:415-429)
+// divided by the count; a support row that reaches outside the staged tile
+// (arms longer than the halo) is summed from global memory instead.
 constexpr int CB_TX = 16, CB_TY = 16, CB_TD = 32;
+
+__host__ __device__ constexpr int cbca_rw() { return CB_TX + CB_TD - 1; }
+
+__host__ __device__ inline size_t cbca_smem_bytes(int halo) {
+  const int SW = CB_TX + 2 * halo, SH = CB_TY + 2 * halo;
+  return (size_t)SW * SH * CB_TD * sizeof(float) +
+         (size_t)4 * SH * (CB_TX + cbca_rw()) * sizeof(int16_t);
+}
 
 __global__ void __launch_bounds__(256) cbca_hwd_tiled_kernel(
     const float* __restrict__ lc, const float* __restrict__ rc, const float* __restrict__ in,
     int H, int W, int D, int direction, int halo, float* __restrict__ out) {
-  extern __shared__ float tile[];  // [(CB_TY+2h) * (CB_TX+2h)][CB_TD]
+  extern __shared__ float tile[];  // [SH*SW][CB_TD], then int16 arms
   const int SW = CB_TX + 2 * halo, SH = CB_TY + 2 * halo;
+  const int RW = cbca_rw();
+  int16_t* sl = reinterpret_cast<int16_t*>(tile + (size_t)SW * SH * CB_TD);  // [4][SH][CB_TX]
+  int16_t* sr = sl + 4 * SH * CB_TX;                                         // [4][SH][RW]
   const int ntx = (W + CB_TX - 1) / CB_TX, nty = (H + CB_TY - 1) / CB_TY;
   const int ntd = (D + CB_TD - 1) / CB_TD;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int64_t HW = (int64_t)H * W;
   for (int64_t t = blockIdx.x; t < (int64_t)ntx * nty * ntd; t += gridDim.x) {
     const int td = (int)(t % ntd), tx = (int)((t / ntd) % ntx), ty = (int)(t / ((int64_t)ntd * ntx));
-    const int x0 = tx * CB_TX - halo, y0 = ty * CB_TY - halo, d0 = td * CB_TD;
+    const int X0 = tx * CB_TX, Y0 = ty * CB_TY, d0 = td * CB_TD;
+    const int x0 = X0 - halo, y0 = Y0 - halo;
+    // first matched column of the tile: x + d*direction over the tile
+    const int xr0 = direction < 0 ? X0 - d0 - (CB_TD - 1) : X0 + d0;
     __syncthreads();
     for (int q = warp; q < SW * SH; q += nwarp) {
       const int yy = y0 + q / SW, xx = x0 + q % SW, d = d0 + lane;
       float v = 0.0f;
-      if (yy >= 0 && yy < H && xx >= 0 && xx < W && d < D) v = in[((int64_t)yy * W + xx) * D + d];
+      if (yy >= 0 && yy < H && xx >= 0 && xx < W && d < D) v = __ldg(in + ((int64_t)yy * W + xx) * D + d);
       tile[q * CB_TD + lane] = v;
+    }
+    for (int q = threadIdx.x; q < 4 * SH * CB_TX; q += blockDim.x) {
+      const int a = q / (SH * CB_TX), r = (q / CB_TX) % SH, c = q % CB_TX;
+      const int yy = y0 + r, xx = X0 + c;
+      sl[q] = (yy >= 0 && yy < H && xx < W) ? (int16_t)__ldg(lc + a * HW + (int64_t)yy * W + xx) : 0;
+    }
+    for (int q = threadIdx.x; q < 4 * SH * RW; q += blockDim.x) {
+      const int a = q / (SH * RW), r = (q / RW) % SH, c = q % RW;
+      const int yy = y0 + r, xx = xr0 + c;
+      sr[q] = (yy >= 0 && yy < H && xx >= 0 && xx < W) ? (int16_t)__ldg(rc + a * HW + (int64_t)yy * W + xx) : 0;
     }
     __syncthreads();
     const int d = d0 + lane;
+    const int dd = d * direction;
     for (int q = warp; q < CB_TX * CB_TY; q += nwarp) {
-      const int y = ty * CB_TY + q / CB_TX, x = tx * CB_TX + q % CB_TX;
+      const int cy = q / CB_TX, cx = q % CB_TX;
+      const int y = Y0 + cy, x = X0 + cx;
       if (y >= H || x >= W || d >= D) continue;
       const int64_t id = ((int64_t)y * W + x) * D + d;
-      const int xm = x + d * direction;
+      const int xm = x + dd;
       if (xm < 0 || xm >= W) {
         out[id] = in[id];
         continue;
       }
-      const int yy_s = (int)fmaxf(lc[((int64_t)2 * H + y) * W + x], rc[((int64_t)2 * H + y) * W + xm]);
-      const int yy_t = (int)fminf(lc[((int64_t)3 * H + y) * W + x], rc[((int64_t)3 * H + y) * W + xm]);
-      const float dd = (float)(d * direction);
+      const int cm = xm - xr0;  // column of xm in the staged right arms
+      const int ry = cy + halo;
+      const int yy_s = max((int)sl[(2 * SH + ry) * CB_TX + cx], (int)sr[(2 * SH + ry) * RW + cm]);
+      const int yy_t = min((int)sl[(3 * SH + ry) * CB_TX + cx], (int)sr[(3 * SH + ry) * RW + cm]);
       float sum = 0.0f;
       int cnt = 0;
       for (int yy = yy_s + 1; yy < yy_t; yy++) {
-        const int xx_s = (int)fmaxf(lc[(int64_t)yy * W + x], rc[(int64_t)yy * W + xm] - dd);
-        const int xx_t = (int)fminf(lc[((int64_t)H + yy) * W + x], rc[((int64_t)H + yy) * W + xm] - dd);
-        const int sy = yy - y0;
-        const bool row_in = sy >= 0 && sy < SH;
-        for (int xx = xx_s + 1; xx < xx_t; xx++) {
-          const int sx = xx - x0;
-          const float v = (row_in && sx >= 0 && sx < SW) ? tile[(sy * SW + sx) * CB_TD + lane]
-                                                         : in[((int64_t)yy * W + xx) * D + d];
-          sum += v;
-          cnt++;
+        const int r = yy - y0;
+        int xx_s, xx_t;
+        const bool row_in = r >= 0 && r < SH;
+        if (row_in) {
+          xx_s = max((int)sl[r * CB_TX + cx], (int)sr[r * RW + cm] - dd);
+          xx_t = min((int)sl[(SH + r) * CB_TX + cx], (int)sr[(SH + r) * RW + cm] - dd);
+        } else {
+          xx_s = (int)fmaxf(lc[(int64_t)yy * W + x], rc[(int64_t)yy * W + xm] - (float)dd);
+          xx_t = (int)fminf(lc[HW + (int64_t)yy * W + x], rc[HW + (int64_t)yy * W + xm] - (float)dd);
         }
+        if (row_in && xx_s + 1 >= x0 && xx_t - 1 < x0 + SW) {
+          const float* rowp = tile + ((size_t)r * SW - x0) * CB_TD + lane;
+          for (int xx = xx_s + 1; xx < xx_t; xx++) sum += rowp[xx * CB_TD];
+        } else {
+          for (int xx = xx_s + 1; xx < xx_t; xx++) sum += in[((int64_t)yy * W + xx) * D + d];
+        }
+        cnt += max(xx_t - xx_s - 1, 0);
       }
       out[id] = sum / (float)cnt;
     }
@@ -536,45 +603,47 @@ int launch_cross(const float* img, int64_t H, int64_t W, int L1, float tau1, flo
   return check_launch("cross");
 }
 
-template <int DIR, int KPL>
-static void sgm_launch(const float* x0, const float* x1, const float* in, int H, int W, int D,
-                       const SgmParams& sp, int mode, float scale, float* out, cudaStream_t st) {
-  const int nlines = DIR <= 1 ? H : W;
-  const int blocks = (nlines * 32 + 127) / 128;
-  sgm_kernel<DIR, KPL><<<blocks, 128, 0, st>>>(x0, x1, in, H, W, D, sp, mode, scale, out);
+int launch_sgm_grad(const float* imL, const float* imR, int64_t H, int64_t W, SgmGrad* g,
+                    cudaStream_t st) {
+  grad_kernel<<<grid_for(H * W, 256), 256, 0, st>>>(imL, H, W, g->lh, g->lv);
+  grad_kernel<<<grid_for(H * W, 256), 256, 0, st>>>(imR, H, W, g->rh, g->rv);
+  return check_launch("sgm_grad");
 }
 
 template <int KPL>
-static void sgm_dir(int dir, const float* x0, const float* x1, const float* in, int H, int W, int D,
-                    const SgmParams& sp, int mode, float scale, float* out, cudaStream_t st) {
-  switch (dir) {
-    case 0: sgm_launch<0, KPL>(x0, x1, in, H, W, D, sp, mode, scale, out, st); break;
-    case 1: sgm_launch<1, KPL>(x0, x1, in, H, W, D, sp, mode, scale, out, st); break;
-    case 2: sgm_launch<2, KPL>(x0, x1, in, H, W, D, sp, mode, scale, out, st); break;
-    default: sgm_launch<3, KPL>(x0, x1, in, H, W, D, sp, mode, scale, out, st); break;
-  }
+static void sgm4_launch(const SgmGrad& g, const float* in, int H, int W, int D, const SgmParams& sp,
+                        const SgmOut& o, cudaStream_t st) {
+  const int lines = 2 * H + 2 * W;
+  const int blocks = (lines * 32 + 127) / 128;
+  constexpr int PF = KPL <= 2 ? 8 : KPL <= 4 ? 6 : KPL <= 8 ? 3 : 1;
+  sgm4_kernel<KPL, PF><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
 }
 
-int launch_sgm_direction(int dir, const float* x0, const float* x1, const float* in, int64_t H,
-                         int64_t W, int D, const SgmParams& sp, int mode, float scale, float* out,
-                         cudaStream_t st) {
+int launch_sgm4(const SgmGrad& g, const float* in, int64_t H, int64_t W, int D, const SgmParams& sp,
+                const SgmOut& o, cudaStream_t st) {
   const int kpl = (D + 31) / 32;
   const int h = (int)H, w = (int)W;
-  if (kpl <= 1) sgm_dir<1>(dir, x0, x1, in, h, w, D, sp, mode, scale, out, st);
-  else if (kpl <= 2) sgm_dir<2>(dir, x0, x1, in, h, w, D, sp, mode, scale, out, st);
-  else if (kpl <= 4) sgm_dir<4>(dir, x0, x1, in, h, w, D, sp, mode, scale, out, st);
-  else if (kpl <= 8) sgm_dir<8>(dir, x0, x1, in, h, w, D, sp, mode, scale, out, st);
-  else if (kpl <= 16) sgm_dir<16>(dir, x0, x1, in, h, w, D, sp, mode, scale, out, st);
-  else sgm_dir<32>(dir, x0, x1, in, h, w, D, sp, mode, scale, out, st);
-  return check_launch("sgm");
+  if (kpl <= 1) sgm4_launch<1>(g, in, h, w, D, sp, o, st);
+  else if (kpl <= 2) sgm4_launch<2>(g, in, h, w, D, sp, o, st);
+  else if (kpl <= 4) sgm4_launch<4>(g, in, h, w, D, sp, o, st);
+  else if (kpl <= 8) sgm4_launch<8>(g, in, h, w, D, sp, o, st);
+  else if (kpl <= 16) sgm4_launch<16>(g, in, h, w, D, sp, o, st);
+  else sgm4_launch<32>(g, in, h, w, D, sp, o, st);
+  return check_launch("sgm4");
+}
+
+int launch_sgm_combine(const SgmOut& o, int64_t n, const float* base, float scale, float* out,
+                       cudaStream_t st) {
+  sgm_combine_kernel<<<grid_for(n, 256), 256, 0, st>>>(o, n, base, scale, out);
+  return check_launch("sgm_combine");
 }
 
 int launch_cbca(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
                 int layout, int direction, float* out, cudaStream_t st, int halo) {
-  if (layout == CBMV_HWD && halo >= 0 && halo <= 8 && H < (1 << 30) && W < (1 << 30)) {
-    const size_t smem = (size_t)(CB_TX + 2 * halo) * (CB_TY + 2 * halo) * CB_TD * sizeof(float);
+  if (layout == CBMV_HWD && halo >= 0 && halo <= 8 && H < 32767 && W < 32767) {
+    const size_t smem = cbca_smem_bytes(halo);
     CBMV_CUDA(cudaFuncSetAttribute(cbca_hwd_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)((CB_TX + 16) * (CB_TY + 16) * CB_TD * sizeof(float))));
+                                   (int)cbca_smem_bytes(8)));
     const int64_t tiles = (int64_t)((W + CB_TX - 1) / CB_TX) * ((H + CB_TY - 1) / CB_TY) *
                           ((D + CB_TD - 1) / CB_TD);
     const unsigned grid = (unsigned)(tiles < (int64_t)1 << 30 ? tiles : (int64_t)1 << 30);
@@ -650,12 +719,18 @@ extern "C" int cbmv_sgm(const float* imL, const float* imR, const float* in, int
   REQ_HW(H, W);
   CBMV_REQUIRE(D > 0 && D <= 1024, CBMV_ERANGE, "D=%d not in 1..1024", D);
   CBMV_REQUIRE(in != out, CBMV_EINVAL, "sgm: in and out must differ");
+  cudaStream_t st = as_stream(stream);
+  const int64_t HW = H * W, V = HW * D;
+  float* scratch = nullptr;
+  CBMV_CUDA(cudaMallocAsync(&scratch, sizeof(float) * (4 * HW + 4 * V), st));
+  SgmGrad g{scratch, scratch + HW, scratch + 2 * HW, scratch + 3 * HW};
+  SgmOut o{{scratch + 4 * HW, scratch + 4 * HW + V, scratch + 4 * HW + 2 * V, scratch + 4 * HW + 3 * V}};
   SgmParams sp{pi1, pi2, tau_so, alpha1, q1, q2, direction};
-  for (int dir = 0; dir < 4; dir++) {
-    int rc = launch_sgm_direction(dir, imL, imR, in, H, W, D, sp, 1, 1.0f, out, as_stream(stream));
-    if (rc) return rc;
-  }
-  return CBMV_OK;
+  int rc = launch_sgm_grad(imL, imR, H, W, &g, st);
+  if (!rc) rc = launch_sgm4(g, in, H, W, D, sp, o, st);
+  if (!rc) rc = launch_sgm_combine(o, V, out, 1.0f, out, st);
+  CBMV_CUDA(cudaFreeAsync(scratch, st));
+  return rc;
 }
 
 extern "C" int cbmv_cbca(const float* crossL, const float* crossR, const float* in, int64_t H,

@@ -13,9 +13,21 @@ struct SgmParams {
 
 int launch_cross(const float* img, int64_t H, int64_t W, int L1, float tau1, float* out,
                  cudaStream_t st);
-int launch_sgm_direction(int dir, const float* x0, const float* x1, const float* in, int64_t H,
-                         int64_t W, int D, const SgmParams& sp, int mode, float scale, float* out,
-                         cudaStream_t st);
+// Neighbour differences of both normalised images (see post.cu grad_kernel).
+struct SgmGrad {
+  float *lh, *lv, *rh, *rv;
+};
+int launch_sgm_grad(const float* imL, const float* imR, int64_t H, int64_t W, SgmGrad* g,
+                    cudaStream_t st);
+// Path costs of the four scan directions, one volume each.
+struct SgmOut {
+  float* dir[4];
+};
+int launch_sgm4(const SgmGrad& g, const float* in, int64_t H, int64_t W, int D, const SgmParams& sp,
+                const SgmOut& o, cudaStream_t st);
+// out = base + (((L0 + L1) + L2) + L3) * scale; base may be null or out.
+int launch_sgm_combine(const SgmOut& o, int64_t n, const float* base, float scale, float* out,
+                       cudaStream_t st);
 // halo: how far (pixels) the cross arms' interior reaches, L1 - 1; supports
 // reaching further are still summed correctly, from global memory.
 int launch_cbca(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
