@@ -40,6 +40,8 @@ SIGNATURES = {
     "cbmv_version": [],
     "cbmv_sync": [_vp],
     "cbmv_census": [_vp, _vp, _i64, _i64, _int, _int, _vp, _int, _int, _vp],
+    "cbmv_census_static": [_vp, _vp, _i64, _i64, _int, _int, _vp, _int, _int, _vp],
+    "cbmv_census_static_max_pixels": [],
     "cbmv_ncc": [_vp, _vp, _i64, _i64, _int, _int, _vp, _int, _int, _vp],
     "cbmv_sobel": [_vp, _i64, _i64, _vp, _int, _vp],
     "cbmv_sadsob": [_vp, _vp, _int, _i64, _i64, _int, _int, _vp, _int, _int, _vp],
@@ -82,7 +84,7 @@ SIGNATURES = {
     "cbmv_run_rf": [_vp, _vp, ctypes.POINTER(cbmv_params), _vp, _vp, _i64, _i64, _int, _vp, _vp],
 }
 _RESTYPE = {"cbmv_last_error": ctypes.c_char_p, "cbmv_version": ctypes.c_char_p,
-            "cbmv_params_default": None}
+            "cbmv_params_default": None, "cbmv_census_static_max_pixels": ctypes.c_int64}
 
 _lib = None
 

@@ -336,6 +336,8 @@ int launch_zsad_cost(const uint8_t* L, const uint8_t* R, const double* ml, const
 
 template int launch_census_cost<double>(const ulonglong2*, const ulonglong2*, int64_t, int64_t, int,
                                         int, int, double*, cudaStream_t);
+template int launch_census_cost<float>(const ulonglong2*, const ulonglong2*, int64_t, int64_t, int,
+                                       int, int, float*, cudaStream_t);
 template int launch_ncc_cost<double>(const uint8_t*, const uint8_t*, const uint32_t*,
                                      const uint32_t*, const double*, const double*, int64_t,
                                      int64_t, int, int, int, double*, cudaStream_t);

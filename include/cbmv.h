@@ -66,6 +66,26 @@ int cbmv_sync(void* stream);
 int cbmv_census(const uint8_t* L, const uint8_t* R, int64_t H, int64_t W, int D, int wsize,
                 void* out, int dtype, int layout, void* stream);
 
+/* census without any device allocation -- no counterpart in the reference.
+ * Same arguments, results and errors as cbmv_census, for callers that may
+ * not allocate device memory when they call the matcher (an arena or
+ * caching allocator that owns the device heap, a CUDA graph being captured,
+ * a plugin host that hands out only input and output buffers).  Its scratch
+ * -- the two census descriptor images -- lives in one fixed device array of
+ * cbmv_census_static_max_pixels() pixels per image (1,048,576; 32 MiB held
+ * by every GPU that loads the library, until the process exits).  Larger
+ * images are rejected with CBMV_ERANGE; use cbmv_census for them.
+ *  - The first call on each device looks up the array's device address
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - All calls on a device share the one array: calls whose work overlaps on
+ *    the GPU (different streams, or threads without ordering) race and
+ *    corrupt each other's results; serialise them on one stream.
+ *  - Each call writes every descriptor it reads, so no clearing is needed
+ *    between calls. */
+int cbmv_census_static(const uint8_t* L, const uint8_t* R, int64_t H, int64_t W, int D,
+                       int wsize, void* out, int dtype, int layout, void* stream);
+int64_t cbmv_census_static_max_pixels(void);
+
 /* nccNister (matchers.cpp:24-205): normalised cross-correlation cost
  * -(w^2 S - A_L A_R) C_L C_R, 1 on flat windows.  wsize odd, <= 15. */
 int cbmv_ncc(const uint8_t* L, const uint8_t* R, int64_t H, int64_t W, int D, int wsize,
