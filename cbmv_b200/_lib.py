@@ -63,6 +63,15 @@ SIGNATURES = {
     "cbmv_forest_info": [_vp, ctypes.POINTER(_int), ctypes.POINTER(_i64), ctypes.POINTER(_i64)],
     "cbmv_forest_destroy": [_vp],
     "cbmv_forest_predict": [_vp, _vp, _i64, _vp, _vp, _vp],
+    "cbmv_gemm_bf16": [_vp, _vp, _vp, _i64, _i64, _i64, _vp, _vp],
+    "cbmv_mlp_num_params": [],
+    "cbmv_mlp_create": [_int, ctypes.POINTER(_vp)],
+    "cbmv_mlp_destroy": [_vp],
+    "cbmv_mlp_set_params": [_vp, _vp],
+    "cbmv_mlp_get_params": [_vp, _vp],
+    "cbmv_mlp_train_step": [_vp, _vp, _vp, _flt, _flt, _vp, _vp],
+    "cbmv_mlp_gradients": [_vp, _vp, _vp, _vp, _vp, _vp],
+    "cbmv_mlp_status": [_vp, ctypes.POINTER(_int)],
     "cbmv_cross": [_vp, _i64, _i64, _int, _flt, _vp, _vp],
     "cbmv_sgm": [_vp, _vp, _vp, _i64, _i64, _int, _flt, _flt, _flt, _flt, _flt, _flt, _int, _vp, _vp],
     "cbmv_cbca": [_vp, _vp, _vp, _i64, _i64, _int, _int, _int, _vp, _vp],

@@ -188,6 +188,44 @@ int cbmv_forest_predict(const cbmv_forest* f, const float* X, int64_t N, double*
                         int32_t* leaves, void* stream);
 
 /* ------------------------------------------------------------------ */
+/* learned classifier (MLP surrogate of the random forest)             */
+/* ------------------------------------------------------------------ */
+
+/* C[M,N] (float32) = A[M,K] * B[N,K]^T on the tcgen05 tensor cores, A and B
+ * bfloat16 row-major (K contiguous), all 16-byte aligned; M % 128 == 0,
+ * N % 32 == 0, K % 64 == 0.  *status (device int) is set to 1 if a
+ * tensor-core completion wait timed out (the result is then invalid). */
+int cbmv_gemm_bf16(const uint16_t* A, const uint16_t* B, float* C, int64_t M, int64_t N, int64_t K,
+                   int* status, void* stream);
+
+/* The classifier network: 20 -> 128 -> 128 -> 64 -> 1, GELU (tanh form),
+ * sigmoid output = P(correct match); its matching cost is 1 - P.  Its
+ * parameter vector (float32, cbmv_mlp_num_params() values) is, in order:
+ * cap[20], mu[20], inv_sd[20] (input transform x' = (min(x,cap)-mu)*inv_sd),
+ * W1[128x20], b1[128], W2[128x128], b2[128], W3[64x128], b3[64], w4[64],
+ * b4.  Training runs on the tcgen05 GEMM above with bfloat16 activations and
+ * float32 accumulation, float32 master weights and Adam. */
+typedef struct cbmv_mlp cbmv_mlp;
+int cbmv_mlp_num_params(void);
+/* batch: samples per training step, a multiple of 128. */
+int cbmv_mlp_create(int batch, cbmv_mlp** out);
+int cbmv_mlp_destroy(cbmv_mlp* m);
+/* Parameters from / to HOST memory; setting them resets the optimiser. */
+int cbmv_mlp_set_params(cbmv_mlp* m, const float* host_params);
+int cbmv_mlp_get_params(const cbmv_mlp* m, float* host_params);
+/* One Adam step (betas 0.9/0.999, decoupled weight decay) on X float32
+ * [batch,20] raw features and y float32 [batch] labels (device memory);
+ * loss (device float, may be NULL) receives the mean binary cross-entropy. */
+int cbmv_mlp_train_step(cbmv_mlp* m, const float* X, const float* y, float lr, float weight_decay,
+                        float* loss, void* stream);
+/* Loss gradients in parameter order without the input transform
+ * (num_params - 60 floats, device memory), no update. */
+int cbmv_mlp_gradients(cbmv_mlp* m, const float* X, const float* y, float* grads, float* loss,
+                       void* stream);
+/* 0 while every tensor-core completion wait has succeeded. */
+int cbmv_mlp_status(const cbmv_mlp* m, int* status);
+
+/* ------------------------------------------------------------------ */
 /* cost optimisation -- post (post.cu), float32 on the device          */
 /* ------------------------------------------------------------------ */
 

@@ -1,0 +1,81 @@
+"""Float64 restatement of the classifier network's forward and backward
+pass (test infrastructure only): the checker of the tcgen05 training kernels.
+
+It follows cbmv_b200's network (include/cbmv.h, cbmv_mlp_*) and rounds to
+bfloat16 exactly where the device does -- the GEMM operands (normalised
+inputs, hidden activations, back-propagated deltas and the weights) -- and
+computes everything else in float64, so the device's remaining differences
+are float32 accumulation only.
+"""
+import numpy as np
+
+F = 20
+
+
+def bf16(x):
+    """Round float64/float32 values to bfloat16 (round to nearest even)."""
+    a = np.asarray(x, np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def gelu(x):
+    k0, k1 = 0.7978845608028654, 0.044715
+    t = np.tanh(k0 * (x + k1 * x ** 3))
+    d = 0.5 * (1 + t) + 0.5 * x * (1 - t * t) * k0 * (1 + 3 * k1 * x * x)
+    return 0.5 * x * (1 + t), d
+
+
+def unpack(vec):
+    v, o, out = np.asarray(vec, np.float64), 0, {}
+    for name, size in [("cap", F), ("mu", F), ("inv_sd", F), ("W1", 128 * F), ("b1", 128),
+                       ("W2", 128 * 128), ("b2", 128), ("W3", 64 * 128), ("b3", 64), ("w4", 64),
+                       ("b4", 1)]:
+        out[name] = v[o:o + size]
+        o += size
+    out["W1"] = out["W1"].reshape(128, F)
+    out["W2"] = out["W2"].reshape(128, 128)
+    out["W3"] = out["W3"].reshape(64, 128)
+    return out
+
+
+def forward(vec, X):
+    p = unpack(vec)
+    # the input transform in float32, as the device computes it
+    c32, m32, s32 = (np.float32(p[k]) for k in ("cap", "mu", "inv_sd"))
+    X0 = bf16((np.minimum(np.asarray(X, np.float32), c32) - m32) * s32)
+    S1 = X0 @ bf16(p["W1"]).T + p["b1"]
+    A1, d1 = gelu(S1)
+    S2 = bf16(A1) @ bf16(p["W2"]).T + p["b2"]
+    A2, d2 = gelu(S2)
+    S3 = bf16(A2) @ bf16(p["W3"]).T + p["b3"]
+    A3, d3 = gelu(S3)
+    z = A3 @ p["w4"] + p["b4"][0]
+    return dict(X0=X0, S1=S1, A1=A1, d1=d1, S2=S2, A2=A2, d2=d2, S3=S3, A3=A3, d3=d3, z=z, p=p)
+
+
+def loss_and_grads(vec, X, y):
+    """Mean BCE and its gradients in parameter order (input transform excluded)."""
+    f = forward(vec, X)
+    p, z = f["p"], f["z"]
+    y = np.asarray(y, np.float64)
+    B = z.shape[0]
+    prob = 1 / (1 + np.exp(-z))
+    loss = np.mean(np.maximum(z, 0) - z * y + np.log1p(np.exp(-np.abs(z))))
+    dz = (prob - y) / B
+    dw4 = f["A3"].T @ dz
+    db4 = dz.sum()
+    dS3 = dz[:, None] * p["w4"][None, :] * f["d3"]
+    db3 = dS3.sum(0)
+    dW3 = bf16(dS3).T @ bf16(f["A2"])
+    dA2 = bf16(dS3) @ bf16(p["W3"])
+    dS2 = dA2 * f["d2"]
+    db2 = dS2.sum(0)
+    dW2 = bf16(dS2).T @ bf16(f["A1"])
+    dA1 = bf16(dS2) @ bf16(p["W2"])
+    dS1 = dA1 * f["d1"]
+    db1 = dS1.sum(0)
+    dW1 = bf16(dS1).T @ f["X0"]
+    g = np.concatenate([dW1.ravel(), db1, dW2.ravel(), db2, dW3.ravel(), db3, dw4, [db4]])
+    return loss, g, prob
