@@ -224,6 +224,26 @@ __global__ void features_kernel(FeatVols fv, const double* __restrict__ stats, i
   }
 }
 
+__global__ void features_gather_kernel(FeatVols fv, const double* __restrict__ stats, int64_t H,
+                                       int64_t W, int D, const int64_t* __restrict__ idx, int64_t n,
+                                       float* __restrict__ out) {
+  const int64_t HW = H * W, N = HW * D;
+  GRID_STRIDE(i, n) {
+    int64_t t = idx[i];
+    t = t < 0 ? 0 : (t >= N ? N - 1 : t);  // indices are validated on the host; clamp anyway
+    const int64_t p = t / D;
+    const int d = (int)(t - p * D);
+    features_store(fv.v, stats, HW, D, p, p % W, d, out + i * 20, 1);
+  }
+}
+
+int launch_features_gather(const double* const* vols, const double* stats, int64_t H, int64_t W,
+                           int D, const int64_t* idx, int64_t n, float* out, cudaStream_t st) {
+  FeatVols fv = {{vols[0], vols[1], vols[2], vols[3]}};
+  features_gather_kernel<<<grid_for(n, kBlock), kBlock, 0, st>>>(fv, stats, H, W, D, idx, n, out);
+  return check_launch("features_gather");
+}
+
 int launch_feature_stats(const double* const* vols, int64_t H, int64_t W, int D, double* stats,
                          cudaStream_t st) {
   const int64_t warps = 2 * H * W;

@@ -77,6 +77,34 @@ __device__ __forceinline__ void features_store(const double* const* vols, const 
   }
 }
 
+// The features of matchers m0 and m0+1 only: f[2g + i] is feature group g
+// (0 cost, 1 ratio, 2 likelihood, 3 right ratio, 4 right likelihood) of
+// matcher m0 + i, i.e. reference column 4g + m0 + i.
+__device__ __forceinline__ void features_pair(const double* const* vols, const double* stats,
+                                              int64_t HW, int D, int64_t p, int64_t x, int d, int m0,
+                                              float* f) {
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    const int m = m0 + i;
+    const double c = vols[m][p * D + d];
+    float r, l;
+    f[i] = (float)c;
+    const double* sl = stats + ((int64_t)(m * 2 + 0) * HW + p) * 2;
+    confidences(c, sl[0], sl[1], kEps[m], kSigma[m], &r, &l);
+    f[2 + i] = r;
+    f[4 + i] = l;
+    if (x >= d) {
+      const double* sr = stats + ((int64_t)(m * 2 + 1) * HW + (p - d)) * 2;
+      confidences(c, sr[0], sr[1], kEps[m], kSigma[m], &r, &l);
+    } else {
+      r = 0.0f;
+      l = 0.0f;
+    }
+    f[6 + i] = r;
+    f[8 + i] = l;
+  }
+}
+
 struct FeatVols {
   const double* v[4];
 };

@@ -528,3 +528,236 @@ extern "C" int cbmv_mlp_status(const cbmv_mlp* n, int* status) {
   CBMV_CUDA(cudaMemcpy(status, n->status, sizeof(int), cudaMemcpyDeviceToHost));
   return CBMV_OK;
 }
+
+// ====================================================================
+// Fused inference: features of 128 consecutive (pixel, d) samples -> the
+// network on the tensor cores -> matching cost 1 - P(correct), float32.
+// Persistent CTAs of 256 threads, two per SM.  Shared memory: the bf16
+// weights (64 KB, loaded once) and one activation tile A [128 x 128] that
+// holds in turn the input tile X0 [128 x 64] (its first atom), the first
+// and the second hidden layer; tensor memory: one 128-column accumulator
+// reused by the three layers.  Every reuse is ordered by the wait on the
+// MMA that last read the buffer.
+// ====================================================================
+#include "features.cuh"
+
+namespace cbmv {
+namespace {
+
+constexpr int kMlpThreads = 256;
+constexpr size_t kSmW1 = 128 * 128, kSmW2 = 2 * 128 * 128, kSmW3 = 2 * 64 * 128;
+constexpr size_t kSmA = 2 * 128 * 128;
+constexpr size_t kSmMlp = 1024 + kSmW1 + kSmW2 + kSmW3 + kSmA;
+
+__device__ __forceinline__ float gelu_fast(float x) {
+  const float k0 = 0.7978845608028654f, k1 = 0.044715f;
+  const float u = k0 * (x + k1 * x * x * x);
+  float t;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+  return 0.5f * x * (1.0f + t);
+}
+
+// bf16 weight matrix [R x K] (row-major, K contiguous) -> SW128 tile in smem
+__device__ void stage_weights(const uint16_t* __restrict__ g, int R, int K, unsigned char* s) {
+  for (int q = threadIdx.x; q < R * (K / 8); q += blockDim.x) {
+    const int r = q / (K / 8), c = q % (K / 8);
+    *reinterpret_cast<uint4*>(s + umma::sw128_offset(R, r, c * 8)) =
+        *reinterpret_cast<const uint4*>(g + (size_t)r * K + c * 8);
+  }
+}
+
+// 16 accumulator columns -> +bias -> GELU -> bf16 into the A tile
+__device__ __forceinline__ void epi_store(const float* v, const float* bias, int c0, int row,
+                                          unsigned char* sA) {
+  uint32_t packed[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const float a = gelu_fast(v[2 * i] + bias[c0 + 2 * i]);
+    const float b = gelu_fast(v[2 * i + 1] + bias[c0 + 2 * i + 1]);
+    packed[i] = (uint32_t)to_bf16(a) | ((uint32_t)to_bf16(b) << 16);
+  }
+  // 16 consecutive k = two 16-byte chunks of the swizzled row
+  *reinterpret_cast<uint4*>(sA + umma::sw128_offset(128, row, c0)) =
+      make_uint4(packed[0], packed[1], packed[2], packed[3]);
+  *reinterpret_cast<uint4*>(sA + umma::sw128_offset(128, row, c0 + 8)) =
+      make_uint4(packed[4], packed[5], packed[6], packed[7]);
+}
+
+__global__ void __launch_bounds__(kMlpThreads, 2)
+    features_mlp_kernel(FeatVols fv, const double* __restrict__ stats, int64_t H, int64_t W, int D,
+                        const float* __restrict__ P, const uint16_t* __restrict__ W1b,
+                        const uint16_t* __restrict__ W2b, const uint16_t* __restrict__ W3b,
+                        float* __restrict__ prob0, int* __restrict__ status) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* sW1 = base;
+  unsigned char* sW2 = sW1 + kSmW1;
+  unsigned char* sW3 = sW2 + kSmW2;
+  unsigned char* sA = sW3 + kSmW3;
+  unsigned char* sX0 = sA;  // the input tile is the first atom of A
+  __shared__ float sP[kNParams - kOffW4 + kNormN + kH1 + kH2 + kH3];
+  __shared__ float partial[2][128];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tmem_base;
+  float* s_norm = sP;                 // cap, mu, inv_sd
+  float* s_b1 = s_norm + kNormN;
+  float* s_b2 = s_b1 + kH1;
+  float* s_b3 = s_b2 + kH2;
+  float* s_w4 = s_b3 + kH3;           // w4[64], b4
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (warp == 0) umma::tmem_alloc(&tmem_base, 128);
+  if (tid == 0) umma::mbar_init(&bar, 1);
+  stage_weights(W1b, 128, 64, sW1);
+  stage_weights(W2b, 128, 128, sW2);
+  stage_weights(W3b, 64, 128, sW3);
+  for (int i = tid; i < kNormN; i += kMlpThreads) s_norm[i] = P[i];
+  for (int i = tid; i < kH1; i += kMlpThreads) s_b1[i] = P[kOffB1 + i];
+  for (int i = tid; i < kH2; i += kMlpThreads) s_b2[i] = P[kOffB2 + i];
+  for (int i = tid; i < kH3; i += kMlpThreads) s_b3[i] = P[kOffB3 + i];
+  for (int i = tid; i < kH3 + 1; i += kMlpThreads) s_w4[i] = P[kOffW4 + i];
+  umma::fence_async_smem();
+  umma::tc_fence_before();
+  __syncthreads();
+  umma::tc_fence_after();
+  const uint32_t tmem = tmem_base;
+  const uint32_t id128 = umma::idesc_bf16(128, 128), id64 = umma::idesc_bf16(128, 64);
+  const uint64_t dX0 = umma::sw128_desc(umma::smem_u32(sX0));
+  const uint64_t dA0 = umma::sw128_desc(umma::smem_u32(sA)), dA1 = umma::sw128_desc(umma::smem_u32(sA + 128 * 128));
+  const uint64_t dW1 = umma::sw128_desc(umma::smem_u32(sW1));
+  const uint64_t dW20 = umma::sw128_desc(umma::smem_u32(sW2)), dW21 = umma::sw128_desc(umma::smem_u32(sW2 + 128 * 128));
+  const uint64_t dW30 = umma::sw128_desc(umma::smem_u32(sW3)), dW31 = umma::sw128_desc(umma::smem_u32(sW3 + 64 * 128));
+
+  const int64_t HW = H * W, N = HW * D;
+  const int64_t tiles = (N + 127) / 128;
+  const int quad = warp & 3, half = warp >> 2;
+  const int row = quad * 32 + lane;  // accumulator row this thread reads
+  const uint32_t trow = tmem + ((uint32_t)(quad * 32) << 16);
+  uint32_t phase = 0;
+  bool ok = true;
+
+  for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    // 1. features of sample (tile*128 + s), matchers {2h, 2h+1} by thread half h
+    {
+      const int s = tid & 127, h = tid >> 7;
+      int64_t t = tile * 128 + s;
+      if (t >= N) t = N - 1;
+      const int64_t p = t / D;
+      const int d = (int)(t - p * D);
+      const int64_t x = p % W;
+      float f[10];
+      features_pair(fv.v, stats, HW, D, p, x, d, 2 * h, f);
+#pragma unroll
+      for (int j = 0; j < 10; j++) {
+        const int k = (j >> 1) * 4 + 2 * h + (j & 1);  // feature column
+        const float v = (fminf(f[j], s_norm[k]) - s_norm[kF + k]) * s_norm[2 * kF + k];
+        *reinterpret_cast<uint16_t*>(sX0 + umma::sw128_offset(128, s, k)) = to_bf16(v);
+      }
+      // zero padding, columns 20..63 (the previous tile left activations here)
+      if (h == 0) {
+#pragma unroll
+        for (int c = 3; c < 8; c++)
+          *reinterpret_cast<uint4*>(sX0 + umma::sw128_offset(128, s, c * 8)) = make_uint4(0, 0, 0, 0);
+      } else {
+#pragma unroll
+        for (int k = 20; k < 24; k++) *reinterpret_cast<uint16_t*>(sX0 + umma::sw128_offset(128, s, k)) = 0;
+      }
+    }
+    umma::fence_async_smem();
+    umma::tc_fence_before();
+    __syncthreads();
+    umma::tc_fence_after();
+    // 2. layer 1: D = X0 W1^T (K = 64)
+    if (tid == 0) {
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tmem, dX0 + 2 * kk, dW1 + 2 * kk, id128, kk > 0);
+      umma::mma_commit(&bar);
+    }
+    ok = umma::mbar_wait(&bar, phase, kWaitLimit);
+    phase ^= 1u;
+    umma::tc_fence_after();
+    if (!ok) break;
+    for (int c0 = half * 64; c0 < half * 64 + 64; c0 += 16) {
+      float v[16];
+      umma::tmem_ld16(trow + c0, v);
+      epi_store(v, s_b1, c0, row, sA);
+    }
+    umma::fence_async_smem();
+    umma::tc_fence_before();
+    __syncthreads();
+    umma::tc_fence_after();
+    // 3. layer 2: D = A1 W2^T (K = 128, two atoms)
+    if (tid == 0) {
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tmem, dA0 + 2 * kk, dW20 + 2 * kk, id128, kk > 0);
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tmem, dA1 + 2 * kk, dW21 + 2 * kk, id128, true);
+      umma::mma_commit(&bar);
+    }
+    ok = umma::mbar_wait(&bar, phase, kWaitLimit);
+    phase ^= 1u;
+    umma::tc_fence_after();
+    if (!ok) break;
+    for (int c0 = half * 64; c0 < half * 64 + 64; c0 += 16) {
+      float v[16];
+      umma::tmem_ld16(trow + c0, v);
+      epi_store(v, s_b2, c0, row, sA);
+    }
+    umma::fence_async_smem();
+    umma::tc_fence_before();
+    __syncthreads();
+    umma::tc_fence_after();
+    // 4. layer 3: D = A2 W3^T (N = 64)
+    if (tid == 0) {
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tmem, dA0 + 2 * kk, dW30 + 2 * kk, id64, kk > 0);
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tmem, dA1 + 2 * kk, dW31 + 2 * kk, id64, true);
+      umma::mma_commit(&bar);
+    }
+    ok = umma::mbar_wait(&bar, phase, kWaitLimit);
+    phase ^= 1u;
+    umma::tc_fence_after();
+    if (!ok) break;
+    // 5. output layer: z = gelu(D + b3) . w4 + b4; cost = 1 - sigmoid(z)
+    float acc = 0.0f;
+    for (int c0 = half * 32; c0 < half * 32 + 32; c0 += 16) {
+      float v[16];
+      umma::tmem_ld16(trow + c0, v);
+#pragma unroll
+      for (int i = 0; i < 16; i++) acc += gelu_fast(v[i] + s_b3[c0 + i]) * s_w4[c0 + i];
+    }
+    partial[half][row] = acc;
+    umma::tc_fence_before();
+    __syncthreads();
+    if (half == 0) {
+      const int64_t t = tile * 128 + row;
+      const float z = (partial[0][row] + partial[1][row]) + s_w4[kH3];
+      if (t < N) prob0[t] = 1.0f / (1.0f + __expf(z));
+    }
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(status, 1);
+    umma::mbar_wait(&bar, phase ^ 1u, kWaitLimit);
+  }
+  umma::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, 128);
+}
+
+}  // namespace
+
+int launch_features_mlp(const double* const* vols, const double* stats, int64_t H, int64_t W, int D,
+                        const cbmv_mlp* m, float* prob0, cudaStream_t st) {
+  int dev = 0, sms = 0;
+  CBMV_CUDA(cudaGetDevice(&dev));
+  CBMV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  CBMV_CUDA(cudaFuncSetAttribute(features_mlp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kSmMlp));
+  FeatVols fv = {{vols[0], vols[1], vols[2], vols[3]}};
+  features_mlp_kernel<<<2 * sms, kMlpThreads, kSmMlp, st>>>(fv, stats, H, W, D, m->P, m->W1b, m->W2b,
+                                                           m->W3b, prob0, m->status);
+  return check_launch("features_mlp");
+}
+
+}  // namespace cbmv

@@ -259,26 +259,19 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
   return CBMV_OK;
 }
 
-extern "C" int cbmv_run_rf(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params* p,
-                           const uint8_t* L, const uint8_t* R, int64_t H, int64_t W, int D,
-                           float* disp, float* prob0) {
-  CBMV_REQUIRE(c && f && L && R && disp, CBMV_EINVAL, "null pointer argument");
-  cbmv_params def;
-  if (!p) {
-    cbmv_params_default(&def);
-    p = &def;
-  }
+// Steps 1-3 of the header comment: the four float64 cost volumes and their
+// per-pixel statistics in the context's workspace.
+static int run_front(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
+                     int64_t H, int64_t W, int D, Work* wout) {
   RC(check_params(p));
   CBMV_REQUIRE(H > p->censw && W > p->censw, CBMV_EINVAL, "image %lldx%lld smaller than the census window",
                (long long)W, (long long)H);
   CBMV_REQUIRE(H <= 65535 && D >= 1 && D <= 1024, CBMV_ERANGE, "H must be <= 65535 and D in 1..1024");
-  CBMV_REQUIRE(forest_view(f)->n_features == 20, CBMV_EINVAL, "the forest must take the 20 CBMV features");
   size_t bytes = 0;
   carve(nullptr, H, W, D, &bytes);
   RC(ensure_workspace(c, bytes));
   Work w = carve(c->ws, H, W, D, &bytes);
   cudaStream_t st = c->stream;
-
   CBMV_CUDA(cudaEventRecord(c->ev[0], st));
   RC(launch_census_desc(L, H, W, p->censw, w.descL, st));
   RC(launch_census_desc(R, H, W, p->censw, w.descR, st));
@@ -296,6 +289,27 @@ extern "C" int cbmv_run_rf(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params*
   const double* vols[4] = {w.vol[0], w.vol[1], w.vol[2], w.vol[3]};
   RC(launch_feature_stats(vols, H, W, D, w.stats, st));
   CBMV_CUDA(cudaEventRecord(c->ev[2], st));
+  *wout = w;
+  return CBMV_OK;
+}
+
+static const cbmv_params* params_or_default(const cbmv_params* p, cbmv_params* def) {
+  if (p) return p;
+  cbmv_params_default(def);
+  return def;
+}
+
+extern "C" int cbmv_run_rf(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params* p,
+                           const uint8_t* L, const uint8_t* R, int64_t H, int64_t W, int D,
+                           float* disp, float* prob0) {
+  CBMV_REQUIRE(c && f && L && R && disp, CBMV_EINVAL, "null pointer argument");
+  cbmv_params def;
+  p = params_or_default(p, &def);
+  CBMV_REQUIRE(forest_view(f)->n_features == 20, CBMV_EINVAL, "the forest must take the 20 CBMV features");
+  Work w;
+  RC(run_front(c, p, L, R, H, W, D, &w));
+  cudaStream_t st = c->stream;
+  const double* vols[4] = {w.vol[0], w.vol[1], w.vol[2], w.vol[3]};
   RC(launch_features_rf(vols, w.stats, H, W, D, f, w.volA, st));
   if (prob0)
     CBMV_CUDA(cudaMemcpyAsync(prob0, w.volA, sizeof(float) * H * W * D, cudaMemcpyDeviceToDevice, st));
@@ -303,4 +317,35 @@ extern "C" int cbmv_run_rf(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params*
   RC(run_post(c, p, L, R, H, W, D, w, disp));
   CBMV_CUDA(cudaEventRecord(c->ev[4], st));
   return CBMV_OK;
+}
+
+extern "C" int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p, const uint8_t* L,
+                            const uint8_t* R, int64_t H, int64_t W, int D, float* disp, float* prob0) {
+  CBMV_REQUIRE(c && m && L && R && disp, CBMV_EINVAL, "null pointer argument");
+  cbmv_params def;
+  p = params_or_default(p, &def);
+  Work w;
+  RC(run_front(c, p, L, R, H, W, D, &w));
+  cudaStream_t st = c->stream;
+  const double* vols[4] = {w.vol[0], w.vol[1], w.vol[2], w.vol[3]};
+  RC(launch_features_mlp(vols, w.stats, H, W, D, m, w.volA, st));
+  if (prob0)
+    CBMV_CUDA(cudaMemcpyAsync(prob0, w.volA, sizeof(float) * H * W * D, cudaMemcpyDeviceToDevice, st));
+  CBMV_CUDA(cudaEventRecord(c->ev[3], st));
+  RC(run_post(c, p, L, R, H, W, D, w, disp));
+  CBMV_CUDA(cudaEventRecord(c->ev[4], st));
+  return CBMV_OK;
+}
+
+extern "C" int cbmv_ctx_features_at(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L,
+                                    const uint8_t* R, int64_t H, int64_t W, int D, const int64_t* idx,
+                                    int64_t n, float* out) {
+  CBMV_REQUIRE(c && L && R && idx && out, CBMV_EINVAL, "null pointer argument");
+  CBMV_REQUIRE(n > 0, CBMV_EINVAL, "n must be positive");
+  cbmv_params def;
+  p = params_or_default(p, &def);
+  Work w;
+  RC(run_front(c, p, L, R, H, W, D, &w));
+  const double* vols[4] = {w.vol[0], w.vol[1], w.vol[2], w.vol[3]};
+  return launch_features_gather(vols, w.stats, H, W, D, idx, n, out, c->stream);
 }

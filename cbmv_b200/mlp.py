@@ -126,3 +126,34 @@ class MlpTrainer:
             self.close()
         except Exception:
             pass
+
+
+class GpuMlp:
+    """A trained network uploaded for inference (cbmv_run_mlp)."""
+
+    def __init__(self, params):
+        _dev.require_cuda()
+        h = ctypes.c_void_p()
+        _lib.call("cbmv_mlp_create", 128, ctypes.byref(h))
+        self.h = h
+        _lib.call("cbmv_mlp_set_params", self.h, params.vec.ctypes.data)
+
+    @classmethod
+    def load(cls, path):
+        return cls(MlpParams.load(path))
+
+    def status(self):
+        s = ctypes.c_int()
+        _lib.call("cbmv_mlp_status", self.h, ctypes.byref(s))
+        return s.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lib().cbmv_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

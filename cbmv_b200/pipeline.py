@@ -44,6 +44,31 @@ class StereoPipeline:
                   prob_out.data_ptr() if prob_out is not None else None)
         return _dev.result(disp, host)
 
+    def run_mlp(self, net, left, right, ndisp, disp_out=None, prob_out=None):
+        """The same path with the learned classifier (cbmv_b200.mlp.GpuMlp)."""
+        l, host = _dev.to_device(left, np.uint8)
+        r, _ = _dev.to_device(right, np.uint8)
+        H, W = l.shape
+        disp = disp_out if disp_out is not None else _dev.empty((H, W), np.float32)
+        _lib.call("cbmv_run_mlp", self.ctx, net.h, ctypes.byref(self.params), l.data_ptr(), r.data_ptr(),
+                  H, W, int(ndisp), disp.data_ptr(),
+                  prob_out.data_ptr() if prob_out is not None else None)
+        return _dev.result(disp, host)
+
+    def features_at(self, left, right, ndisp, idx):
+        """20 float32 features of the samples idx = (y*W + x)*D + d (device tensor [n,20])."""
+        import torch
+        l, _ = _dev.to_device(left, np.uint8)
+        r, _ = _dev.to_device(right, np.uint8)
+        H, W = l.shape
+        ix, _ = _dev.to_device(idx, np.int64)
+        if ix.numel() and (int(ix.min()) < 0 or int(ix.max()) >= H * W * int(ndisp)):
+            raise ValueError("sample index outside the H*W*D volume")
+        out = torch.empty((ix.numel(), 20), dtype=torch.float32, device="cuda")
+        _lib.call("cbmv_ctx_features_at", self.ctx, ctypes.byref(self.params), l.data_ptr(), r.data_ptr(),
+                  H, W, int(ndisp), ix.data_ptr(), ix.numel(), out.data_ptr())
+        return out
+
     def timings(self):
         """Stage times of the last run in ms: matchers, feature statistics,
         features+classifier, post, total (after a synchronize)."""

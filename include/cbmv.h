@@ -304,6 +304,19 @@ int cbmv_ctx_destroy(cbmv_ctx* c);
 int cbmv_run_rf(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params* p, const uint8_t* L,
                 const uint8_t* R, int64_t H, int64_t W, int D, float* disp, float* prob0);
 
+/* The same path with the learned classifier in place of the forest: the
+ * network's matching cost 1 - P(correct) feeds the post-processing.  The
+ * features and the network run fused on the tensor cores (no feature matrix
+ * in HBM).  Tensor-core wait timeouts are reported by cbmv_mlp_status. */
+int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p, const uint8_t* L,
+                 const uint8_t* R, int64_t H, int64_t W, int D, float* disp, float* prob0);
+
+/* Training-sample emission (the GPU counterpart of train.py:100-273): the
+ * 20 float32 features of the samples idx[i] = (y*W + x)*D + d of the pair
+ * (L, R); idx int64 [n], out float32 [n,20], device memory. */
+int cbmv_ctx_features_at(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
+                         int64_t H, int64_t W, int D, const int64_t* idx, int64_t n, float* out);
+
 /* Stage timings of the last cbmv_run_* call in milliseconds (CUDA events):
  * [0] matchers, [1] feature statistics, [2] features+classifier, [3] post,
  * [4] total.  Valid after the stream has been synchronised. */

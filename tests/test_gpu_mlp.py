@@ -74,3 +74,45 @@ def test_mlp_training_reduces_loss(gpu):
         losses.append(tr.step(Xt[s:s + 1024], yt[s:s + 1024], 3e-3).item())
     assert tr.status() == 0
     assert np.mean(losses[-8:]) < 0.5 * np.mean(losses[:4]), losses
+
+
+def test_fused_inference_matches_oracle_forward(gpu, small_pair):
+    """cbmv_run_mlp's matching cost (features + three tcgen05 layers fused,
+    tanh.approx GELU) against the float64 network on the same features."""
+    from cbmv_b200.mlp import GpuMlp, MlpParams, input_stats
+    from cbmv_b200.pipeline import StereoPipeline
+    from oracle import mlp_ref
+    L, R, _, _ = small_pair
+    H, W = L.shape
+    D = 24
+    pipe = StereoPipeline()
+    idx = torch.arange(H * W * D, device="cuda")
+    X = pipe.features_at(L, R, D, idx).cpu().numpy()
+    cap, mu, sd = input_stats(X)
+    net = MlpParams.init(5, cap, mu, sd)
+    v = net.views()
+    v["b1"][:] = 0.05
+    v["b3"][:] = -0.1
+    v["b4"][:] = 0.2
+    g = GpuMlp(net)
+    prob = torch.empty((H, W, D), device="cuda")
+    pipe.run_mlp(g, L, R, D, prob_out=prob)
+    torch.cuda.synchronize()
+    assert g.status() == 0
+    f = mlp_ref.forward(net.vec, X)
+    want = 1.0 / (1.0 + np.exp(f["z"]))
+    got = prob.cpu().numpy().reshape(-1)
+    assert np.abs(got - want).max() < 5e-3, np.abs(got - want).max()
+    assert np.mean(np.abs(got - want)) < 5e-4
+
+
+def test_training_samples_follow_labels(gpu):
+    from cbmv_b200 import synth
+    from cbmv_b200.train_mlp import pick_samples
+    L, R, gt, nonocc = synth.make_pair(seed=3, width=80, height=50, ndisp=24, planes=3, dmin=2, dmax=18)
+    idx, lab = pick_samples(gt, nonocc, 500, 1, ndisp=24)
+    d = idx % 24
+    g = gt.reshape(-1)[idx // 24]
+    assert np.all(np.abs(d[lab == 1] - g[lab == 1]) <= 1)
+    assert np.all(np.abs(d[lab == 0] - g[lab == 0]) > 1)
+    assert abs(lab.mean() - 0.5) < 0.02
