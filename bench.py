@@ -2,12 +2,15 @@
 
 Workload: one synthetic rectified pair at 694x554, D=128 (seeded, the
 reference's README-scale Middlebury size), 49,212,928 (pixel, d) units.  A
-step is the whole test path for that pair: four matchers, 20 features,
-random forest (50 trees, depth <= 20, trained on 30 seeded pairs, see
-tests/golden/make_forest.py), then the MC-CNN `_mem` post-processing to the
-disparity map.  With N GPUs (torchrun), every rank processes its own pair
-(seed = rank): weak scaling by independent pairs, no collective on the data
-path.
+step is the whole test path for that pair: four matchers, 20 features, the
+per-(pixel,d) classifier, then the MC-CNN `_mem` post-processing to the
+disparity map.  Both classifiers are timed: the random forest (50 trees,
+depth <= 20, trained on 30 seeded pairs, tests/golden/make_forest.py) and
+the bf16 MLP (tests/golden/mlp_694x554.npz, cbmv_b200/train_mlp.py).  The
+RF judges the MLP: both run on 20 held-out seeded pairs and the MLP is the
+headline only when its bad-2.0 is within 0.5 percentage points of the RF's.
+With N GPUs (torchrun), every rank processes its own pair (seed = rank):
+weak scaling by independent pairs, no collective on the data path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cbmv|reference]
 
@@ -33,10 +36,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FOREST = os.path.join(ROOT, "tests", "golden", "forest_694x554.npz")
+MLP = os.path.join(ROOT, "tests", "golden", "mlp_694x554.npz")
 W0, H0, D0 = 694, 554, 128
 UNITS = W0 * H0 * D0
-METRIC = "pixel·disparities/s end-to-end at 694×554, D=128 (RF classifier)"
+METRIC = "pixel·disparities/s end-to-end at 694×554, D=128; MLP vs RF at matched bad-2.0"
 BYTES_PER_UNIT_FUSED = 4.0  # algorithmic HBM bytes of matchers+features+classifier per (p,d)
+# dense flops of the 20-128-128-64-1 network per (p,d): 2*(20*128 + 128*128 + 128*64 + 64)
+FLOPS_PER_UNIT_MLP = 2.0 * (20 * 128 + 128 * 128 + 128 * 64 + 64)
 
 
 def peaks():
@@ -45,6 +51,17 @@ def peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def tensor_peak():
+    """Dense bf16 TFLOP/s: the burst figure (the classifier kernel runs for
+    milliseconds inside a step, not a seconds-long loop)."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]), "measured (burst)"
+    return 1590.0, "fallback (burst)"
 
 
 class Clocks:
@@ -130,11 +147,51 @@ def barrier(ws):
     torch.cuda.synchronize()
 
 
+def _time_path(run, a, ws, flush, st, pipe):
+    """Device time of `a.steps` runs (L2 flushed before each) and the mean
+    stage times; returns (ms, stage)."""
+    import torch
+    for _ in range(a.warmup):
+        run()
+    barrier(ws)
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    stage = {"matchers": 0.0, "stats": 0.0, "classify": 0.0, "post": 0.0, "total": 0.0}
+    for k in range(a.steps):
+        flush.fill_(float(k))
+        ev0[k].record(st)
+        run()
+        ev1[k].record(st)
+        st.synchronize()
+        for kk, v in pipe.timings().items():
+            stage[kk] += v
+    barrier(ws)
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1)) / a.steps
+    return reduce_max(ms, ws), {k: v / a.steps for k, v in stage.items()}
+
+
+def _time_e2e(run_host, a, ws, flush, st):
+    """Wall time of the public call with pinned host images (H2D, whole
+    path, D2H of the disparity map inside the timed region)."""
+    for _ in range(2):
+        run_host()
+    barrier(ws)
+    tot = 0.0
+    for k in range(a.steps):
+        flush.fill_(float(k))
+        st.synchronize()
+        t0 = time.perf_counter()
+        run_host()
+        tot += (time.perf_counter() - t0) * 1e3
+    return reduce_max(tot / a.steps, ws)
+
+
 def run_cbmv(a, ws, rank, local):
     import torch
-    from cbmv_b200 import synth
+    from cbmv_b200 import evaluate, synth
     from cbmv_b200.forest import FlatForest
     from cbmv_b200.forest_gpu import GpuForest
+    from cbmv_b200.mlp import GpuMlp
     from cbmv_b200.pipeline import StereoPipeline
 
     if not os.path.exists(a.forest):
@@ -147,86 +204,104 @@ def run_cbmv(a, ws, rank, local):
     units = L.shape[0] * W0 * D0
     flat = FlatForest.load(a.forest)
     gf = GpuForest(flat)
+    net = GpuMlp.load(a.mlp) if os.path.exists(a.mlp) else None
     pipe = StereoPipeline(gf)
     l = torch.from_numpy(L).to(dev)
     r = torch.from_numpy(R).to(dev)
     disp = torch.empty(L.shape, dtype=torch.float32, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > L2
     st = torch.cuda.current_stream()
+    Lh = torch.from_numpy(L).pin_memory()
+    Rh = torch.from_numpy(R).pin_memory()
 
-    for _ in range(a.warmup):
-        pipe.run_rf(l, r, D0, disp_out=disp)
-    barrier(ws)
-    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
-    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
-    stage = {"matchers": 0.0, "stats": 0.0, "classify": 0.0, "post": 0.0, "total": 0.0}
+    if a.classifier == "mlp" and net is None:
+        raise SystemExit("MLP parameters missing: %s (python -m cbmv_b200.train_mlp)" % a.mlp)
+    paths = {}
+    if a.classifier in ("both", "rf"):
+        paths["rf"] = (lambda: pipe.run_rf(l, r, D0, disp_out=disp), lambda: pipe.run_rf(Lh, Rh, D0))
+    if a.classifier in ("both", "mlp") and net is not None:
+        paths["mlp"] = (lambda: pipe.run_mlp(net, l, r, D0, disp_out=disp),
+                        lambda: pipe.run_mlp(net, Lh, Rh, D0))
+    res = {}
     with Clocks(local) as clk:
-        for k in range(a.steps):
-            flush.fill_(float(k))
-            ev0[k].record(st)
-            pipe.run_rf(l, r, D0, disp_out=disp)
-            ev1[k].record(st)
-            st.synchronize()
-            for kk, v in pipe.timings().items():
-                stage[kk] += v
-        barrier(ws)
-    ms = sum(e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1)) / a.steps
-    ms = reduce_max(ms, ws)
-    stage = {k: v / a.steps for k, v in stage.items()}
-    value = units * ws / (ms / 1e3)
+        for name, (run_dev, run_host) in paths.items():
+            ms, stage = _time_path(run_dev, a, ws, flush, st, pipe)
+            d = disp.cpu().numpy()
+            res[name] = {"ms": ms, "stage_ms": stage, "bad2_nonocc": evaluate.bad_x(d, gt, nonocc)}
+    for name, (_, run_host) in paths.items():
+        res[name]["e2e_ms"] = _time_e2e(run_host, a, ws, flush, st)
+    if net is not None and net.status() != 0:
+        raise RuntimeError("a tensor-core wait of the MLP kernel timed out")
+
+    # held-out accuracy: the RF judges the MLP (bad-2.0 on 20 seeded pairs)
+    matched = None
+    if net is not None and a.classifier == "both" and not a.no_eval and rank == 0:
+        ev = evaluate.compare_loaded(pipe, net, evaluate.HELD_OUT, D0)
+        matched = {"seeds": "%d-%d" % (ev["seeds"][0], ev["seeds"][-1]), "bad2_rf": ev["bad2_rf"],
+                   "bad2_mlp": ev["bad2_mlp"], "delta_pp": 100 * (ev["bad2_mlp"] - ev["bad2_rf"]),
+                   "within_0.5pp": bool(ev["bad2_mlp"] - ev["bad2_rf"] <= 0.005)}
+    # the headline classifier: the MLP where it matches the RF's bad-2.0, else the RF
+    if a.classifier == "both":
+        head = "mlp" if matched is not None and matched["within_0.5pp"] else "rf"
+    else:
+        head = a.classifier
+    h = res[head]
+
     # kernel launches per step (pipeline.cu): 8 per-pixel terms, 4 cost volumes,
-    # 4 feature statistics, 1 features+forest, post: 4 normalisation, 2 cross,
+    # 4 feature statistics, 1 features+classifier, post: 4 normalisation, 2 cross,
     # 4 x sgm_i SGM directions, cbca_i2 CBCA, WTA+subpixel, median, mean2d
     launches = 8 + 4 + 4 + 1 + 4 + 2 + 4 * 2 + 4 + 3
 
-    # end to end through the public call with pinned host buffers
-    Lh = torch.from_numpy(L).pin_memory()
-    Rh = torch.from_numpy(R).pin_memory()
-    for _ in range(2):
-        pipe.run_rf(Lh, Rh, D0)
-    barrier(ws)
-    e2e_ms = 0.0
-    for k in range(a.steps):
-        flush.fill_(float(k))
-        st.synchronize()
-        t0 = time.perf_counter()
-        out = pipe.run_rf(Lh, Rh, D0)  # H2D of both images, the whole path, D2H of the map
-        e2e_ms += (time.perf_counter() - t0) * 1e3
-        assert out.shape == L.shape
-    e2e_ms = reduce_max(e2e_ms / a.steps, ws)
-
-    # accuracy of this pair (bad-2.0 on non-occluded pixels)
-    d = disp.cpu().numpy()
-    bad2 = float(np.mean(np.abs(d[nonocc] - gt[nonocc]) > 2.0))
-
-    peak, peak_kind = peaks()
-    t_cls = stage["classify"]
-    achieved = BYTES_PER_UNIT_FUSED * units / (t_cls / 1e3) / 1e9
-    traffic = None
+    hbm, hbm_kind = peaks()
+    tc, tc_kind = tensor_peak()
+    traffic = {}
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get("features_rf_kernel")
+        traffic = json.load(open(tp))
+    if "rf" in res:
+        rf_achieved = BYTES_PER_UNIT_FUSED * units / (res["rf"]["stage_ms"]["classify"] / 1e3) / 1e9
+        res["rf"]["roofline"] = {
+            "bound": "hbm", "kernel": "features_rf_kernel", "achieved": rf_achieved, "peak": hbm,
+            "unit": "GB/s", "frac": rf_achieved / hbm, "traffic": traffic.get("features_rf_kernel"),
+            "peak_kind": hbm_kind, "bytes_per_unit": BYTES_PER_UNIT_FUSED,
+            "note": "the forest walk is bound by dependent node-visit gathers, not HBM"}
+    if "mlp" in res:
+        mlp_tflops = FLOPS_PER_UNIT_MLP * units / (res["mlp"]["stage_ms"]["classify"] / 1e3) / 1e12
+        roof_mlp = {"bound": "tensor", "kernel": "features_mlp_kernel", "achieved": mlp_tflops,
+                    "peak": tc, "unit": "TFLOP/s", "frac": mlp_tflops / tc,
+                    "traffic": traffic.get("features_mlp_kernel"), "peak_kind": tc_kind,
+                    "flops_per_unit": FLOPS_PER_UNIT_MLP,
+                    "note": "dense flops of 20-128-128-64-1 per (pixel,d); the kernel also builds "
+                            "the 20 features from the four f64 cost volumes (%.0f B/unit)"
+                            % BYTES_PER_UNIT_FUSED}
+        res["mlp"]["roofline"] = roof_mlp
+    roof = res[head]["roofline"]
+
+    classifier = {"rf": "random_forest (50 trees, depth<=20)",
+                  "mlp": "bf16 MLP 20-128-128-64-1 on tcgen05 (RF as judge)"}[head]
     line = {
-        "metric": METRIC, "value": value, "unit": "pixel·disparities/s", "n_gpus": ws,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32",
+        "metric": METRIC, "value": units * ws / (h["ms"] / 1e3), "unit": "pixel·disparities/s",
+        "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": h["ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16/f32" if head == "mlp" else "f64/f32",
         "data": "synthetic (seeded 694x554 pair per rank; L2 flushed between steps)",
-        "config": {"workload": "694x554 D=128 test path: 4 matchers, 20 features, RF 50 trees "
-                               "depth<=20, MC-CNN _mem post", "width": W0, "height": int(L.shape[0]), "ndisp": D0,
-                   "units_per_pair": units, "classifier": "random_forest",
-                   "forest_nodes": int(flat.n_nodes), "l2": "flushed (256 MB write) between steps",
+        "config": {"workload": "694x554 D=128 test path: 4 matchers, 20 features, %s, MC-CNN _mem post"
+                               % classifier, "width": W0, "height": int(L.shape[0]), "ndisp": D0,
+                   "units_per_pair": units, "classifier": head, "forest_nodes": int(flat.n_nodes),
+                   "l2": "flushed (256 MB write) between steps",
                    "parallelism": "replica per GPU, one pair per rank"},
-        "stage_ms": stage,
-        "bad2_nonocc": bad2,
+        "stage_ms": h["stage_ms"],
+        "bad2_nonocc": h["bad2_nonocc"],
         "gpu_launches": launches * a.steps,
-        "e2e": {"value": units * ws / (e2e_ms / 1e3), "unit": "pixel·disparities/s",
-                "ms_per_step": e2e_ms, "h2d_bytes_per_step": 2 * L.size,
+        "e2e": {"value": units * ws / (h["e2e_ms"] / 1e3), "unit": "pixel·disparities/s",
+                "ms_per_step": h["e2e_ms"], "h2d_bytes_per_step": 2 * L.size,
                 "d2h_bytes_per_step": 4 * L.size},
-        "roofline": {"bound": "hbm", "kernel": "features_rf_kernel", "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                     "peak_kind": peak_kind, "bytes_per_unit": BYTES_PER_UNIT_FUSED,
-                     "note": "dominant kernel is the forest walk, bound by node-visit gathers, "
-                             "not HBM"},
+        "roofline": roof,
+        "classifiers": {k: {"value": units * ws / (v["ms"] / 1e3), "ms_per_step": v["ms"],
+                            "e2e_ms": v["e2e_ms"], "stage_ms": v["stage_ms"],
+                            "bad2_nonocc": v["bad2_nonocc"], "roofline": v["roofline"]}
+                        for k, v in res.items()},
+        "matched_bad2": matched,
         "clocks": clk.summary(),
     }
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
@@ -331,6 +406,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["cbmv", "reference"], default="cbmv")
     ap.add_argument("--forest", default=FOREST)
+    ap.add_argument("--mlp", default=MLP, help="trained MLP parameters (cbmv_b200.train_mlp)")
+    ap.add_argument("--classifier", choices=["both", "rf", "mlp"], default="both",
+                    help="classifier paths to time (both: the MLP is the headline when it matches "
+                         "the RF's held-out bad-2.0)")
+    ap.add_argument("--no-eval", action="store_true",
+                    help="skip the held-out bad-2.0 comparison (the RF stays the headline)")
     ap.add_argument("--cpu-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--height", type=int, default=H0,

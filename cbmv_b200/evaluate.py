@@ -23,12 +23,16 @@ def bad_x(disp, gt, mask, thr=2.0):
 
 
 def compare(forest_path, mlp_path, seeds=HELD_OUT, ndisp=128):
-    import torch
     from .forest_gpu import GpuForest
     from .mlp import GpuMlp
     from .pipeline import StereoPipeline
-    pipe = StereoPipeline(GpuForest.load(forest_path))
-    net = GpuMlp.load(mlp_path)
+    return compare_loaded(StereoPipeline(GpuForest.load(forest_path)), GpuMlp.load(mlp_path), seeds, ndisp)
+
+
+def compare_loaded(pipe, net, seeds=HELD_OUT, ndisp=128):
+    """bad-2.0 (non-occluded) of the RF and MLP paths on the seeded 694x554
+    pairs `seeds`, with a pipeline that holds the forest and an uploaded net."""
+    import torch
     rows = []
     for s in seeds:
         L, R, gt, nonocc = synth.pair_694x554(s)
