@@ -176,8 +176,12 @@ __global__ void d_indices_kernel(const int32_t* __restrict__ gt, int64_t N, int 
 // denominator}; view 0 = left reference (row p of the volume), view 1 =
 // right reference (right pixel p: entries C[p + d, d], RAND_MAX when
 // x + d >= W, featextract.cpp:115-152).  One warp per (pixel, view).
+// Row statistics of matcher m: (min, den) in float64 for the exact features
+// and, when statsf is given, (min, 1/den) in float32 for the classifier
+// network (min = 2^31 and 1/den = 0 where the row has only sentinels).
 __global__ void feature_stats_kernel(const double* __restrict__ vol, int m, int64_t H, int64_t W,
-                                     int D, double sigma, double* __restrict__ stats) {
+                                     int D, double sigma, double* __restrict__ stats,
+                                     float2* __restrict__ statsf) {
   const int64_t HW = H * W;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x / 32);
   const int lane = threadIdx.x & 31;
@@ -207,6 +211,9 @@ __global__ void feature_stats_kernel(const double* __restrict__ vol, int m, int6
       double* o = stats + ((int64_t)(m * 2 + view) * HW + p) * 2;
       o[0] = mn;
       o[1] = den;
+      if (statsf)
+        statsf[(int64_t)(m * 2 + view) * HW + p] =
+            mn == kRandMax ? make_float2(kRandMaxF, 0.0f) : make_float2((float)mn, (float)(1.0 / den));
     }
   }
 }
@@ -245,11 +252,11 @@ int launch_features_gather(const double* const* vols, const double* stats, int64
 }
 
 int launch_feature_stats(const double* const* vols, int64_t H, int64_t W, int D, double* stats,
-                         cudaStream_t st) {
+                         cudaStream_t st, float2* statsf) {
   const int64_t warps = 2 * H * W;
   for (int m = 0; m < 4; m++)
     feature_stats_kernel<<<grid_for(warps * 32, kBlock), kBlock, 0, st>>>(vols[m], m, H, W, D,
-                                                                          hSigma[m], stats);
+                                                                          hSigma[m], stats, statsf);
   return check_launch("feature_stats");
 }
 
@@ -379,7 +386,7 @@ extern "C" int cbmv_features(const double* census, const double* ncc, const doub
   double* stats = nullptr;
   CBMV_CUDA(cudaMallocAsync(&stats, sizeof(double) * 16 * H * W, st));
   const double* vols[4] = {census, ncc, sob, sad};
-  int rc = launch_feature_stats(vols, H, W, D, stats, st);
+  int rc = launch_feature_stats(vols, H, W, D, stats, st, nullptr);
   if (!rc) {
     FeatVols fv = {{census, ncc, sob, sad}};
     features_kernel<<<grid_for(H * W * D, kBlock), kBlock, 0, st>>>(fv, stats, H, W, D, out);

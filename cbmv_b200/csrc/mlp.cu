@@ -532,231 +532,375 @@ extern "C" int cbmv_mlp_status(const cbmv_mlp* n, int* status) {
 // ====================================================================
 // Fused inference: features of 128 consecutive (pixel, d) samples -> the
 // network on the tensor cores -> matching cost 1 - P(correct), float32.
-// Persistent CTAs of 256 threads, two per SM.  Shared memory: the bf16
-// weights (64 KB, loaded once) and one activation tile A [128 x 128] that
-// holds in turn the input tile X0 [128 x 64] (its first atom), the first
-// and the second hidden layer; tensor memory: one 128-column accumulator
-// reused by the three layers.  Every reuse is ordered by the wait on the
-// MMA that last read the buffer.
+//
+// One persistent CTA per SM, four independent groups of 256 threads; each
+// group owns a 128-row tile in flight (its activation buffer in shared
+// memory and 128 tensor-memory columns), so while one group's MMAs run the
+// others compute features or epilogues.  Threads r and r + 128 of a group
+// share row r of its tile: each forms the features of two matchers of
+// sample r, then handles half of that row's columns in each epilogue.  The
+// group's first thread issues its MMAs and commits them to the group's
+// mbarrier; groups synchronise on named barriers only.
+//
+// Arithmetic, per layer (the float32 accumulator in tensor memory):
+//   layer 1  K = 32: 20 normalised features, two constant-one columns whose
+//            weights are b1 split into bf16 high and low parts, zeros;
+//   layers 2, 3: the bias is stored into the accumulator (tcgen05.st)
+//            before the MMA, which accumulates onto it;
+//   hidden activations are kept as 2 * GELU(s) in bf16 -- computed as
+//            x * (1 + tanh(k0 * x * (1 + k1 * x^2))) on packed bf16 pairs --
+//            and the following layer's weights are staged times 0.5 (an
+//            exact scaling), so the products are unchanged;
+//   output   layer 4 is an MMA too: N = 16, rows 0 and 1 of its weight tile
+//            are the high and low bf16 parts of 0.5 * w4, z = D[0] + D[1] +
+//            b4, cost = 1 - sigmoid(z) = 1 / (1 + exp(z)).
+// The features themselves are formed in float32 (they enter the network as
+// bf16), from the float64 cost volumes and float32 row statistics (min,
+// 1/den), with one reciprocal 1/(c + e) shared by the left and right ratio.
 // ====================================================================
 #include "features.cuh"
 
 namespace cbmv {
 namespace {
 
-constexpr int kMlpThreads = 256;
-constexpr size_t kSmW1 = 128 * 128, kSmW2 = 2 * 128 * 128, kSmW3 = 2 * 64 * 128;
-constexpr size_t kSmA = 2 * 128 * 128;
-constexpr size_t kSmMlp = 1024 + kSmW1 + kSmW2 + kSmW3 + kSmA;
+constexpr int kGroups = 4;                        // tiles in flight per CTA
+constexpr int kGroupThreads = 256;               // two threads per tile row
+constexpr int kInfThreads = kGroupThreads * kGroups;
+constexpr size_t kSmW1i = 128 * 128;      // [128 x 64] SW128, K = 32 used
+constexpr size_t kSmW2i = 2 * 128 * 128;  // [128 x 128]
+constexpr size_t kSmW3i = 2 * 64 * 128;   // [64 x 128]
+constexpr size_t kSmW4i = 16 * 128;       // [16 x 64]
+constexpr size_t kSmTile = 2 * 128 * 128; // a group's activation tile [128 x 128]
+constexpr size_t kSmInf = 1024 + kSmW1i + kSmW2i + kSmW3i + kSmW4i + kGroups * kSmTile;
+constexpr uint16_t kBf16One = 0x3F80;
 
-__device__ __forceinline__ float gelu_fast(float x) {
-  const float k0 = 0.7978845608028654f, k1 = 0.044715f;
-  const float u = k0 * (x + k1 * x * x * x);
-  float t;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
-  return 0.5f * x * (1.0f + t);
+static __constant__ float kEpsF[4] = {0.01f, 1.01f, 0.01f, 0.01f};
+static __constant__ float kInvSigmaF[4] = {(float)(1.0 / (2.0 * 8 * 8)), (float)(1.0 / 0.02),
+                                           (float)(1.0 / (2.0 * 100 * 100)), (float)(1.0 / (2.0 * 100 * 100))};
+
+__device__ __forceinline__ void group_sync(int g) {
+  asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "n"(kGroupThreads) : "memory");
+}
+// barrier of the group that also ANDs a flag over its threads
+__device__ __forceinline__ bool group_all(int g, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(g + 1), "n"(kGroupThreads)
+      : "memory");
+  return r != 0;
 }
 
-// bf16 weight matrix [R x K] (row-major, K contiguous) -> SW128 tile in smem
-__device__ void stage_weights(const uint16_t* __restrict__ g, int R, int K, unsigned char* s) {
-  for (int q = threadIdx.x; q < R * (K / 8); q += blockDim.x) {
-    const int r = q / (K / 8), c = q % (K / 8);
-    *reinterpret_cast<uint4*>(s + umma::sw128_offset(R, r, c * 8)) =
-        *reinterpret_cast<const uint4*>(g + (size_t)r * K + c * 8);
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          taddr),
+      "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]),
+      "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15])
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// Two float32 values as a packed bf16 pair (low = a), round to nearest even
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+  const __nv_bfloat162 x = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&x);
+}
+
+// 2 * GELU of two float32 pre-activations, as a packed bf16 pair (low = a)
+__device__ __forceinline__ uint32_t gelu2x_bf16(float a, float b) {
+  const uint32_t xb = pack_bf16x2(a, b);
+  const __nv_bfloat162 x = *reinterpret_cast<const __nv_bfloat162*>(&xb);
+  const __nv_bfloat162 c0 = __float2bfloat162_rn(0.7978845608028654f);
+  const __nv_bfloat162 c1 = __float2bfloat162_rn(0.7978845608028654f * 0.044715f);
+  const __nv_bfloat162 u = __hmul2(x, __hfma2(__hmul2(x, x), c1, c0));
+  uint32_t ub = *reinterpret_cast<const uint32_t*>(&u), tb;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(tb) : "r"(ub));
+  const __nv_bfloat162 t = *reinterpret_cast<const __nv_bfloat162*>(&tb);
+  const __nv_bfloat162 r = __hfma2(x, t, x);
+  return *reinterpret_cast<const uint32_t*>(&r);
+}
+
+// ratio and likelihood of cost c (featextract.cpp:333 and :440) in float32
+// against its row statistics st = (min, 1/den); inv_ce = 1 / (c + e)
+__device__ __forceinline__ void conf_f32(float c, float inv_ce, float2 st, float e, float inv_sigma,
+                                         float* ratio, float* lik) {
+  const float t = c - st.x;
+  *ratio = st.x == kRandMaxF ? 0.0f : (st.x + e) * inv_ce;
+  *lik = __expf(-(t * t) * inv_sigma) * st.y;  // 1/den = 0 on sentinel rows
+}
+
+// Stage the inference weights from the float32 parameter vector.
+__device__ void stage_inference_weights(const float* __restrict__ P, unsigned char* sW1, unsigned char* sW2,
+                                        unsigned char* sW3, unsigned char* sW4) {
+  for (int q = threadIdx.x; q < 128 * 64; q += blockDim.x) {
+    const int r = q >> 6, k = q & 63;
+    const float b = P[kOffB1 + r];
+    const float bh = __bfloat162float(__float2bfloat16_rn(b));
+    float v = 0.0f;
+    if (k < kF) v = P[kOffW1 + r * kF + k];
+    else if (k == kF) v = bh;
+    else if (k == kF + 1) v = b - bh;
+    *reinterpret_cast<uint16_t*>(sW1 + umma::sw128_offset(128, r, k)) = to_bf16(v);
+  }
+  for (int q = threadIdx.x; q < 128 * 128; q += blockDim.x) {
+    const int r = q >> 7, k = q & 127;
+    *reinterpret_cast<uint16_t*>(sW2 + umma::sw128_offset(128, r, k)) = to_bf16(0.5f * P[kOffW2 + q]);
+  }
+  for (int q = threadIdx.x; q < 64 * 128; q += blockDim.x) {
+    const int r = q >> 7, k = q & 127;
+    *reinterpret_cast<uint16_t*>(sW3 + umma::sw128_offset(64, r, k)) = to_bf16(0.5f * P[kOffW3 + q]);
+  }
+  for (int q = threadIdx.x; q < 16 * 64; q += blockDim.x) {
+    const int r = q >> 6, k = q & 63;
+    const float w = 0.5f * P[kOffW4 + k];
+    const float wh = __bfloat162float(__float2bfloat16_rn(w));
+    const float v = r == 0 ? wh : r == 1 ? w - wh : 0.0f;
+    *reinterpret_cast<uint16_t*>(sW4 + umma::sw128_offset(16, r, k)) = to_bf16(v);
   }
 }
 
-// 16 accumulator columns -> +bias -> GELU -> bf16 into the A tile
-__device__ __forceinline__ void epi_store(const float* v, const float* bias, int c0, int row,
-                                          unsigned char* sA) {
-  uint32_t packed[8];
+// One hidden-layer epilogue of row `row`, this thread's NC accumulator
+// columns from c_begin: 2*GELU as bf16 into the activation tile; the first
+// `nprefill` of these columns then receive the next layer's bias.
+template <int NC>
+__device__ __forceinline__ void epilogue_hidden(uint32_t tlane, unsigned char* sA, int row, int c_begin,
+                                                const float* next_bias, int nprefill) {
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
-    const float a = gelu_fast(v[2 * i] + bias[c0 + 2 * i]);
-    const float b = gelu_fast(v[2 * i + 1] + bias[c0 + 2 * i + 1]);
-    packed[i] = (uint32_t)to_bf16(a) | ((uint32_t)to_bf16(b) << 16);
+  for (int c = c_begin; c < c_begin + NC; c += 16) {
+    float v[16];
+    umma::tmem_ld16(tlane + c, v);
+    uint32_t h[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) h[i] = gelu2x_bf16(v[2 * i], v[2 * i + 1]);
+    *reinterpret_cast<uint4*>(sA + umma::sw128_offset(128, row, c)) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4*>(sA + umma::sw128_offset(128, row, c + 8)) = make_uint4(h[4], h[5], h[6], h[7]);
+    if (c - c_begin < nprefill) {
+#pragma unroll
+      for (int i = 0; i < 16; i += 4) {
+        const float4 q = *reinterpret_cast<const float4*>(next_bias + c + i);
+        v[i] = q.x;
+        v[i + 1] = q.y;
+        v[i + 2] = q.z;
+        v[i + 3] = q.w;
+      }
+      tmem_st16(tlane + c, v);
+    }
   }
-  // 16 consecutive k = two 16-byte chunks of the swizzled row
-  *reinterpret_cast<uint4*>(sA + umma::sw128_offset(128, row, c0)) =
-      make_uint4(packed[0], packed[1], packed[2], packed[3]);
-  *reinterpret_cast<uint4*>(sA + umma::sw128_offset(128, row, c0 + 8)) =
-      make_uint4(packed[4], packed[5], packed[6], packed[7]);
+  if (nprefill > 0) tmem_wait_st();
 }
 
-__global__ void __launch_bounds__(kMlpThreads, 2)
-    features_mlp_kernel(FeatVols fv, const double* __restrict__ stats, int64_t H, int64_t W, int D,
-                        const float* __restrict__ P, const uint16_t* __restrict__ W1b,
-                        const uint16_t* __restrict__ W2b, const uint16_t* __restrict__ W3b,
-                        float* __restrict__ prob0, int* __restrict__ status) {
+__global__ void __launch_bounds__(kInfThreads, 1)
+    features_mlp_kernel(FeatVols fv, const float2* __restrict__ statsf, int64_t H, int64_t W, int D,
+                        const float* __restrict__ P, float* __restrict__ prob0, int* __restrict__ status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* sW1 = base;
-  unsigned char* sW2 = sW1 + kSmW1;
-  unsigned char* sW3 = sW2 + kSmW2;
-  unsigned char* sA = sW3 + kSmW3;
-  unsigned char* sX0 = sA;  // the input tile is the first atom of A
-  __shared__ float sP[kNParams - kOffW4 + kNormN + kH1 + kH2 + kH3];
-  __shared__ float partial[2][128];
-  __shared__ uint64_t bar;
+  unsigned char* sW2 = sW1 + kSmW1i;
+  unsigned char* sW3 = sW2 + kSmW2i;
+  unsigned char* sW4 = sW3 + kSmW3i;
+  unsigned char* sTiles = sW4 + kSmW4i;
+  __shared__ __align__(16) float s_norm[kNormN];
+  __shared__ __align__(16) float s_b2[kH2];
+  __shared__ __align__(16) float s_b3[kH3];
+  __shared__ float s_b4;
+  __shared__ uint64_t bars[kGroups];
   __shared__ uint32_t tmem_base;
-  float* s_norm = sP;                 // cap, mu, inv_sd
-  float* s_b1 = s_norm + kNormN;
-  float* s_b2 = s_b1 + kH1;
-  float* s_b3 = s_b2 + kH2;
-  float* s_w4 = s_b3 + kH3;           // w4[64], b4
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x, g = tid / kGroupThreads, gt = tid % kGroupThreads;
+  const int row = gt & 127, half = gt >> 7, wq = (gt >> 5) & 3;
 
-  if (warp == 0) umma::tmem_alloc(&tmem_base, 128);
-  if (tid == 0) umma::mbar_init(&bar, 1);
-  stage_weights(W1b, 128, 64, sW1);
-  stage_weights(W2b, 128, 128, sW2);
-  stage_weights(W3b, 64, 128, sW3);
-  for (int i = tid; i < kNormN; i += kMlpThreads) s_norm[i] = P[i];
-  for (int i = tid; i < kH1; i += kMlpThreads) s_b1[i] = P[kOffB1 + i];
-  for (int i = tid; i < kH2; i += kMlpThreads) s_b2[i] = P[kOffB2 + i];
-  for (int i = tid; i < kH3; i += kMlpThreads) s_b3[i] = P[kOffB3 + i];
-  for (int i = tid; i < kH3 + 1; i += kMlpThreads) s_w4[i] = P[kOffW4 + i];
+  if (tid < 32) umma::tmem_alloc(&tmem_base, 128 * kGroups);
+  if (tid < kGroups) umma::mbar_init(&bars[tid], 1);
+  stage_inference_weights(P, sW1, sW2, sW3, sW4);
+  for (int i = tid; i < kNormN; i += kInfThreads) s_norm[i] = P[i];
+  for (int i = tid; i < kH2; i += kInfThreads) s_b2[i] = P[kOffB2 + i];
+  for (int i = tid; i < kH3; i += kInfThreads) s_b3[i] = P[kOffB3 + i];
+  if (tid == 0) s_b4 = P[kOffB4];
   umma::fence_async_smem();
   umma::tc_fence_before();
   __syncthreads();
   umma::tc_fence_after();
-  const uint32_t tmem = tmem_base;
-  const uint32_t id128 = umma::idesc_bf16(128, 128), id64 = umma::idesc_bf16(128, 64);
-  const uint64_t dX0 = umma::sw128_desc(umma::smem_u32(sX0));
-  const uint64_t dA0 = umma::sw128_desc(umma::smem_u32(sA)), dA1 = umma::sw128_desc(umma::smem_u32(sA + 128 * 128));
-  const uint64_t dW1 = umma::sw128_desc(umma::smem_u32(sW1));
-  const uint64_t dW20 = umma::sw128_desc(umma::smem_u32(sW2)), dW21 = umma::sw128_desc(umma::smem_u32(sW2 + 128 * 128));
-  const uint64_t dW30 = umma::sw128_desc(umma::smem_u32(sW3)), dW31 = umma::sw128_desc(umma::smem_u32(sW3 + 64 * 128));
+
+  unsigned char* sA = sTiles + g * kSmTile;
+  uint64_t* bar = &bars[g];
+  const uint32_t tacc = tmem_base + (uint32_t)(g * 128);
+  const uint32_t tlane = tacc + ((uint32_t)(wq * 32) << 16);
+  const bool leader = gt == 0;
+  constexpr uint32_t id128 = umma::idesc_bf16(128, 128), id64 = umma::idesc_bf16(128, 64),
+                     id16 = umma::idesc_bf16(128, 16);
+  // operand descriptors, formed where the leader issues (keeps them out of the other threads' registers)
+#define DESC(ptr) umma::sw128_desc(umma::smem_u32(ptr))
 
   const int64_t HW = H * W, N = HW * D;
   const int64_t tiles = (N + 127) / 128;
-  const int quad = warp & 3, half = warp >> 2;
-  const int row = quad * 32 + lane;  // accumulator row this thread reads
-  const uint32_t trow = tmem + ((uint32_t)(quad * 32) << 16);
+  const int64_t tstride = (int64_t)gridDim.x * kGroups;
+  // this thread's sample t = tile * 128 + row as (pixel p, disparity d, column x), advanced incrementally
+  int64_t tile = (int64_t)blockIdx.x * kGroups + g;
+  int64_t t = tile * 128 + row;
+  int64_t p = t / D;
+  int d = (int)(t - p * D);
+  int64_t x = p % W;
+  const int64_t step = tstride * 128;
+  const int64_t sp = step / D;
+  const int sd = (int)(step - sp * D);
+  const int64_t sx = sp % W;
   uint32_t phase = 0;
   bool ok = true;
 
-  for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-    // 1. features of sample (tile*128 + s), matchers {2h, 2h+1} by thread half h
+  for (; tile < tiles; tile += tstride) {
+    // 1. features of sample t, matchers 2*half and 2*half+1 -> row of X0 (the first atom of the tile)
     {
-      const int s = tid & 127, h = tid >> 7;
-      int64_t t = tile * 128 + s;
-      if (t >= N) t = N - 1;
-      const int64_t p = t / D;
-      const int d = (int)(t - p * D);
-      const int64_t x = p % W;
-      float f[10];
-      features_pair(fv.v, stats, HW, D, p, x, d, 2 * h, f);
+      const bool valid = t < N;
+      const int64_t tv = valid ? t : 0, pv = valid ? p : 0;
+      const int dv = valid ? d : 0;
+      const bool has_right = valid && x >= d;
+      float f[10];  // f[2q + i]: feature group q of matcher 2*half + i
 #pragma unroll
-      for (int j = 0; j < 10; j++) {
-        const int k = (j >> 1) * 4 + 2 * h + (j & 1);  // feature column
-        const float v = (fminf(f[j], s_norm[k]) - s_norm[kF + k]) * s_norm[2 * kF + k];
-        *reinterpret_cast<uint16_t*>(sX0 + umma::sw128_offset(128, s, k)) = to_bf16(v);
+      for (int i = 0; i < 2; i++) {
+        const int m = 2 * half + i;
+        const double* vol = i == 0 ? (half ? fv.v[2] : fv.v[0]) : (half ? fv.v[3] : fv.v[1]);
+        const float c = (float)vol[tv];
+        const float2 sl = statsf[(int64_t)(m * 2) * HW + pv];
+        const float2 sr = has_right ? statsf[(int64_t)(m * 2 + 1) * HW + pv - dv] : make_float2(kRandMaxF, 0.0f);
+        const float inv_ce = __fdividef(1.0f, c + kEpsF[m]);
+        f[i] = c;
+        conf_f32(c, inv_ce, sl, kEpsF[m], kInvSigmaF[m], &f[2 + i], &f[4 + i]);
+        conf_f32(c, inv_ce, sr, kEpsF[m], kInvSigmaF[m], &f[6 + i], &f[8 + i]);
       }
-      // zero padding, columns 20..63 (the previous tile left activations here)
-      if (h == 0) {
 #pragma unroll
-        for (int c = 3; c < 8; c++)
-          *reinterpret_cast<uint4*>(sX0 + umma::sw128_offset(128, s, c * 8)) = make_uint4(0, 0, 0, 0);
-      } else {
-#pragma unroll
-        for (int k = 20; k < 24; k++) *reinterpret_cast<uint16_t*>(sX0 + umma::sw128_offset(128, s, k)) = 0;
+      for (int q = 0; q < 5; q++) {
+        const int k = 4 * q + 2 * half;  // reference column of f[2q]
+        const float a = (fminf(f[2 * q], s_norm[k]) - s_norm[kF + k]) * s_norm[2 * kF + k];
+        const float b = (fminf(f[2 * q + 1], s_norm[k + 1]) - s_norm[kF + k + 1]) * s_norm[2 * kF + k + 1];
+        *reinterpret_cast<uint32_t*>(sA + umma::sw128_offset(128, row, k)) = pack_bf16x2(a, b);
+      }
+      if (half) {  // columns 20, 21: the bias inputs; 22..31: zero
+        *reinterpret_cast<uint2*>(sA + umma::sw128_offset(128, row, 20)) =
+            make_uint2((uint32_t)kBf16One | ((uint32_t)kBf16One << 16), 0u);
+        *reinterpret_cast<uint4*>(sA + umma::sw128_offset(128, row, 24)) = make_uint4(0u, 0u, 0u, 0u);
       }
     }
     umma::fence_async_smem();
     umma::tc_fence_before();
-    __syncthreads();
+    group_sync(g);
     umma::tc_fence_after();
-    // 2. layer 1: D = X0 W1^T (K = 64)
-    if (tid == 0) {
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tmem, dX0 + 2 * kk, dW1 + 2 * kk, id128, kk > 0);
-      umma::mma_commit(&bar);
+    // 2. layer 1 (K = 32) -> accumulator columns 0..127
+    if (leader) {
+      const uint64_t dA0 = DESC(sA), dW1 = DESC(sW1);
+      umma::mma_bf16(tacc, dA0, dW1, id128, false);
+      umma::mma_bf16(tacc, dA0 + 2, dW1 + 2, id128, true);
+      umma::mma_commit(bar);
     }
-    ok = umma::mbar_wait(&bar, phase, kWaitLimit);
+    ok = group_all(g, umma::mbar_wait(bar, phase, kWaitLimit));
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
-    for (int c0 = half * 64; c0 < half * 64 + 64; c0 += 16) {
-      float v[16];
-      umma::tmem_ld16(trow + c0, v);
-      epi_store(v, s_b1, c0, row, sA);
-    }
+    epilogue_hidden<64>(tlane, sA, row, 64 * half, s_b2, 64);
     umma::fence_async_smem();
     umma::tc_fence_before();
-    __syncthreads();
+    group_sync(g);
     umma::tc_fence_after();
-    // 3. layer 2: D = A1 W2^T (K = 128, two atoms)
-    if (tid == 0) {
+    // 3. layer 2 (K = 128) onto the bias b2
+    if (leader) {
+      const uint64_t dA0 = DESC(sA), dA1 = DESC(sA + 128 * 128), dW20 = DESC(sW2), dW21 = DESC(sW2 + 128 * 128);
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tmem, dA0 + 2 * kk, dW20 + 2 * kk, id128, kk > 0);
+      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA0 + 2 * kk, dW20 + 2 * kk, id128, true);
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tmem, dA1 + 2 * kk, dW21 + 2 * kk, id128, true);
-      umma::mma_commit(&bar);
+      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA1 + 2 * kk, dW21 + 2 * kk, id128, true);
+      umma::mma_commit(bar);
     }
-    ok = umma::mbar_wait(&bar, phase, kWaitLimit);
+    ok = group_all(g, umma::mbar_wait(bar, phase, kWaitLimit));
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
-    for (int c0 = half * 64; c0 < half * 64 + 64; c0 += 16) {
-      float v[16];
-      umma::tmem_ld16(trow + c0, v);
-      epi_store(v, s_b2, c0, row, sA);
-    }
+    // b3 goes to columns 0..63, which only the first half has read
+    epilogue_hidden<64>(tlane, sA, row, 64 * half, s_b3, half ? 0 : 64);
     umma::fence_async_smem();
     umma::tc_fence_before();
-    __syncthreads();
+    group_sync(g);
     umma::tc_fence_after();
-    // 4. layer 3: D = A2 W3^T (N = 64)
-    if (tid == 0) {
+    // 4. layer 3 (N = 64) onto the bias b3
+    if (leader) {
+      const uint64_t dA0 = DESC(sA), dA1 = DESC(sA + 128 * 128), dW30 = DESC(sW3), dW31 = DESC(sW3 + 64 * 128);
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tmem, dA0 + 2 * kk, dW30 + 2 * kk, id64, kk > 0);
+      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA0 + 2 * kk, dW30 + 2 * kk, id64, true);
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tmem, dA1 + 2 * kk, dW31 + 2 * kk, id64, true);
-      umma::mma_commit(&bar);
+      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA1 + 2 * kk, dW31 + 2 * kk, id64, true);
+      umma::mma_commit(bar);
     }
-    ok = umma::mbar_wait(&bar, phase, kWaitLimit);
+    ok = group_all(g, umma::mbar_wait(bar, phase, kWaitLimit));
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
-    // 5. output layer: z = gelu(D + b3) . w4 + b4; cost = 1 - sigmoid(z)
-    float acc = 0.0f;
-    for (int c0 = half * 32; c0 < half * 32 + 32; c0 += 16) {
-      float v[16];
-      umma::tmem_ld16(trow + c0, v);
-#pragma unroll
-      for (int i = 0; i < 16; i++) acc += gelu_fast(v[i] + s_b3[c0 + i]) * s_w4[c0 + i];
-    }
-    partial[half][row] = acc;
+    epilogue_hidden<32>(tlane, sA, row, 32 * half, nullptr, 0);
+    umma::fence_async_smem();
     umma::tc_fence_before();
-    __syncthreads();
+    group_sync(g);
+    umma::tc_fence_after();
+    // 5. output layer (N = 16, rows 0/1 = high/low parts of w4) -> columns 64..79
+    if (leader) {
+      const uint64_t dA0 = DESC(sA), dW4 = DESC(sW4);
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc + 64, dA0 + 2 * kk, dW4 + 2 * kk, id16, kk > 0);
+      umma::mma_commit(bar);
+    }
+    ok = group_all(g, umma::mbar_wait(bar, phase, kWaitLimit));
+    phase ^= 1u;
+    umma::tc_fence_after();
+    if (!ok) break;
     if (half == 0) {
-      const int64_t t = tile * 128 + row;
-      const float z = (partial[0][row] + partial[1][row]) + s_w4[kH3];
+      uint32_t z2[2];
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];"
+                   : "=r"(z2[0]), "=r"(z2[1])
+                   : "r"(tlane + 64));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      const float z = (__uint_as_float(z2[0]) + __uint_as_float(z2[1])) + s_b4;
       if (t < N) prob0[t] = 1.0f / (1.0f + __expf(z));
     }
+    umma::tc_fence_before();
+    // advance this thread's sample by tstride tiles
+    t += step;
+    p += sp;
+    d += sd;
+    x += sx;
+    if (d >= D) {
+      d -= D;
+      p += 1;
+      x += 1;
+    }
+    if (x >= W) x -= W;
   }
   if (!ok) {
-    if (tid == 0) atomicExch(status, 1);
-    umma::mbar_wait(&bar, phase ^ 1u, kWaitLimit);
+    if (leader) atomicExch(status, 1);
+    // let this group's MMAs still in flight finish (bounded) before the memory is freed
+    umma::mbar_wait(bar, phase ^ 1u, kWaitLimit);
   }
   umma::tc_fence_before();
   __syncthreads();
-  if (warp == 0) umma::tmem_dealloc(tmem, 128);
+  if (tid < 32) umma::tmem_dealloc(tmem_base, 128 * kGroups);
+#undef DESC
 }
 
 }  // namespace
 
-int launch_features_mlp(const double* const* vols, const double* stats, int64_t H, int64_t W, int D,
+int launch_features_mlp(const double* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
                         const cbmv_mlp* m, float* prob0, cudaStream_t st) {
   int dev = 0, sms = 0;
   CBMV_CUDA(cudaGetDevice(&dev));
   CBMV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   CBMV_CUDA(cudaFuncSetAttribute(features_mlp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kSmMlp));
+                                 (int)kSmInf));
+  CBMV_REQUIRE(((uintptr_t)statsf & 7) == 0, CBMV_EINVAL, "feature statistics must be 8-byte aligned");
+  const int64_t tiles = (H * W * D + 127) / 128;
+  const int64_t need = (tiles + kGroups - 1) / kGroups;
+  const int grid = (int)(need < sms ? need : sms);
   FeatVols fv = {{vols[0], vols[1], vols[2], vols[3]}};
-  features_mlp_kernel<<<2 * sms, kMlpThreads, kSmMlp, st>>>(fv, stats, H, W, D, m->P, m->W1b, m->W2b,
-                                                           m->W3b, prob0, m->status);
+  features_mlp_kernel<<<grid, kInfThreads, kSmInf, st>>>(fv, statsf, H, W, D, m->P, prob0, m->status);
   return check_launch("features_mlp");
 }
 

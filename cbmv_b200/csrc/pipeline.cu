@@ -97,6 +97,7 @@ struct Work {
   int32_t *sobL, *sobR;
   double* vol[4];
   double* stats;
+  float2* statsf;  // (min, 1/den) in float32 for the classifier network
   float *volA, *volB;
   float *imL, *imR, *crossL, *crossR, *dtmp, *dtmp2;
   float* grad;  // SGM neighbour differences: left h/v, right h/v
@@ -119,6 +120,7 @@ Work carve(void* base, int64_t H, int64_t W, int D, size_t* bytes) {
   w.sobR = c.take<int32_t>(HW);
   for (int m = 0; m < 4; m++) w.vol[m] = c.take<double>(V);
   w.stats = c.take<double>(16 * HW);
+  w.statsf = c.take<float2>(8 * HW);
   w.volA = c.take<float>(V);
   w.volB = c.take<float>(V);
   w.imL = c.take<float>(HW);
@@ -287,7 +289,7 @@ static int run_front(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const 
   RC(launch_zsad_cost<double>(L, R, w.muL, w.muR, H, W, D, p->sadw, CBMV_HWD, w.vol[3], st));
   CBMV_CUDA(cudaEventRecord(c->ev[1], st));
   const double* vols[4] = {w.vol[0], w.vol[1], w.vol[2], w.vol[3]};
-  RC(launch_feature_stats(vols, H, W, D, w.stats, st));
+  RC(launch_feature_stats(vols, H, W, D, w.stats, st, w.statsf));
   CBMV_CUDA(cudaEventRecord(c->ev[2], st));
   *wout = w;
   return CBMV_OK;
@@ -328,7 +330,7 @@ extern "C" int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p
   RC(run_front(c, p, L, R, H, W, D, &w));
   cudaStream_t st = c->stream;
   const double* vols[4] = {w.vol[0], w.vol[1], w.vol[2], w.vol[3]};
-  RC(launch_features_mlp(vols, w.stats, H, W, D, m, w.volA, st));
+  RC(launch_features_mlp(vols, w.statsf, H, W, D, m, w.volA, st));
   if (prob0)
     CBMV_CUDA(cudaMemcpyAsync(prob0, w.volA, sizeof(float) * H * W * D, cudaMemcpyDeviceToDevice, st));
   CBMV_CUDA(cudaEventRecord(c->ev[3], st));

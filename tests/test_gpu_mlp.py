@@ -77,8 +77,12 @@ def test_mlp_training_reduces_loss(gpu):
 
 
 def test_fused_inference_matches_oracle_forward(gpu, small_pair):
-    """cbmv_run_mlp's matching cost (features + three tcgen05 layers fused,
-    tanh.approx GELU) against the float64 network on the same features."""
+    """cbmv_run_mlp's matching cost (float32 features + four tcgen05 layers
+    fused, packed-bf16 GELU) against (a) the oracle's model of the same
+    arithmetic (bf16 rounding at every step of GELU, exact tanh): max 5e-3,
+    mean 3e-4 on P -- tanh.approx and the float32 features differ from it by
+    about one bf16 unit here and there; (b) the float64 network on the same
+    features: max 3e-2, mean 2e-3 -- the cost of bf16 GELU arithmetic."""
     from cbmv_b200.mlp import GpuMlp, MlpParams, input_stats
     from cbmv_b200.pipeline import StereoPipeline
     from oracle import mlp_ref
@@ -99,11 +103,14 @@ def test_fused_inference_matches_oracle_forward(gpu, small_pair):
     pipe.run_mlp(g, L, R, D, prob_out=prob)
     torch.cuda.synchronize()
     assert g.status() == 0
-    f = mlp_ref.forward(net.vec, X)
-    want = 1.0 / (1.0 + np.exp(f["z"]))
     got = prob.cpu().numpy().reshape(-1)
-    assert np.abs(got - want).max() < 5e-3, np.abs(got - want).max()
-    assert np.mean(np.abs(got - want)) < 5e-4
+    model = 1.0 / (1.0 + np.exp(mlp_ref.forward_fused(net.vec, X)))
+    exact = 1.0 / (1.0 + np.exp(mlp_ref.forward(net.vec, X)["z"]))
+    e_model, e_exact = np.abs(got - model), np.abs(got - exact)
+    print("fused vs model: max %.2e mean %.2e; vs float64 network: max %.2e mean %.2e"
+          % (e_model.max(), e_model.mean(), e_exact.max(), e_exact.mean()))
+    assert e_model.max() < 5e-3 and e_model.mean() < 3e-4, (e_model.max(), e_model.mean())
+    assert e_exact.max() < 3e-2 and e_exact.mean() < 2e-3, (e_exact.max(), e_exact.mean())
 
 
 def test_training_samples_follow_labels(gpu):
