@@ -31,7 +31,8 @@ class cbmv_params(ctypes.Structure):
                 ("pi1", _flt), ("pi2", _flt), ("sgm_q1", _flt), ("sgm_q2", _flt),
                 ("alpha1", _flt), ("tau_so", _flt), ("sgm_i", _int), ("L1", _int),
                 ("tau1", _flt), ("cbca_i1", _int), ("cbca_i2", _int), ("median_i", _int),
-                ("median_w", _int), ("blur_sigma", _flt), ("blur_t", _flt), ("direction", _int)]
+                ("median_w", _int), ("blur_sigma", _flt), ("blur_t", _flt), ("direction", _int),
+                ("exact_cbca", _int)]
 
 
 # name -> argtypes (all return int status unless listed in _RESTYPE)
@@ -75,6 +76,7 @@ SIGNATURES = {
     "cbmv_cross": [_vp, _i64, _i64, _int, _flt, _vp, _vp],
     "cbmv_sgm": [_vp, _vp, _vp, _i64, _i64, _int, _flt, _flt, _flt, _flt, _flt, _flt, _int, _vp, _vp],
     "cbmv_cbca": [_vp, _vp, _vp, _i64, _i64, _int, _int, _int, _vp, _vp],
+    "cbmv_cbca_separable": [_vp, _vp, _vp, _i64, _i64, _int, _int, _int, _vp, _vp],
     "cbmv_wta": [_vp, _i64, _i64, _int, _int, _vp, _vp],
     "cbmv_subpixel": [_vp, _vp, _i64, _i64, _int, _int, _vp, _vp],
     "cbmv_median2d": [_vp, _i64, _i64, _int, _vp, _vp],

@@ -49,6 +49,7 @@ extern "C" void cbmv_params_default(cbmv_params* p) {
   p->blur_sigma = 2.2f;
   p->blur_t = 1.3f;
   p->direction = -1;  // test.py:501
+  p->exact_cbca = 0;
 }
 
 struct cbmv_ctx {
@@ -230,8 +231,12 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
   RC(launch_cross(w.imR, H, W, p->L1, p->tau1, w.crossR, st));
   float* cur = w.volA;
   float* oth = w.volB;
+  auto cbca = [&](const float* in, float* out) {
+    return p->exact_cbca ? launch_cbca(w.crossL, w.crossR, in, H, W, D, CBMV_HWD, p->direction, out, st, p->L1 - 1)
+                         : launch_cbca_sep(w.crossL, w.crossR, in, H, W, D, p->direction, out, st, p->L1 - 1);
+  };
   for (int i = 0; i < p->cbca_i1; i++) {
-    RC(launch_cbca(w.crossL, w.crossR, cur, H, W, D, CBMV_HWD, p->direction, oth, st, p->L1 - 1));
+    RC(cbca(cur, oth));
     float* t = cur; cur = oth; oth = t;
   }
   SgmParams sp{p->pi1, p->pi2, p->tau_so, p->alpha1, p->sgm_q1, p->sgm_q2, p->direction};
@@ -247,7 +252,7 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
     float* t = cur; cur = oth; oth = t;
   }
   for (int i = 0; i < p->cbca_i2; i++) {
-    RC(launch_cbca(w.crossL, w.crossR, cur, H, W, D, CBMV_HWD, p->direction, oth, st, p->L1 - 1));
+    RC(cbca(cur, oth));
     float* t = cur; cur = oth; oth = t;
   }
   float* d0 = w.dtmp;

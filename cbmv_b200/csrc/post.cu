@@ -331,6 +331,102 @@ __global__ void __launch_bounds__(256) cbca_hwd_tiled_kernel(
   }
 }
 
+// cbca on [H,W,D] volumes in separable form, the row-then-column
+// decomposition of integral-image aggregation: the support row of row yy
+// for (x, d) is the same interval for every centre row y (it depends on the
+// arms of (yy, x) and (yy, x + d*direction) only), so
+//   R(yy, x, d) = sum of the support row,   C(yy, x, d) = its length,
+//   out(y, x, d) = sum over the support rows yy of R / sum of C.
+// A CTA owns CS_TY x CS_TX pixels x 32 disparities (lane = disparity): it
+// forms R and C for its rows and HALO rows above and below into shared
+// memory, then the column sums.  Both sums run over fixed 2*HALO+1 taps,
+// masked to the support, in ascending order; with arms of at most
+// HALO = L1 - 1 pixels every support element is within the taps.  The
+// result differs from the reference's single running float sum
+// (post.cu:415-429) by rounding only.
+constexpr int CS_TX = 8, CS_TY = 32, CS_TD = 32;
+
+template <int HALO>
+constexpr size_t cbca_sep_smem_bytes() {
+  return (size_t)(CS_TY + 2 * HALO) * CS_TX * CS_TD * (sizeof(float) + sizeof(uint8_t));
+}
+
+template <int HALO>
+__global__ void __launch_bounds__(256) cbca_hwd_sep_kernel(
+    const float* __restrict__ lc, const float* __restrict__ rc, const float* __restrict__ in, int H, int W,
+    int D, int direction, float* __restrict__ out) {
+  constexpr int SR = CS_TY + 2 * HALO;
+  extern __shared__ float sR[];                                   // [SR][CS_TX][CS_TD]
+  uint8_t* sC = reinterpret_cast<uint8_t*>(sR + SR * CS_TX * CS_TD);  // [SR][CS_TX][CS_TD]
+  const int ntd = (D + CS_TD - 1) / CS_TD, ntx = (W + CS_TX - 1) / CS_TX;
+  const int64_t t = blockIdx.x;
+  const int td = (int)(t % ntd), tx = (int)((t / ntd) % ntx), ty = (int)(t / ((int64_t)ntd * ntx));
+  const int X0 = tx * CS_TX, Y0 = ty * CS_TY;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int d = td * CS_TD + lane, dd = d * direction;
+  const int64_t HW = (int64_t)H * W;
+  // row sums of rows Y0 - HALO .. Y0 + CS_TY + HALO - 1
+  for (int q = warp; q < SR * CS_TX; q += nwarp) {
+    const int r = q / CS_TX, c = q % CS_TX;
+    const int yy = Y0 - HALO + r, x = X0 + c, xm = x + dd;
+    float sum = 0.0f;
+    int cnt = 0;
+    if (yy >= 0 && yy < H && x < W && d < D && xm >= 0 && xm < W) {
+      const int64_t o = (int64_t)yy * W;
+      const int xxs = max((int)__ldg(lc + o + x), (int)__ldg(rc + o + xm) - dd);
+      const int xxt = min((int)__ldg(lc + HW + o + x), (int)__ldg(rc + HW + o + xm) - dd);
+      const float* row = in + o * D + d;
+#pragma unroll
+      for (int k = -HALO; k <= HALO; k++) {
+        const int xx = x + k;
+        if (xx > xxs && xx < xxt && xx >= 0 && xx < W) sum += __ldg(row + (int64_t)xx * D);
+      }
+      cnt = max(xxt - xxs - 1, 0);
+    }
+    sR[(r * CS_TX + c) * CS_TD + lane] = sum;
+    sC[(r * CS_TX + c) * CS_TD + lane] = (uint8_t)cnt;
+  }
+  __syncthreads();
+  // column sums over the support rows
+  for (int q = warp; q < CS_TY * CS_TX; q += nwarp) {
+    const int cy = q / CS_TX, c = q % CS_TX;
+    const int y = Y0 + cy, x = X0 + c, xm = x + dd;
+    if (y >= H || x >= W || d >= D) continue;
+    const int64_t id = ((int64_t)y * W + x) * D + d;
+    if (xm < 0 || xm >= W) {
+      out[id] = __ldg(in + id);
+      continue;
+    }
+    const int64_t o = (int64_t)y * W;
+    const int yys = max((int)__ldg(lc + 2 * HW + o + x), (int)__ldg(rc + 2 * HW + o + xm));
+    const int yyt = min((int)__ldg(lc + 3 * HW + o + x), (int)__ldg(rc + 3 * HW + o + xm));
+    float sum = 0.0f;
+    int cnt = 0;
+#pragma unroll
+    for (int k = -HALO; k <= HALO; k++) {
+      const int yy = y + k;
+      if (yy > yys && yy < yyt) {
+        const int i = ((cy + HALO + k) * CS_TX + c) * CS_TD + lane;
+        sum += sR[i];
+        cnt += sC[i];
+      }
+    }
+    out[id] = sum / (float)cnt;
+  }
+}
+
+template <int HALO>
+int launch_cbca_sep_h(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
+                      int direction, float* out, cudaStream_t st) {
+  constexpr size_t smem = cbca_sep_smem_bytes<HALO>();
+  CBMV_CUDA(cudaFuncSetAttribute(cbca_hwd_sep_kernel<HALO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  const int64_t tiles = (int64_t)((W + CS_TX - 1) / CS_TX) * ((H + CS_TY - 1) / CS_TY) *
+                        ((D + CS_TD - 1) / CS_TD);
+  cbca_hwd_sep_kernel<HALO><<<(unsigned)tiles, 256, smem, st>>>(lc, rc, in, (int)H, (int)W, D, direction, out);
+  return check_launch("cbca_sep");
+}
+
 // Winner-take-all (first minimum, as np.argmin) and the subpixel parabola
 // (post.cu:453-483).  One warp per pixel on [H,W,D] volumes.
 __global__ void wta_subpixel_hwd_kernel(const float* __restrict__ c, int64_t HW, int D,
@@ -656,6 +752,24 @@ int launch_cbca(const float* lc, const float* rc, const float* in, int64_t H, in
   return check_launch("cbca");
 }
 
+int launch_cbca_sep(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
+                    int direction, float* out, cudaStream_t st, int halo) {
+  CBMV_REQUIRE(H < (1 << 30) / CS_TY && W < (1 << 30) && (int64_t)((W + CS_TX - 1) / CS_TX) *
+                   ((H + CS_TY - 1) / CS_TY) * ((D + CS_TD - 1) / CS_TD) < ((int64_t)1 << 31),
+               CBMV_ERANGE, "cbca: volume too large");
+  switch (halo) {
+    case 1: return launch_cbca_sep_h<1>(lc, rc, in, H, W, D, direction, out, st);
+    case 2: return launch_cbca_sep_h<2>(lc, rc, in, H, W, D, direction, out, st);
+    case 3: return launch_cbca_sep_h<3>(lc, rc, in, H, W, D, direction, out, st);
+    case 4: return launch_cbca_sep_h<4>(lc, rc, in, H, W, D, direction, out, st);
+    case 5: return launch_cbca_sep_h<5>(lc, rc, in, H, W, D, direction, out, st);
+    case 6: return launch_cbca_sep_h<6>(lc, rc, in, H, W, D, direction, out, st);
+    case 7: return launch_cbca_sep_h<7>(lc, rc, in, H, W, D, direction, out, st);
+    case 8: return launch_cbca_sep_h<8>(lc, rc, in, H, W, D, direction, out, st);
+    default: return launch_cbca(lc, rc, in, H, W, D, CBMV_HWD, direction, out, st, halo);
+  }
+}
+
 int launch_wta_subpixel(const float* cost, int64_t H, int64_t W, int D, float* disp_int,
                         float* disp, cudaStream_t st) {
   wta_subpixel_hwd_kernel<<<grid_for(H * W * 32, 256), 256, 0, st>>>(cost, H * W, D, disp_int, disp);
@@ -742,6 +856,17 @@ extern "C" int cbmv_cbca(const float* crossL, const float* crossR, const float* 
   CBMV_REQUIRE(direction == 1 || direction == -1, CBMV_EINVAL, "direction must be +-1");
   CBMV_REQUIRE(layout == CBMV_HWD || layout == CBMV_DHW, CBMV_EINVAL, "bad layout");
   return launch_cbca(crossL, crossR, in, H, W, D, layout, direction, out, as_stream(stream));
+}
+
+extern "C" int cbmv_cbca_separable(const float* crossL, const float* crossR, const float* in, int64_t H,
+                                   int64_t W, int D, int L1, int direction, float* out, void* stream) {
+  REQ_PTR(crossL && crossR && in && out);
+  REQ_HW(H, W);
+  CBMV_REQUIRE(D > 0, CBMV_EINVAL, "bad D");
+  CBMV_REQUIRE(in != out, CBMV_EINVAL, "cbca: in and out must differ");
+  CBMV_REQUIRE(direction == 1 || direction == -1, CBMV_EINVAL, "direction must be +-1");
+  CBMV_REQUIRE(L1 >= 2 && L1 <= 9, CBMV_EINVAL, "cbca_separable: L1 must be in 2..9");
+  return launch_cbca_sep(crossL, crossR, in, H, W, D, direction, out, as_stream(stream), L1 - 1);
 }
 
 extern "C" int cbmv_wta(const float* cost, int64_t H, int64_t W, int D, int layout, float* disp,

@@ -32,6 +32,10 @@ int launch_sgm_combine(const SgmOut& o, int64_t n, const float* base, float scal
 // reaching further are still summed correctly, from global memory.
 int launch_cbca(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
                 int layout, int direction, float* out, cudaStream_t st, int halo = 5);
+// cbca on [H,W,D] in separable form (row sums, then column sums); arms of
+// at most `halo` pixels (L1 - 1), halo 1..8 (larger: the reference-order kernel)
+int launch_cbca_sep(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
+                    int direction, float* out, cudaStream_t st, int halo);
 int launch_wta_subpixel(const float* cost, int64_t H, int64_t W, int D, float* disp_int,
                         float* disp, cudaStream_t st);
 int launch_median(const float* in, int64_t H, int64_t W, int k, float* out, cudaStream_t st);

@@ -241,6 +241,12 @@ int cbmv_sgm(const float* imL, const float* imR, const float* in, int64_t H, int
 /* cbca (post.cu:399-450) on a volume of layout `layout`; in != out. */
 int cbmv_cbca(const float* crossL, const float* crossR, const float* in, int64_t H, int64_t W,
               int D, int layout, int direction, float* out, void* stream);
+/* cbca of the same arms and volume in separable form (row sums, then column
+ * sums of each support; the fused pipeline's default): [H,W,D] layout only,
+ * arms from cbmv_cross with the same L1 (2..9); in != out.  Equal to
+ * cbmv_cbca up to float rounding. */
+int cbmv_cbca_separable(const float* crossL, const float* crossR, const float* in, int64_t H,
+                        int64_t W, int D, int L1, int direction, float* out, void* stream);
 /* np.argmin over d (test.py:408-409), first minimum; disp float32 [H,W]. */
 int cbmv_wta(const float* cost, int64_t H, int64_t W, int D, int layout, float* disp,
              void* stream);
@@ -286,6 +292,10 @@ typedef struct cbmv_params {
   int cbca_i1, cbca_i2, median_i, median_w;
   float blur_sigma, blur_t;
   int direction;
+  /* CBCA summation: 0 (default) row sums then column sums of each support
+   * (separable form, rounding differs from the reference's); 1 one running
+   * float sum per support in the reference's order (post.cu:415-429). */
+  int exact_cbca;
 } cbmv_params;
 void cbmv_params_default(cbmv_params* p);
 

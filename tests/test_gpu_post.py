@@ -152,3 +152,26 @@ def test_dropin_post_module_runs_reference_driver(gpu, oracle_cpu, scene):
     from cbmv_b200 import libfeatextract as fte
     got_i = glue.postprocessing_mem_interp(post, fte, imgl, imgr, cost, -1)
     assert np.mean(np.abs(got_i - ref_i) <= 0.5) >= 0.99
+
+
+@pytest.mark.parametrize("direction", [-1, 1])
+def test_cbca_separable_matches_model_exactly(gpu, oracle_cpu, scene, direction):
+    """cbmv_cbca_separable (the fused pipeline's default CBCA) against the
+    oracle's float32 model of its summation order: bit-exact; against the
+    reference-order cbca: relative 1e-5."""
+    from cbmv_b200 import _lib
+    from oracle import post_model
+    imgl, imgr, vol, D = scene
+    lc, rc = _crosses(oracle_cpu, imgl, imgr)
+    H, W = imgl.shape
+    tl, tr, ts = _t(lc), _t(rc), _t(vol)
+    out = torch.empty_like(ts)
+    _lib.call("cbmv_cbca_separable", tl.data_ptr(), tr.data_ptr(), ts.data_ptr(), H, W, D, 6,
+              direction, out.data_ptr(), None)
+    ref_order = torch.empty_like(ts)
+    _lib.call("cbmv_cbca", tl.data_ptr(), tr.data_ptr(), ts.data_ptr(), H, W, D, _lib.HWD, direction,
+              ref_order.data_ptr(), None)
+    got = out.cpu().numpy()
+    assert np.array_equal(got, post_model.cbca_separable(lc, rc, vol, direction, 5))
+    ro = ref_order.cpu().numpy()
+    assert np.max(np.abs(got - ro) / np.maximum(np.abs(ro), 1e-30)) <= 1e-5

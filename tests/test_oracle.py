@@ -145,3 +145,30 @@ def test_rf_oracle_matches_sklearn(oracle_cpu):
     p0, leaves = oracle_cpu.rf_predict(ff, Xt, return_leaves=True)
     assert np.array_equal(leaves, np.stack([e.apply(Xt) for e in rf.estimators_], 1))
     assert np.array_equal(p0, rf.predict_proba(Xt)[:, 0])
+
+
+def test_separable_cbca_model_close_to_reference_order(oracle_cpu):
+    """The separable summation order (oracle/post_model.py, the fused
+    pipeline's default CBCA) against the reference's single running sum:
+    relative difference <= 1e-5 everywhere, most elements identical."""
+    from oracle import glue, post_model
+    from cbmv_b200 import synth
+    L, R, _, _ = synth.make_pair(seed=7, width=90, height=60, ndisp=16, planes=4, dmin=2, dmax=14)
+    imgl, imgr = glue.normalise_images(L, R)
+    o = oracle_cpu.post
+    a, b = o.CUDA_float_array(imgl), o.CUDA_float_array(imgr)
+    lc, rc = o.CUDA_float_array(np.zeros(1)), o.CUDA_float_array(np.zeros(1))
+    o.cross(a, lc, 6, .07)
+    o.cross(b, rc, 6, .07)
+    H, W, D = 60, 90, 16
+    vol = np.random.default_rng(4).random((H, W, D)).astype(np.float32)
+    for direction in (-1, 1):
+        dhw64 = np.ascontiguousarray(np.transpose(vol, (2, 0, 1))).astype(np.float64)
+        ref = np.empty(dhw64.shape, np.float64)
+        oracle_cpu.lib().orc_cbca(lc.a.ctypes.data, rc.a.ctypes.data, dhw64.ctypes.data, D, H, W,
+                                  direction, ref.ctypes.data)
+        ref = np.transpose(ref.astype(np.float32), (1, 2, 0))
+        got = post_model.cbca_separable(lc.a, rc.a, vol, direction, 5)
+        rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-30)
+        assert rel.max() <= 1e-5, rel.max()
+        assert np.mean(got == ref) > 0.5
