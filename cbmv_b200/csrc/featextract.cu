@@ -251,6 +251,104 @@ int launch_features_gather(const double* const* vols, const double* stats, int64
   return check_launch("features_gather");
 }
 
+// ---------------------------------------------- float32 row statistics
+// The classifier network's row statistics (min, 1/den) in float32 from
+// float32 volumes (the learned path never needs the float64 features):
+// statsf[(m*2 + view)*HW + p], min = 2^31 and 1/den = 0 where the row holds
+// only sentinels.  All four matchers in one launch (blockIdx.y = matcher).
+struct VolsF {
+  const float* v[4];
+};
+static __constant__ float kInvSigmaF32[4] = {(float)(1.0 / (2.0 * 8 * 8)), (float)(1.0 / 0.02),
+                                             (float)(1.0 / (2.0 * 100 * 100)), (float)(1.0 / (2.0 * 100 * 100))};
+
+__device__ __forceinline__ float2 stats_pair(float mn, float den) {
+  return mn == kRandMaxF ? make_float2(kRandMaxF, 0.0f) : make_float2(mn, 1.0f / den);
+}
+
+// view 0: one warp per pixel, the pixel's D costs are contiguous
+__global__ void stats_f32_left_kernel(VolsF vols, int64_t HW, int D, float2* __restrict__ statsf) {
+  const int m = blockIdx.y;
+  const float* __restrict__ vol = vols.v[m];
+  const float inv_sigma = kInvSigmaF32[m];
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < HW; p += nw) {
+    const float* r = vol + p * D;
+    float mn = kRandMaxF;
+    for (int d = lane; d < D; d += 32) mn = fminf(mn, __ldg(r + d));
+    for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    float den = 0.0f;
+    for (int d = lane; d < D; d += 32) {
+      const float t = __ldg(r + d) - mn;
+      den += __expf(-(t * t) * inv_sigma);
+    }
+    for (int o = 16; o; o >>= 1) den += __shfl_xor_sync(0xffffffffu, den, o);
+    if (lane == 0) statsf[(int64_t)(m * 2) * HW + p] = stats_pair(mn, den);
+  }
+}
+
+// view 1: right pixel x' of row y sees C[y, x' + d, d] (the fill C[0,0,0]
+// where x' + d >= W, featextract.cpp:115-152).  A CTA owns RS_PIX right
+// pixels of one row; for each 32-wide disparity chunk it stages the
+// (RS_PIX + 32) x 32 block of the volume the chunk's diagonals cross
+// (coalesced along d) and each thread walks its diagonal in shared memory.
+constexpr int RS_PIX = 256;
+
+__global__ void __launch_bounds__(RS_PIX) stats_f32_right_kernel(VolsF vols, int64_t H, int64_t W, int D,
+                                                                 float2* __restrict__ statsf) {
+  __shared__ float tile[(RS_PIX + 32) * 33];
+  const int m = blockIdx.y;
+  const float* __restrict__ vol = vols.v[m];
+  const float fill = __ldg(vol);
+  const float inv_sigma = kInvSigmaF32[m];
+  const int64_t nxb = (W + RS_PIX - 1) / RS_PIX;
+  const int64_t y = blockIdx.x / nxb;
+  const int64_t X0 = (blockIdx.x % nxb) * RS_PIX;
+  const int tid = threadIdx.x;
+  const int64_t xr = X0 + tid;
+  float mn = kRandMaxF, den = 0.0f;
+  for (int pass = 0; pass < 2; pass++) {
+    for (int d0 = 0; d0 < D; d0 += 32) {
+      __syncthreads();
+      for (int q = tid; q < (RS_PIX + 32) * 32; q += RS_PIX) {
+        const int i = q >> 5, j = q & 31;
+        const int64_t x = X0 + d0 + i;
+        const int d = d0 + j;
+        float v = fill;
+        if (x < W && d < D) v = __ldg(vol + (y * W + x) * D + d);
+        tile[i * 33 + j] = v;
+      }
+      __syncthreads();
+      if (xr < W) {
+        const int nj = D - d0 < 32 ? D - d0 : 32;
+        if (pass == 0) {
+          for (int j = 0; j < nj; j++) mn = fminf(mn, tile[(tid + j) * 33 + j]);
+        } else {
+          for (int j = 0; j < nj; j++) {
+            const float t = tile[(tid + j) * 33 + j] - mn;
+            den += __expf(-(t * t) * inv_sigma);
+          }
+        }
+      }
+    }
+  }
+  if (xr < W) statsf[(int64_t)(m * 2 + 1) * H * W + y * W + xr] = stats_pair(mn, den);
+}
+
+int launch_feature_stats_f32(const float* const* vols, int64_t H, int64_t W, int D, float2* statsf,
+                             cudaStream_t st) {
+  const VolsF v = {{vols[0], vols[1], vols[2], vols[3]}};
+  const int64_t HW = H * W;
+  const int64_t lblocks = (HW + 7) / 8;  // 8 warps per block, one pixel each
+  stats_f32_left_kernel<<<dim3((unsigned)(lblocks < 65535 * 16 ? lblocks : 65535 * 16), 4), 256, 0, st>>>(
+      v, HW, D, statsf);
+  const int64_t rblocks = H * ((W + RS_PIX - 1) / RS_PIX);
+  CBMV_REQUIRE(rblocks < ((int64_t)1 << 31), CBMV_ERANGE, "image too large for the statistics grid");
+  stats_f32_right_kernel<<<dim3((unsigned)rblocks, 4), RS_PIX, 0, st>>>(v, H, W, D, statsf);
+  return check_launch("feature_stats_f32");
+}
+
 int launch_feature_stats(const double* const* vols, int64_t H, int64_t W, int D, double* stats,
                          cudaStream_t st, float2* statsf) {
   const int64_t warps = 2 * H * W;

@@ -345,6 +345,13 @@ template int launch_sadsob_cost<double>(const int32_t*, const int32_t*, int64_t,
                                         int, double*, cudaStream_t);
 template int launch_zsad_cost<double>(const uint8_t*, const uint8_t*, const double*, const double*,
                                       int64_t, int64_t, int, int, int, double*, cudaStream_t);
+template int launch_ncc_cost<float>(const uint8_t*, const uint8_t*, const uint32_t*, const uint32_t*,
+                                    const double*, const double*, int64_t, int64_t, int, int, int, float*,
+                                    cudaStream_t);
+template int launch_sadsob_cost<float>(const int32_t*, const int32_t*, int64_t, int64_t, int, int, int,
+                                       float*, cudaStream_t);
+template int launch_zsad_cost<float>(const uint8_t*, const uint8_t*, const double*, const double*,
+                                     int64_t, int64_t, int, int, int, float*, cudaStream_t);
 
 }  // namespace cbmv
 

@@ -555,13 +555,17 @@ extern "C" int cbmv_mlp_status(const cbmv_mlp* n, int* status) {
 //            are the high and low bf16 parts of 0.5 * w4, z = D[0] + D[1] +
 //            b4, cost = 1 - sigmoid(z) = 1 / (1 + exp(z)).
 // The features themselves are formed in float32 (they enter the network as
-// bf16), from the float64 cost volumes and float32 row statistics (min,
-// 1/den), with one reciprocal 1/(c + e) shared by the left and right ratio.
+// bf16), from float32 cost volumes and float32 row statistics (min, 1/den),
+// with one reciprocal 1/(c + e) shared by the left and right ratio.
 // ====================================================================
 #include "features.cuh"
 
 namespace cbmv {
 namespace {
+
+struct FeatVolsF {
+  const float* v[4];
+};
 
 constexpr int kGroups = 4;                        // tiles in flight per CTA
 constexpr int kGroupThreads = 256;               // two threads per tile row
@@ -696,7 +700,7 @@ __device__ __forceinline__ void epilogue_hidden(uint32_t tlane, unsigned char* s
 }
 
 __global__ void __launch_bounds__(kInfThreads, 1)
-    features_mlp_kernel(FeatVols fv, const float2* __restrict__ statsf, int64_t H, int64_t W, int D,
+    features_mlp_kernel(FeatVolsF fv, const float2* __restrict__ statsf, int64_t H, int64_t W, int D,
                         const float* __restrict__ P, float* __restrict__ prob0, int* __restrict__ status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -763,8 +767,8 @@ __global__ void __launch_bounds__(kInfThreads, 1)
 #pragma unroll
       for (int i = 0; i < 2; i++) {
         const int m = 2 * half + i;
-        const double* vol = i == 0 ? (half ? fv.v[2] : fv.v[0]) : (half ? fv.v[3] : fv.v[1]);
-        const float c = (float)vol[tv];
+        const float* vol = i == 0 ? (half ? fv.v[2] : fv.v[0]) : (half ? fv.v[3] : fv.v[1]);
+        const float c = __ldg(vol + tv);
         const float2 sl = statsf[(int64_t)(m * 2) * HW + pv];
         const float2 sr = has_right ? statsf[(int64_t)(m * 2 + 1) * HW + pv - dv] : make_float2(kRandMaxF, 0.0f);
         const float inv_ce = __fdividef(1.0f, c + kEpsF[m]);
@@ -888,7 +892,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
 
 }  // namespace
 
-int launch_features_mlp(const double* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
+int launch_features_mlp(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
                         const cbmv_mlp* m, float* prob0, cudaStream_t st) {
   int dev = 0, sms = 0;
   CBMV_CUDA(cudaGetDevice(&dev));
@@ -899,7 +903,7 @@ int launch_features_mlp(const double* const* vols, const float2* statsf, int64_t
   const int64_t tiles = (H * W * D + 127) / 128;
   const int64_t need = (tiles + kGroups - 1) / kGroups;
   const int grid = (int)(need < sms ? need : sms);
-  FeatVols fv = {{vols[0], vols[1], vols[2], vols[3]}};
+  FeatVolsF fv = {{vols[0], vols[1], vols[2], vols[3]}};
   features_mlp_kernel<<<grid, kInfThreads, kSmInf, st>>>(fv, statsf, H, W, D, m->P, prob0, m->status);
   return check_launch("features_mlp");
 }

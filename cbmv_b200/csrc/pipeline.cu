@@ -266,10 +266,13 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
   return CBMV_OK;
 }
 
-// Steps 1-3 of the header comment: the four float64 cost volumes and their
-// per-pixel statistics in the context's workspace.
+// Steps 1-3 of the header comment: the four cost volumes and their
+// per-pixel statistics in the context's workspace.  f32 = false: float64
+// volumes and float64 statistics (the exact features of the random forest
+// and of the training samples); f32 = true: float32 volumes (in the first
+// half of each float64 buffer) and float32 statistics only, for the network.
 static int run_front(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
-                     int64_t H, int64_t W, int D, Work* wout) {
+                     int64_t H, int64_t W, int D, Work* wout, bool f32 = false) {
   RC(check_params(p));
   CBMV_REQUIRE(H > p->censw && W > p->censw, CBMV_EINVAL, "image %lldx%lld smaller than the census window",
                (long long)W, (long long)H);
@@ -288,13 +291,26 @@ static int run_front(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const 
   RC(launch_zsad_means(R, H, W, p->sadw, w.muR, st));
   RC(launch_sobel_i32(L, H, W, w.sobL, st));
   RC(launch_sobel_i32(R, H, W, w.sobR, st));
+  if (f32) {
+    float* v[4] = {(float*)w.vol[0], (float*)w.vol[1], (float*)w.vol[2], (float*)w.vol[3]};
+    RC(launch_census_cost<float>(w.descL, w.descR, H, W, D, p->censw, CBMV_HWD, v[0], st));
+    RC(launch_ncc_cost<float>(L, R, w.AL, w.AR, w.CL, w.CR, H, W, D, p->nccw, CBMV_HWD, v[1], st));
+    RC(launch_sadsob_cost<float>(w.sobL, w.sobR, H, W, D, p->sobw, CBMV_HWD, v[2], st));
+    RC(launch_zsad_cost<float>(L, R, w.muL, w.muR, H, W, D, p->sadw, CBMV_HWD, v[3], st));
+    CBMV_CUDA(cudaEventRecord(c->ev[1], st));
+    const float* vf[4] = {v[0], v[1], v[2], v[3]};
+    RC(launch_feature_stats_f32(vf, H, W, D, w.statsf, st));
+    CBMV_CUDA(cudaEventRecord(c->ev[2], st));
+    *wout = w;
+    return CBMV_OK;
+  }
   RC(launch_census_cost<double>(w.descL, w.descR, H, W, D, p->censw, CBMV_HWD, w.vol[0], st));
   RC(launch_ncc_cost<double>(L, R, w.AL, w.AR, w.CL, w.CR, H, W, D, p->nccw, CBMV_HWD, w.vol[1], st));
   RC(launch_sadsob_cost<double>(w.sobL, w.sobR, H, W, D, p->sobw, CBMV_HWD, w.vol[2], st));
   RC(launch_zsad_cost<double>(L, R, w.muL, w.muR, H, W, D, p->sadw, CBMV_HWD, w.vol[3], st));
   CBMV_CUDA(cudaEventRecord(c->ev[1], st));
   const double* vols[4] = {w.vol[0], w.vol[1], w.vol[2], w.vol[3]};
-  RC(launch_feature_stats(vols, H, W, D, w.stats, st, w.statsf));
+  RC(launch_feature_stats(vols, H, W, D, w.stats, st));
   CBMV_CUDA(cudaEventRecord(c->ev[2], st));
   *wout = w;
   return CBMV_OK;
@@ -332,9 +348,9 @@ extern "C" int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p
   cbmv_params def;
   p = params_or_default(p, &def);
   Work w;
-  RC(run_front(c, p, L, R, H, W, D, &w));
+  RC(run_front(c, p, L, R, H, W, D, &w, true));
   cudaStream_t st = c->stream;
-  const double* vols[4] = {w.vol[0], w.vol[1], w.vol[2], w.vol[3]};
+  const float* vols[4] = {(float*)w.vol[0], (float*)w.vol[1], (float*)w.vol[2], (float*)w.vol[3]};
   RC(launch_features_mlp(vols, w.statsf, H, W, D, m, w.volA, st));
   if (prob0)
     CBMV_CUDA(cudaMemcpyAsync(prob0, w.volA, sizeof(float) * H * W * D, cudaMemcpyDeviceToDevice, st));

@@ -29,7 +29,10 @@ int launch_zsad_cost(const uint8_t* L, const uint8_t* R, const double* ml, const
                      int64_t H, int64_t W, int D, int w, int layout, T* out, cudaStream_t st);
 int launch_feature_stats(const double* const* vols, int64_t H, int64_t W, int D, double* stats,
                          cudaStream_t st, float2* statsf = nullptr);
-int launch_features_mlp(const double* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
+// (min, 1/den) in float32 of float32 volumes, both views, the four matchers
+int launch_feature_stats_f32(const float* const* vols, int64_t H, int64_t W, int D, float2* statsf,
+                             cudaStream_t st);
+int launch_features_mlp(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
                         const cbmv_mlp* m, float* prob0, cudaStream_t st);
 // The 20 features (float32) of the samples idx[i] = (y*W + x)*D + d.
 int launch_features_gather(const double* const* vols, const double* stats, int64_t H, int64_t W,

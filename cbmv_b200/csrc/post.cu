@@ -340,7 +340,8 @@ __global__ void __launch_bounds__(256) cbca_hwd_tiled_kernel(
 // A CTA owns CS_TY x CS_TX pixels x 32 disparities (lane = disparity): it
 // forms R and C for its rows and HALO rows above and below into shared
 // memory, then the column sums.  Both sums run over fixed 2*HALO+1 taps,
-// masked to the support, in ascending order; with arms of at most
+// masked to the support, in ascending order, from register windows (a tile
+// row's inputs; a column's R and C); with arms of at most
 // HALO = L1 - 1 pixels every support element is within the taps.  The
 // result differs from the reference's single running float sum
 // (post.cu:415-429) by rounding only.
@@ -352,66 +353,92 @@ constexpr size_t cbca_sep_smem_bytes() {
 }
 
 template <int HALO>
-__global__ void __launch_bounds__(256) cbca_hwd_sep_kernel(
+__global__ void __launch_bounds__(256, 2) cbca_hwd_sep_kernel(
     const float* __restrict__ lc, const float* __restrict__ rc, const float* __restrict__ in, int H, int W,
     int D, int direction, float* __restrict__ out) {
-  constexpr int SR = CS_TY + 2 * HALO;
-  extern __shared__ float sR[];                                   // [SR][CS_TX][CS_TD]
+  constexpr int SR = CS_TY + 2 * HALO;   // rows of R: the tile's and HALO above and below
+  constexpr int NV = CS_TX + 2 * HALO;   // input columns a tile row needs
+  constexpr int G = 16;                  // output rows per column-sum window
+  static_assert(CS_TX == 8 && CS_TY % G == 0, "one warp per tile column");
+  extern __shared__ float sR[];                                       // [SR][CS_TX][CS_TD]
   uint8_t* sC = reinterpret_cast<uint8_t*>(sR + SR * CS_TX * CS_TD);  // [SR][CS_TX][CS_TD]
   const int ntd = (D + CS_TD - 1) / CS_TD, ntx = (W + CS_TX - 1) / CS_TX;
   const int64_t t = blockIdx.x;
   const int td = (int)(t % ntd), tx = (int)((t / ntd) % ntx), ty = (int)(t / ((int64_t)ntd * ntx));
   const int X0 = tx * CS_TX, Y0 = ty * CS_TY;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int d = td * CS_TD + lane, dd = d * direction;
+  const bool dok = d < D;
   const int64_t HW = (int64_t)H * W;
-  // row sums of rows Y0 - HALO .. Y0 + CS_TY + HALO - 1
-  for (int q = warp; q < SR * CS_TX; q += nwarp) {
-    const int r = q / CS_TX, c = q % CS_TX;
-    const int yy = Y0 - HALO + r, x = X0 + c, xm = x + dd;
-    float sum = 0.0f;
-    int cnt = 0;
-    if (yy >= 0 && yy < H && x < W && d < D && xm >= 0 && xm < W) {
-      const int64_t o = (int64_t)yy * W;
-      const int xxs = max((int)__ldg(lc + o + x), (int)__ldg(rc + o + xm) - dd);
-      const int xxt = min((int)__ldg(lc + HW + o + x), (int)__ldg(rc + HW + o + xm) - dd);
-      const float* row = in + o * D + d;
+  // 1. row sums: warp w forms R and C of tile rows w, w + 8, ... for all CS_TX columns
+  //    from the NV input values of its row, held in registers
+  for (int r = warp; r < SR; r += 8) {
+    const int yy = Y0 - HALO + r;
+    const bool rok = yy >= 0 && yy < H && dok;
+    float v[NV];
+    const int64_t o = (int64_t)(rok ? yy : 0) * W;
+    const float* row = in + o * D + d;
 #pragma unroll
-      for (int k = -HALO; k <= HALO; k++) {
-        const int xx = x + k;
-        if (xx > xxs && xx < xxt && xx >= 0 && xx < W) sum += __ldg(row + (int64_t)xx * D);
-      }
-      cnt = max(xxt - xxs - 1, 0);
+    for (int j = 0; j < NV; j++) {
+      const int xx = X0 - HALO + j;
+      v[j] = (rok && xx >= 0 && xx < W) ? __ldg(row + (int64_t)xx * D) : 0.0f;
     }
-    sR[(r * CS_TX + c) * CS_TD + lane] = sum;
-    sC[(r * CS_TX + c) * CS_TD + lane] = (uint8_t)cnt;
+#pragma unroll
+    for (int c = 0; c < CS_TX; c++) {
+      const int x = X0 + c, xm = x + dd;
+      float sum = 0.0f;
+      int cnt = 0;
+      if (rok && x < W && xm >= 0 && xm < W) {
+        // support row of (yy, x, d) in tap coordinates: ks < k < kt
+        const int ks = max((int)__ldg(lc + o + x), (int)__ldg(rc + o + xm) - dd) - x;
+        const int kt = min((int)__ldg(lc + HW + o + x), (int)__ldg(rc + HW + o + xm) - dd) - x;
+#pragma unroll
+        for (int k = -HALO; k <= HALO; k++)
+          if (k > ks && k < kt) sum += v[c + HALO + k];
+        cnt = max(kt - ks - 1, 0);
+      }
+      sR[(r * CS_TX + c) * CS_TD + lane] = sum;
+      sC[(r * CS_TX + c) * CS_TD + lane] = (uint8_t)cnt;
+    }
   }
   __syncthreads();
-  // column sums over the support rows
-  for (int q = warp; q < CS_TY * CS_TX; q += nwarp) {
-    const int cy = q / CS_TX, c = q % CS_TX;
-    const int y = Y0 + cy, x = X0 + c, xm = x + dd;
-    if (y >= H || x >= W || d >= D) continue;
-    const int64_t id = ((int64_t)y * W + x) * D + d;
-    if (xm < 0 || xm >= W) {
-      out[id] = __ldg(in + id);
-      continue;
-    }
-    const int64_t o = (int64_t)y * W;
-    const int yys = max((int)__ldg(lc + 2 * HW + o + x), (int)__ldg(rc + 2 * HW + o + xm));
-    const int yyt = min((int)__ldg(lc + 3 * HW + o + x), (int)__ldg(rc + 3 * HW + o + xm));
-    float sum = 0.0f;
-    int cnt = 0;
+  // 2. column sums: warp c owns tile column c; G output rows at a time from a
+  //    register window of G + 2*HALO rows of R and C
+  const int c = warp, x = X0 + c, xm = x + dd;
+  if (x >= W || !dok) return;
+  const bool xok = xm >= 0 && xm < W;
+#pragma unroll 1
+  for (int g0 = 0; g0 < CS_TY; g0 += G) {
+    float wr[G + 2 * HALO];
+    int wc[G + 2 * HALO];
 #pragma unroll
-    for (int k = -HALO; k <= HALO; k++) {
-      const int yy = y + k;
-      if (yy > yys && yy < yyt) {
-        const int i = ((cy + HALO + k) * CS_TX + c) * CS_TD + lane;
-        sum += sR[i];
-        cnt += sC[i];
-      }
+    for (int j = 0; j < G + 2 * HALO; j++) {
+      const int i = ((g0 + j) * CS_TX + c) * CS_TD + lane;
+      wr[j] = sR[i];
+      wc[j] = sC[i];
     }
-    out[id] = sum / (float)cnt;
+#pragma unroll
+    for (int cy = 0; cy < G; cy++) {
+      const int y = Y0 + g0 + cy;
+      if (y >= H) break;
+      const int64_t o = (int64_t)y * W;
+      const int64_t id = (o + x) * D + d;
+      if (!xok) {
+        out[id] = __ldg(in + id);
+        continue;
+      }
+      const int ks = max((int)__ldg(lc + 2 * HW + o + x), (int)__ldg(rc + 2 * HW + o + xm)) - y;
+      const int kt = min((int)__ldg(lc + 3 * HW + o + x), (int)__ldg(rc + 3 * HW + o + xm)) - y;
+      float sum = 0.0f;
+      int cnt = 0;
+#pragma unroll
+      for (int k = -HALO; k <= HALO; k++)
+        if (k > ks && k < kt) {
+          sum += wr[cy + HALO + k];
+          cnt += wc[cy + HALO + k];
+        }
+      out[id] = sum / (float)cnt;
+    }
   }
 }
 
