@@ -13,6 +13,8 @@
 //
 // Thread mapping: for [H,W,D] outputs consecutive threads take consecutive
 // d of a pixel (coalesced stores); for [D,H,W] they take consecutive x.
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace cbmv {
@@ -241,6 +243,101 @@ __global__ void zsad_cost_kernel(const uint8_t* __restrict__ L, const uint8_t* _
   out[vol_index(layout, c.y, c.x, c.d, H, W, D)] = cvt_out<T>(v);
 }
 
+// ------------------------------------------- float32 strip matchers
+// The three window matchers for the learned classifier's float32 volumes
+// ([H,W,D]): a warp owns 32 disparities (lane = d) of one row and walks a
+// strip of SX columns; the window's L and R columns sit in a register ring,
+// so each step loads one new column of each (L uniform across the warp, R
+// at x - d per lane).  Window sums are exact integers (SAD of Sobel
+// responses, sum of L*R, ZSAD as sum |25 (L - R) - (sum L - sum R)| / 25), so
+// the float32 result equals the rounding of the reference's value (its
+// float64 ZSAD chain differs from the exact quotient by ~1e-15 relative).
+// Validity and sentinels as in the reference kernels above.
+enum StripMode { kStripNcc = 0, kStripSadSob = 1, kStripZsad = 2 };
+constexpr int kStripX = 16;
+
+template <int MODE, int WIN>
+__global__ void __launch_bounds__(128) matcher_strip_kernel(
+    const void* __restrict__ Lp, const void* __restrict__ Rp, const uint32_t* __restrict__ Al,
+    const uint32_t* __restrict__ Ar, const double* __restrict__ Cl, const double* __restrict__ Cr,
+    const double* __restrict__ ml, const double* __restrict__ mr, int64_t H, int64_t W, int D,
+    float* __restrict__ out) {
+  using Px = typename std::conditional<MODE == kStripSadSob, int32_t, uint8_t>::type;
+  const Px* L = static_cast<const Px*>(Lp);
+  const Px* R = static_cast<const Px*>(Rp);
+  constexpr int r = WIN / 2;
+  const int64_t y = blockIdx.y;
+  const int64_t x0 = (int64_t)blockIdx.x * kStripX;
+  const int d = blockIdx.z * 128 + threadIdx.x;
+  if (d >= D) return;
+  // window rows, clamped into the image (values of clamped rows are never used)
+  int64_t rowoff[WIN];
+#pragma unroll
+  for (int wh = 0; wh < WIN; wh++) {
+    int64_t yy = y - r + wh;
+    yy = yy < 0 ? 0 : (yy >= H ? H - 1 : yy);
+    rowoff[wh] = yy * W;
+  }
+  int lw[WIN][WIN], rw[WIN][WIN];  // [ring slot][window row]
+  auto load_col = [&](int slot, int64_t c) {
+    const int64_t cl = c < 0 ? 0 : (c >= W ? W - 1 : c);
+    int64_t cr = c - d;
+    cr = cr < 0 ? 0 : (cr >= W ? W - 1 : cr);
+#pragma unroll
+    for (int wh = 0; wh < WIN; wh++) {
+      lw[slot][wh] = (int)__ldg(L + rowoff[wh] + cl);
+      rw[slot][wh] = (int)__ldg(R + rowoff[wh] + cr);
+    }
+  };
+#pragma unroll
+  for (int j = 0; j < WIN - 1; j++) load_col(j, x0 - r + j);
+  const bool row_ok = y >= r && y < H - WIN + r;
+#pragma unroll
+  for (int s = 0; s < kStripX; s++) {
+    const int64_t x = x0 + s;
+    if (x >= W) break;
+    load_col((s + WIN - 1) % WIN, x + r);
+    // ring slot (s + k) % WIN holds column x - r + k
+    float v = kRandMaxF;
+    if (row_ok && x >= d + r && x < W - WIN + r) {
+      if (MODE == kStripSadSob) {
+        int acc = 0;
+#pragma unroll
+        for (int k = 0; k < WIN; k++)
+#pragma unroll
+          for (int wh = 0; wh < WIN; wh++) acc += abs(lw[(s + k) % WIN][wh] - rw[(s + k) % WIN][wh]);
+        v = (float)acc;
+      } else if (MODE == kStripZsad) {
+        const int64_t pl = y * W + x;
+        const int m = (int)llrint(ml[pl] * (WIN * WIN)) - (int)llrint(mr[pl - d] * (WIN * WIN));
+        int acc = 0;
+#pragma unroll
+        for (int k = 0; k < WIN; k++)
+#pragma unroll
+          for (int wh = 0; wh < WIN; wh++)
+            acc += abs((WIN * WIN) * (lw[(s + k) % WIN][wh] - rw[(s + k) % WIN][wh]) - m);
+        v = (float)((double)acc / (double)(WIN * WIN));
+      } else {
+        const int64_t pl = y * W + x, pr = pl - d;
+        unsigned acc = 0;
+#pragma unroll
+        for (int k = 0; k < WIN; k++)
+#pragma unroll
+          for (int wh = 0; wh < WIN; wh++) acc += (unsigned)(lw[(s + k) % WIN][wh] * rw[(s + k) % WIN][wh]);
+        const double cl = Cl[pl], cr = Cr[pr];
+        if (isfinite(cl) && isfinite(cr)) {
+          const unsigned long long aa = (unsigned long long)Al[pl] * (unsigned long long)Ar[pr];
+          const double num = (double)(WIN * WIN) * (double)acc - (double)aa;
+          v = (float)(-num * cl * cr);
+        } else {
+          v = 1.0f;
+        }
+      }
+    }
+    out[(y * W + x) * D + d] = v;
+  }
+}
+
 int check_common(const void* a, const void* b, const void* out, int64_t H, int64_t W, int D, int w,
                  int dtype, int layout, int wmax) {
   CBMV_REQUIRE(a && b && out, CBMV_EINVAL, "null pointer argument");
@@ -332,6 +429,38 @@ int launch_zsad_cost(const uint8_t* L, const uint8_t* R, const double* ml, const
   zsad_cost_kernel<T><<<vol_grid(layout, H, W, D), kBlock, 0, st>>>(L, R, ml, mr, H, W, D, w, layout,
                                                                     out);
   return check_launch("zsad_cost");
+}
+
+template <int MODE, int WIN>
+static int launch_strip(const void* L, const void* R, const uint32_t* Al, const uint32_t* Ar, const double* Cl,
+                        const double* Cr, const double* ml, const double* mr, int64_t H, int64_t W, int D,
+                        float* out, cudaStream_t st) {
+  const dim3 grid((unsigned)((W + kStripX - 1) / kStripX), (unsigned)H, (unsigned)((D + 127) / 128));
+  matcher_strip_kernel<MODE, WIN><<<grid, 128, 0, st>>>(L, R, Al, Ar, Cl, Cr, ml, mr, H, W, D, out);
+  return check_launch("matcher_strip");
+}
+
+// float32 [H,W,D] matchers of the learned path: the strip kernels for the
+// default windows, the general kernels otherwise
+int launch_ncc_cost_f32(const uint8_t* L, const uint8_t* R, const uint32_t* Al, const uint32_t* Ar,
+                        const double* Cl, const double* Cr, int64_t H, int64_t W, int D, int w, float* out,
+                        cudaStream_t st) {
+  if (w == 3 && H <= 65535)
+    return launch_strip<kStripNcc, 3>(L, R, Al, Ar, Cl, Cr, nullptr, nullptr, H, W, D, out, st);
+  return launch_ncc_cost<float>(L, R, Al, Ar, Cl, Cr, H, W, D, w, CBMV_HWD, out, st);
+}
+int launch_sadsob_cost_f32(const int32_t* SL, const int32_t* SR, int64_t H, int64_t W, int D, int w, float* out,
+                           cudaStream_t st) {
+  if (w == 5 && H <= 65535)
+    return launch_strip<kStripSadSob, 5>(SL, SR, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, H, W, D,
+                                         out, st);
+  return launch_sadsob_cost<float>(SL, SR, H, W, D, w, CBMV_HWD, out, st);
+}
+int launch_zsad_cost_f32(const uint8_t* L, const uint8_t* R, const double* ml, const double* mr, int64_t H,
+                         int64_t W, int D, int w, float* out, cudaStream_t st) {
+  if (w == 5 && H <= 65535)
+    return launch_strip<kStripZsad, 5>(L, R, nullptr, nullptr, nullptr, nullptr, ml, mr, H, W, D, out, st);
+  return launch_zsad_cost<float>(L, R, ml, mr, H, W, D, w, CBMV_HWD, out, st);
 }
 
 template int launch_census_cost<double>(const ulonglong2*, const ulonglong2*, int64_t, int64_t, int,

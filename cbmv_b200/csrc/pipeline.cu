@@ -294,9 +294,9 @@ static int run_front(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const 
   if (f32) {
     float* v[4] = {(float*)w.vol[0], (float*)w.vol[1], (float*)w.vol[2], (float*)w.vol[3]};
     RC(launch_census_cost<float>(w.descL, w.descR, H, W, D, p->censw, CBMV_HWD, v[0], st));
-    RC(launch_ncc_cost<float>(L, R, w.AL, w.AR, w.CL, w.CR, H, W, D, p->nccw, CBMV_HWD, v[1], st));
-    RC(launch_sadsob_cost<float>(w.sobL, w.sobR, H, W, D, p->sobw, CBMV_HWD, v[2], st));
-    RC(launch_zsad_cost<float>(L, R, w.muL, w.muR, H, W, D, p->sadw, CBMV_HWD, v[3], st));
+    RC(launch_ncc_cost_f32(L, R, w.AL, w.AR, w.CL, w.CR, H, W, D, p->nccw, v[1], st));
+    RC(launch_sadsob_cost_f32(w.sobL, w.sobR, H, W, D, p->sobw, v[2], st));
+    RC(launch_zsad_cost_f32(L, R, w.muL, w.muR, H, W, D, p->sadw, v[3], st));
     CBMV_CUDA(cudaEventRecord(c->ev[1], st));
     const float* vf[4] = {v[0], v[1], v[2], v[3]};
     RC(launch_feature_stats_f32(vf, H, W, D, w.statsf, st));
@@ -357,6 +357,19 @@ extern "C" int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p
   CBMV_CUDA(cudaEventRecord(c->ev[3], st));
   RC(run_post(c, p, L, R, H, W, D, w, disp));
   CBMV_CUDA(cudaEventRecord(c->ev[4], st));
+  return CBMV_OK;
+}
+
+extern "C" int cbmv_ctx_volumes_f32(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
+                                    int64_t H, int64_t W, int D, float* out) {
+  CBMV_REQUIRE(c && L && R && out, CBMV_EINVAL, "null pointer argument");
+  cbmv_params def;
+  p = params_or_default(p, &def);
+  Work w;
+  RC(run_front(c, p, L, R, H, W, D, &w, true));
+  const size_t V = (size_t)H * W * D;
+  for (int m = 0; m < 4; m++)
+    CBMV_CUDA(cudaMemcpyAsync(out + m * V, w.vol[m], sizeof(float) * V, cudaMemcpyDeviceToDevice, c->stream));
   return CBMV_OK;
 }
 

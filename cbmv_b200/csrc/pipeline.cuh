@@ -27,6 +27,14 @@ int launch_zsad_means(const uint8_t* img, int64_t H, int64_t W, int w, double* m
 template <class T>
 int launch_zsad_cost(const uint8_t* L, const uint8_t* R, const double* ml, const double* mr,
                      int64_t H, int64_t W, int D, int w, int layout, T* out, cudaStream_t st);
+// float32 [H,W,D] window matchers for the learned path (strip kernels)
+int launch_ncc_cost_f32(const uint8_t* L, const uint8_t* R, const uint32_t* Al, const uint32_t* Ar,
+                        const double* Cl, const double* Cr, int64_t H, int64_t W, int D, int w, float* out,
+                        cudaStream_t st);
+int launch_sadsob_cost_f32(const int32_t* SL, const int32_t* SR, int64_t H, int64_t W, int D, int w, float* out,
+                           cudaStream_t st);
+int launch_zsad_cost_f32(const uint8_t* L, const uint8_t* R, const double* ml, const double* mr, int64_t H,
+                         int64_t W, int D, int w, float* out, cudaStream_t st);
 int launch_feature_stats(const double* const* vols, int64_t H, int64_t W, int D, double* stats,
                          cudaStream_t st, float2* statsf = nullptr);
 // (min, 1/den) in float32 of float32 volumes, both views, the four matchers

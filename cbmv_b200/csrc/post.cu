@@ -353,12 +353,12 @@ constexpr size_t cbca_sep_smem_bytes() {
 }
 
 template <int HALO>
-__global__ void __launch_bounds__(256, 2) cbca_hwd_sep_kernel(
+__global__ void __launch_bounds__(256, 4) cbca_hwd_sep_kernel(
     const float* __restrict__ lc, const float* __restrict__ rc, const float* __restrict__ in, int H, int W,
     int D, int direction, float* __restrict__ out) {
   constexpr int SR = CS_TY + 2 * HALO;   // rows of R: the tile's and HALO above and below
   constexpr int NV = CS_TX + 2 * HALO;   // input columns a tile row needs
-  constexpr int G = 16;                  // output rows per column-sum window
+  constexpr int G = 8;                   // output rows per column-sum window
   static_assert(CS_TX == 8 && CS_TY % G == 0, "one warp per tile column");
   extern __shared__ float sR[];                                       // [SR][CS_TX][CS_TD]
   uint8_t* sC = reinterpret_cast<uint8_t*>(sR + SR * CS_TX * CS_TD);  // [SR][CS_TX][CS_TD]

@@ -55,6 +55,18 @@ class StereoPipeline:
                   prob_out.data_ptr() if prob_out is not None else None)
         return _dev.result(disp, host)
 
+    def volumes_f32(self, left, right, ndisp):
+        """The learned path's four float32 matcher volumes (census, NCC,
+        SAD-on-Sobel, ZSAD) as a device tensor [4,H,W,D]."""
+        import torch
+        l, _ = _dev.to_device(left, np.uint8)
+        r, _ = _dev.to_device(right, np.uint8)
+        H, W = l.shape
+        out = torch.empty((4, H, W, int(ndisp)), dtype=torch.float32, device="cuda")
+        _lib.call("cbmv_ctx_volumes_f32", self.ctx, ctypes.byref(self.params), l.data_ptr(), r.data_ptr(),
+                  H, W, int(ndisp), out.data_ptr())
+        return out
+
     def features_at(self, left, right, ndisp, idx):
         """20 float32 features of the samples idx = (y*W + x)*D + d (device tensor [n,20])."""
         import torch

@@ -324,6 +324,14 @@ int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p, const uin
 /* Training-sample emission (the GPU counterpart of train.py:100-273): the
  * 20 float32 features of the samples idx[i] = (y*W + x)*D + d of the pair
  * (L, R); idx int64 [n], out float32 [n,20], device memory. */
+/* The four float32 matcher volumes of the learned path (census, NCC,
+ * SAD-on-Sobel, ZSAD; the reference's test.py:122-138 costs, [H,W,D]
+ * layout) into out float32 [4,H,W,D], device memory.  Census, NCC and
+ * SAD-on-Sobel equal the float32 rounding of the reference's values; ZSAD is
+ * the exact window quotient, within one float32 unit of it. */
+int cbmv_ctx_volumes_f32(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
+                         int64_t H, int64_t W, int D, float* out);
+
 int cbmv_ctx_features_at(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
                          int64_t H, int64_t W, int D, const int64_t* idx, int64_t n, float* out);
 

@@ -72,3 +72,22 @@ def test_bad_arguments_raise(gpu):
         mtc.census(L, R, 8, 13)  # 169 bits > 128
     with pytest.raises(CbmvError):
         mtc.zsad(L, R, 8, 4)
+
+
+@pytest.mark.parametrize("D", [24, 130])
+def test_learned_path_f32_volumes(gpu, small_pair, D):
+    """The learned path's float32 volumes (strip kernels for NCC, SAD-on-Sobel
+    and ZSAD) against the float64 matchers rounded to float32: census, NCC
+    and SAD-on-Sobel bit-exact, ZSAD within one float32 unit."""
+    from cbmv_b200 import libmatchers as mtc, libfeatextract as fte
+    from cbmv_b200.pipeline import StereoPipeline
+    L, R, _, _ = small_pair
+    vols = StereoPipeline().volumes_f32(L, R, D).cpu().numpy()
+    ref = [mtc.census(L, R, D, 11), fte.swap_axes(mtc.nccNister(L, R, D, 3)),
+           fte.swap_axes(mtc.sadsob(mtc.sobel(L), mtc.sobel(R), D, 5)), fte.swap_axes(mtc.zsad(L, R, D, 5))]
+    for m in range(3):
+        assert np.array_equal(vols[m], ref[m].astype(np.float32)), m
+    z, zr = vols[3], ref[3].astype(np.float32)
+    ulp = np.abs(z.view(np.int32).astype(np.int64) - zr.view(np.int32).astype(np.int64))
+    assert ulp.max() <= 1
+    assert np.mean(ulp == 0) > 0.999
