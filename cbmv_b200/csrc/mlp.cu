@@ -539,8 +539,9 @@ extern "C" int cbmv_mlp_status(const cbmv_mlp* n, int* status) {
 // others compute features or epilogues.  Threads r and r + 128 of a group
 // share row r of its tile: each forms the features of two matchers of
 // sample r, then handles half of that row's columns in each epilogue.  The
-// group's first thread issues its MMAs and commits them to the group's
-// mbarrier; groups synchronise on named barriers only.
+// group's first thread issues its MMAs, commits them to the group's
+// mbarrier and alone polls it; the others wait on the group's named barrier
+// (no issue slots spent spinning), which also hands them the poll's result.
 //
 // Arithmetic, per layer (the float32 accumulator in tensor memory):
 //   layer 1  K = 32: 20 normalised features, two constant-one columns whose
@@ -800,7 +801,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       umma::mma_bf16(tacc, dA0 + 2, dW1 + 2, id128, true);
       umma::mma_commit(bar);
     }
-    ok = group_all(g, umma::mbar_wait(bar, phase, kWaitLimit));
+    ok = group_all(g, leader ? umma::mbar_wait(bar, phase, kWaitLimit) : true);
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
@@ -818,7 +819,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA1 + 2 * kk, dW21 + 2 * kk, id128, true);
       umma::mma_commit(bar);
     }
-    ok = group_all(g, umma::mbar_wait(bar, phase, kWaitLimit));
+    ok = group_all(g, leader ? umma::mbar_wait(bar, phase, kWaitLimit) : true);
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
@@ -837,7 +838,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA1 + 2 * kk, dW31 + 2 * kk, id64, true);
       umma::mma_commit(bar);
     }
-    ok = group_all(g, umma::mbar_wait(bar, phase, kWaitLimit));
+    ok = group_all(g, leader ? umma::mbar_wait(bar, phase, kWaitLimit) : true);
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
@@ -853,7 +854,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc + 64, dA0 + 2 * kk, dW4 + 2 * kk, id16, kk > 0);
       umma::mma_commit(bar);
     }
-    ok = group_all(g, umma::mbar_wait(bar, phase, kWaitLimit));
+    ok = group_all(g, leader ? umma::mbar_wait(bar, phase, kWaitLimit) : true);
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
@@ -880,9 +881,11 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     if (x >= W) x -= W;
   }
   if (!ok) {
-    if (leader) atomicExch(status, 1);
     // let this group's MMAs still in flight finish (bounded) before the memory is freed
-    umma::mbar_wait(bar, phase ^ 1u, kWaitLimit);
+    if (leader) {
+      atomicExch(status, 1);
+      umma::mbar_wait(bar, phase ^ 1u, kWaitLimit);
+    }
   }
   umma::tc_fence_before();
   __syncthreads();

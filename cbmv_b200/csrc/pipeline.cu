@@ -97,6 +97,7 @@ struct Work {
   double *CL, *CR, *muL, *muR;
   int32_t *sobL, *sobR;
   double* vol[4];
+  bool f32;  // matcher volumes in float32
   double* stats;
   float2* statsf;  // (min, 1/den) in float32 for the classifier network
   float *volA, *volB;
@@ -105,7 +106,9 @@ struct Work {
   double* mom;
 };
 
-Work carve(void* base, int64_t H, int64_t W, int D, size_t* bytes) {
+// f32: the four matcher volumes hold float32 (4 B per (p,d) each) instead of
+// float64; the four SGM direction volumes then alias them one to one.
+Work carve(void* base, int64_t H, int64_t W, int D, size_t* bytes, bool f32 = false) {
   Carve c{(char*)base};
   Work w;
   const size_t HW = (size_t)H * W, V = HW * (size_t)D;
@@ -119,7 +122,8 @@ Work carve(void* base, int64_t H, int64_t W, int D, size_t* bytes) {
   w.muR = c.take<double>(HW);
   w.sobL = c.take<int32_t>(HW);
   w.sobR = c.take<int32_t>(HW);
-  for (int m = 0; m < 4; m++) w.vol[m] = c.take<double>(V);
+  for (int m = 0; m < 4; m++) w.vol[m] = f32 ? (double*)c.take<float>(V) : c.take<double>(V);
+  w.f32 = f32;
   w.stats = c.take<double>(16 * HW);
   w.statsf = c.take<float2>(8 * HW);
   w.volA = c.take<float>(V);
@@ -241,9 +245,10 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
   }
   SgmParams sp{p->pi1, p->pi2, p->tau_so, p->alpha1, p->sgm_q1, p->sgm_q2, p->direction};
   SgmGrad g{w.grad, w.grad + HW, w.grad + 2 * HW, w.grad + 3 * HW};
-  // the four direction volumes reuse the float64 cost volumes, dead by now
+  // the four direction volumes reuse the cost volumes, dead by now
   const int64_t V = HW * D;
-  SgmOut so{{(float*)w.vol[0], (float*)w.vol[0] + V, (float*)w.vol[1], (float*)w.vol[1] + V}};
+  SgmOut so = w.f32 ? SgmOut{{(float*)w.vol[0], (float*)w.vol[1], (float*)w.vol[2], (float*)w.vol[3]}}
+                    : SgmOut{{(float*)w.vol[0], (float*)w.vol[0] + V, (float*)w.vol[1], (float*)w.vol[1] + V}};
   if (p->sgm_i > 0) RC(launch_sgm_grad(w.imL, w.imR, H, W, &g, st));
   for (int i = 0; i < p->sgm_i; i++) {
     // out = ((L0 + L1 + L2) + L3) / 4   (test.py:379-383)
@@ -278,9 +283,9 @@ static int run_front(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const 
                (long long)W, (long long)H);
   CBMV_REQUIRE(H <= 65535 && D >= 1 && D <= 1024, CBMV_ERANGE, "H must be <= 65535 and D in 1..1024");
   size_t bytes = 0;
-  carve(nullptr, H, W, D, &bytes);
+  carve(nullptr, H, W, D, &bytes, f32);
   RC(ensure_workspace(c, bytes));
-  Work w = carve(c->ws, H, W, D, &bytes);
+  Work w = carve(c->ws, H, W, D, &bytes, f32);
   cudaStream_t st = c->stream;
   CBMV_CUDA(cudaEventRecord(c->ev[0], st));
   RC(launch_census_desc(L, H, W, p->censw, w.descL, st));

@@ -149,6 +149,18 @@ def pair_694x554(seed=0):
     return make_pair(**p)
 
 
+def pair_1482x994(seed=1):
+    p = dict(PAIR_1482x994)
+    p["seed"] = seed
+    return make_pair(**p)
+
+
+def pair_2880x1988(seed=5):
+    p = dict(PAIR_2880x1988)
+    p["seed"] = seed
+    return make_pair(**p)
+
+
 def batch_specs(n=64, seed0=4000):
     """Uneven batch: W~U[320,1500], H~U[240,1000], D in {64,128,192,256}, planes~U[6,24]."""
     out = []
