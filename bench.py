@@ -401,6 +401,90 @@ def run_reference(a, ws, rank, local):
     }
 
 
+def _make_pair_spec(spec):
+    from cbmv_b200 import synth
+    return synth.make_pair(**spec)
+
+
+def run_batch(a, ws, rank, local):
+    """--batch: 64 seeded pairs of uneven size (W~U[320,1500], H~U[240,1000],
+    D in {64,128,192,256}, seeds 4000..4063) through the learned path as one
+    CUDA graph launch per step, launch shape from the autotuner; per-pair
+    latency p50/p99 beside the aggregate throughput, and the same pairs run
+    one after another (one pipeline call each) for comparison."""
+    import multiprocessing as mp
+    import torch
+    from cbmv_b200 import _lib, evaluate, synth
+    from cbmv_b200.batch import StereoBatch, tune_batch
+    from cbmv_b200.mlp import GpuMlp
+    from cbmv_b200.pipeline import StereoPipeline
+    specs = synth.batch_specs(a.batch_pairs, 4000 + 1000 * rank)
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        pairs = pool.map(_make_pair_spec, specs)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    shapes = [(sp["height"], sp["width"], sp["ndisp"]) for sp in specs]
+    units = int(sum(h * w * d for h, w, d in shapes))
+    lefts = [torch.from_numpy(p[0]).to(dev) for p in pairs]
+    rights = [torch.from_numpy(p[1]).to(dev) for p in pairs]
+    net = GpuMlp.load(a.mlp)
+    t_tune = time.perf_counter()
+    tune = tune_batch(shapes, net, lefts, rights, log=lambda m: print(m, file=sys.stderr))
+    t_tune = time.perf_counter() - t_tune
+    b = StereoBatch(shapes, streams=tune["streams"])
+    prm = _lib.default_params(mlp_ctas=tune["mlp_ctas"])
+    st = torch.cuda.current_stream()
+    for _ in range(a.warmup):
+        b.run_mlp(net, lefts, rights, prm)
+    barrier(ws)
+    spans, pair_ms, done_ms = [], [], []
+    with Clocks(local) as clk:
+        for k in range(a.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            b.run_mlp(net, lefts, rights, prm)
+            e1.record(st)
+            e1.synchronize()
+            spans.append(e0.elapsed_time(e1))
+            t = b.timings()
+            pair_ms.append(t["pair_ms"])
+            done_ms.append(t["done_ms"])
+        barrier(ws)
+    ms = reduce_max(float(np.mean(spans)), ws)
+    disp = [t.cpu().numpy() for t in b.disp]
+    bad = float(np.mean([evaluate.bad_x(d, p[2], p[3]) for d, p in zip(disp, pairs)]))
+    pair_ms, done_ms = np.concatenate(pair_ms), np.concatenate(done_ms)
+    # the same pairs one pipeline call each, back to back on one stream
+    pipe = StereoPipeline()
+    outs = [torch.empty(l.shape, dtype=torch.float32, device=dev) for l in lefts]
+    for i in range(len(shapes)):
+        pipe.run_mlp(net, lefts[i], rights[i], shapes[i][2], disp_out=outs[i])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for i in range(len(shapes)):
+        pipe.run_mlp(net, lefts[i], rights[i], shapes[i][2], disp_out=outs[i])
+    e1.record(st)
+    e1.synchronize()
+    seq_ms = e0.elapsed_time(e1)
+    same = all(np.array_equal(o.cpu().numpy(), d) for o, d in zip(outs, disp))
+    return {
+        "metric": "pixel·disparities/s, %d uneven pairs in one CUDA graph launch (learned classifier)" % len(shapes),
+        "value": units * ws / (ms / 1e3), "unit": "pixel·disparities/s", "n_gpus": ws, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16/f32", "data": "synthetic (seeded uneven pairs, seeds 4000+)",
+        "config": {"workload": "%d pairs W~U[320,1500] H~U[240,1000] D in {64,128,192,256}" % len(shapes),
+                   "units": units, "autotune": {k: tune[k] for k in ("streams", "mlp_ctas", "ms", "tried")},
+                   "autotune_seconds": t_tune, "parallelism": "pairs over concurrent contexts in one graph"},
+        "latency_ms": {"pair_p50": float(np.percentile(pair_ms, 50)), "pair_p99": float(np.percentile(pair_ms, 99)),
+                       "done_p50": float(np.percentile(done_ms, 50)), "done_p99": float(np.percentile(done_ms, 99)),
+                       "note": "pair: a pair's first to last kernel; done: graph start to the pair's end"},
+        "sequential_ms": seq_ms, "sequential_value": units / (seq_ms / 1e3),
+        "identical_to_sequential": bool(same), "bad2_nonocc_mean": bad,
+        "gpu_launches": "1 graph launch per step", "clocks": clk.summary(),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -412,6 +496,9 @@ def main():
     ap.add_argument("--classifier", choices=["both", "rf", "mlp"], default="both",
                     help="classifier paths to time (both: the MLP is the headline when it matches "
                          "the RF's held-out bad-2.0)")
+    ap.add_argument("--batch", action="store_true",
+                    help="the batched workload: uneven pairs in one graph launch (autotuned)")
+    ap.add_argument("--batch-pairs", type=int, default=64)
     ap.add_argument("--no-eval", action="store_true",
                     help="skip the held-out bad-2.0 comparison (the RF stays the headline)")
     ap.add_argument("--cpu-rows", type=int, default=48)
@@ -425,6 +512,8 @@ def main():
             a.steps = 3
         a.warmup = min(a.warmup, 1)
         line = run_reference(a, ws, rank, local)
+    elif a.batch:
+        line = run_batch(a, ws, rank, local)
     else:
         line = run_cbmv(a, ws, rank, local)
     if rank == 0 and line is not None:

@@ -32,7 +32,7 @@ class cbmv_params(ctypes.Structure):
                 ("alpha1", _flt), ("tau_so", _flt), ("sgm_i", _int), ("L1", _int),
                 ("tau1", _flt), ("cbca_i1", _int), ("cbca_i2", _int), ("median_i", _int),
                 ("median_w", _int), ("blur_sigma", _flt), ("blur_t", _flt), ("direction", _int),
-                ("exact_cbca", _int)]
+                ("exact_cbca", _int), ("mlp_ctas", _int)]
 
 
 # name -> argtypes (all return int status unless listed in _RESTYPE)
@@ -96,6 +96,10 @@ SIGNATURES = {
     "cbmv_run_mlp": [_vp, _vp, ctypes.POINTER(cbmv_params), _vp, _vp, _i64, _i64, _int, _vp, _vp],
     "cbmv_ctx_features_at": [_vp, ctypes.POINTER(cbmv_params), _vp, _vp, _i64, _i64, _int, _vp, _i64, _vp],
     "cbmv_ctx_volumes_f32": [_vp, ctypes.POINTER(cbmv_params), _vp, _vp, _i64, _i64, _int, _vp],
+    "cbmv_batch_create": [_int, _vp, _vp, _vp, _int, _vp],
+    "cbmv_batch_destroy": [_vp],
+    "cbmv_batch_run_mlp": [_vp, _vp, ctypes.POINTER(cbmv_params), _vp, _vp, _vp, _vp],
+    "cbmv_batch_timings": [_vp, _vp, _vp, _vp],
 }
 _RESTYPE = {"cbmv_last_error": ctypes.c_char_p, "cbmv_version": ctypes.c_char_p,
             "cbmv_params_default": None, "cbmv_census_static_max_pixels": ctypes.c_int64}

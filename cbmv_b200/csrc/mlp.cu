@@ -896,7 +896,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
 }  // namespace
 
 int launch_features_mlp(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
-                        const cbmv_mlp* m, float* prob0, cudaStream_t st) {
+                        const cbmv_mlp* m, float* prob0, cudaStream_t st, int max_ctas) {
   int dev = 0, sms = 0;
   CBMV_CUDA(cudaGetDevice(&dev));
   CBMV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -905,7 +905,8 @@ int launch_features_mlp(const float* const* vols, const float2* statsf, int64_t 
   CBMV_REQUIRE(((uintptr_t)statsf & 7) == 0, CBMV_EINVAL, "feature statistics must be 8-byte aligned");
   const int64_t tiles = (H * W * D + 127) / 128;
   const int64_t need = (tiles + kGroups - 1) / kGroups;
-  const int grid = (int)(need < sms ? need : sms);
+  const int cap = max_ctas > 0 && max_ctas < sms ? max_ctas : sms;
+  const int grid = (int)(need < cap ? need : cap);
   FeatVolsF fv = {{vols[0], vols[1], vols[2], vols[3]}};
   features_mlp_kernel<<<grid, kInfThreads, kSmInf, st>>>(fv, statsf, H, W, D, m->P, prob0, m->status);
   return check_launch("features_mlp");

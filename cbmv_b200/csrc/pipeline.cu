@@ -19,6 +19,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "common.cuh"
@@ -50,6 +51,7 @@ extern "C" void cbmv_params_default(cbmv_params* p) {
   p->blur_t = 1.3f;
   p->direction = -1;  // test.py:501
   p->exact_cbca = 0;
+  p->mlp_ctas = 0;
 }
 
 struct cbmv_ctx {
@@ -356,7 +358,7 @@ extern "C" int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p
   RC(run_front(c, p, L, R, H, W, D, &w, true));
   cudaStream_t st = c->stream;
   const float* vols[4] = {(float*)w.vol[0], (float*)w.vol[1], (float*)w.vol[2], (float*)w.vol[3]};
-  RC(launch_features_mlp(vols, w.statsf, H, W, D, m, w.volA, st));
+  RC(launch_features_mlp(vols, w.statsf, H, W, D, m, w.volA, st, p->mlp_ctas));
   if (prob0)
     CBMV_CUDA(cudaMemcpyAsync(prob0, w.volA, sizeof(float) * H * W * D, cudaMemcpyDeviceToDevice, st));
   CBMV_CUDA(cudaEventRecord(c->ev[3], st));
@@ -389,4 +391,203 @@ extern "C" int cbmv_ctx_features_at(cbmv_ctx* c, const cbmv_params* p, const uin
   RC(run_front(c, p, L, R, H, W, D, &w));
   const double* vols[4] = {w.vol[0], w.vol[1], w.vol[2], w.vol[3]};
   return launch_features_gather(vols, w.stats, H, W, D, idx, n, out, c->stream);
+}
+
+// ====================================================================
+// Batches: many pairs of uneven size in one CUDA graph launch.
+// ====================================================================
+struct cbmv_batch {
+  int n = 0;
+  std::vector<int64_t> H, W;
+  std::vector<int> D;
+  std::vector<std::vector<int>> order;  // context -> its pairs, in run order
+  std::vector<cudaStream_t> streams;
+  std::vector<cbmv_ctx*> ctx;
+  cudaEvent_t fork = nullptr, t0 = nullptr;
+  std::vector<cudaEvent_t> ev_start, ev_end, join;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  // what the graph was captured with
+  std::vector<const uint8_t*> L, R;
+  std::vector<float*> disp;
+  const cbmv_mlp* net = nullptr;
+  cbmv_params params{};
+  // the graph is captured on and launched into the batch's own stream (the
+  // caller's may be the legacy default stream, which cannot be captured),
+  // ordered after and before the caller's stream by events
+  cudaStream_t origin = nullptr;
+  cudaEvent_t in_ev = nullptr, out_ev = nullptr;
+};
+
+static void batch_free(cbmv_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (cbmv_ctx* c : b->ctx) cbmv_ctx_destroy(c);
+  for (cudaStream_t s : b->streams) cudaStreamDestroy(s);
+  for (cudaEvent_t e : b->ev_start) cudaEventDestroy(e);
+  for (cudaEvent_t e : b->ev_end) cudaEventDestroy(e);
+  for (cudaEvent_t e : b->join) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->t0) cudaEventDestroy(b->t0);
+  if (b->in_ev) cudaEventDestroy(b->in_ev);
+  if (b->out_ev) cudaEventDestroy(b->out_ev);
+  if (b->origin) cudaStreamDestroy(b->origin);
+  delete b;
+}
+
+extern "C" int cbmv_batch_create(int n, const int64_t* H, const int64_t* W, const int* D, int streams,
+                                 cbmv_batch** out) {
+  CBMV_REQUIRE(out && H && W && D, CBMV_EINVAL, "null pointer argument");
+  CBMV_REQUIRE(n >= 1 && n <= 4096, CBMV_EINVAL, "batch of %d pairs (1..4096)", n);
+  CBMV_REQUIRE(streams >= 1 && streams <= 32, CBMV_EINVAL, "streams must be in 1..32");
+  for (int i = 0; i < n; i++)
+    CBMV_REQUIRE(H[i] > 11 && W[i] > 11 && H[i] <= 65535 && D[i] >= 1 && D[i] <= 1024, CBMV_EINVAL,
+                 "pair %d: bad shape %lldx%lld, D=%d", i, (long long)W[i], (long long)H[i], D[i]);
+  cbmv_batch* b = new cbmv_batch();
+  b->n = n;
+  b->H.assign(H, H + n);
+  b->W.assign(W, W + n);
+  b->D.assign(D, D + n);
+  const int K = std::min(streams, n);
+  // longest first onto the least-loaded context
+  std::vector<int> idx(n);
+  for (int i = 0; i < n; i++) idx[i] = i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int c) {
+    return H[a] * W[a] * D[a] > H[c] * W[c] * D[c];
+  });
+  std::vector<double> load(K, 0.0);
+  b->order.resize(K);
+  for (int i : idx) {
+    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    b->order[k].push_back(i);
+    load[k] += (double)H[i] * W[i] * D[i];
+  }
+  int rc = CBMV_OK;
+  auto fail = [&](int code) {
+    batch_free(b);
+    return code;
+  };
+  for (int k = 0; k < K; k++) {
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(set_error(CBMV_ECUDA, "cudaStreamCreate failed"));
+    b->streams.push_back(s);
+    cbmv_ctx* c = nullptr;
+    if ((rc = cbmv_ctx_create(s, &c))) return fail(rc);
+    b->ctx.push_back(c);
+    size_t need = 0;
+    for (int i : b->order[k]) {
+      size_t bytes = 0;
+      carve(nullptr, H[i], W[i], D[i], &bytes, true);
+      need = std::max(need, bytes);
+    }
+    if ((rc = ensure_workspace(c, need))) return fail(rc);
+  }
+  b->ev_start.resize(n);
+  b->ev_end.resize(n);
+  b->join.resize(K);
+  bool ok = cudaEventCreate(&b->fork) == cudaSuccess && cudaEventCreate(&b->t0) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->in_ev, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->out_ev, cudaEventDisableTiming) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking) == cudaSuccess;
+  for (int i = 0; i < n && ok; i++)
+    ok = cudaEventCreate(&b->ev_start[i]) == cudaSuccess && cudaEventCreate(&b->ev_end[i]) == cudaSuccess;
+  for (int k = 0; k < K && ok; k++) ok = cudaEventCreate(&b->join[k]) == cudaSuccess;
+  if (!ok) return fail(set_error(CBMV_ECUDA, "cudaEventCreate failed"));
+  *out = b;
+  return CBMV_OK;
+}
+
+extern "C" int cbmv_batch_destroy(cbmv_batch* b) {
+  if (!b) return CBMV_OK;
+  if (b->origin) cudaStreamSynchronize(b->origin);
+  for (cudaStream_t s : b->streams) cudaStreamSynchronize(s);
+  batch_free(b);
+  return CBMV_OK;
+}
+
+static int batch_capture(cbmv_batch* b, const cbmv_mlp* m, const cbmv_params* p) {
+  const int K = (int)b->ctx.size();
+  cudaStream_t origin = b->origin;
+  for (int k = 0; k < K; k++) RC(ensure_gaussian(b->ctx[k], p->blur_sigma));  // may allocate: before capture
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  if (b->graph) {
+    cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  CBMV_CUDA(cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal));
+  int rc = CBMV_OK;
+  cudaError_t e = cudaEventRecord(b->fork, origin);
+  if (e == cudaSuccess) e = cudaEventRecordWithFlags(b->t0, origin, cudaEventRecordExternal);
+  for (int k = 0; k < K && e == cudaSuccess; k++) e = cudaStreamWaitEvent(b->streams[k], b->fork, 0);
+  for (int k = 0; k < K && e == cudaSuccess && rc == CBMV_OK; k++) {
+    for (int i : b->order[k]) {
+      e = cudaEventRecordWithFlags(b->ev_start[i], b->streams[k], cudaEventRecordExternal);
+      if (e != cudaSuccess) break;
+      rc = cbmv_run_mlp(b->ctx[k], m, p, b->L[i], b->R[i], b->H[i], b->W[i], b->D[i], b->disp[i], nullptr);
+      if (rc != CBMV_OK) break;
+      e = cudaEventRecordWithFlags(b->ev_end[i], b->streams[k], cudaEventRecordExternal);
+      if (e != cudaSuccess) break;
+    }
+    if (e == cudaSuccess && rc == CBMV_OK) e = cudaEventRecord(b->join[k], b->streams[k]);
+    if (e == cudaSuccess && rc == CBMV_OK) e = cudaStreamWaitEvent(origin, b->join[k], 0);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e_end = cudaStreamEndCapture(origin, &g);  // always end, so the stream is usable again
+  if (rc != CBMV_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess || e_end != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return set_error(CBMV_ECUDA, "batch graph capture: %s",
+                     cudaGetErrorString(e != cudaSuccess ? e : e_end));
+  }
+  b->graph = g;
+  CBMV_CUDA(cudaGraphInstantiate(&b->exec, g, 0));
+  b->net = m;
+  b->params = *p;
+  return CBMV_OK;
+}
+
+extern "C" int cbmv_batch_run_mlp(cbmv_batch* b, const cbmv_mlp* m, const cbmv_params* p, const uint8_t* const* L,
+                                  const uint8_t* const* R, float* const* disp, void* stream) {
+  CBMV_REQUIRE(b && m && L && R && disp, CBMV_EINVAL, "null pointer argument");
+  cbmv_params def;
+  p = params_or_default(p, &def);
+  RC(check_params(p));
+  for (int i = 0; i < b->n; i++) CBMV_REQUIRE(L[i] && R[i] && disp[i], CBMV_EINVAL, "pair %d: null pointer", i);
+  cudaStream_t user = as_stream(stream);
+  bool same = b->exec && b->net == m && memcmp(&b->params, p, sizeof(cbmv_params)) == 0;
+  for (int i = 0; i < b->n && same; i++) same = b->L[i] == L[i] && b->R[i] == R[i] && b->disp[i] == disp[i];
+  if (!same) {
+    b->L.assign(L, L + b->n);
+    b->R.assign(R, R + b->n);
+    b->disp.assign(disp, disp + b->n);
+    RC(batch_capture(b, m, p));
+  }
+  CBMV_CUDA(cudaEventRecord(b->in_ev, user));
+  CBMV_CUDA(cudaStreamWaitEvent(b->origin, b->in_ev, 0));
+  CBMV_CUDA(cudaGraphLaunch(b->exec, b->origin));
+  CBMV_CUDA(cudaEventRecord(b->out_ev, b->origin));
+  CBMV_CUDA(cudaStreamWaitEvent(user, b->out_ev, 0));
+  return CBMV_OK;
+}
+
+extern "C" int cbmv_batch_timings(cbmv_batch* b, float* pair_ms, float* done_ms, float* total_ms) {
+  CBMV_REQUIRE(b && pair_ms && done_ms && total_ms, CBMV_EINVAL, "null pointer argument");
+  CBMV_REQUIRE(b->exec, CBMV_ESTATE, "the batch has not run");
+  float total = 0.0f;
+  for (int i = 0; i < b->n; i++) {
+    CBMV_CUDA(cudaEventSynchronize(b->ev_end[i]));
+    CBMV_CUDA(cudaEventElapsedTime(&pair_ms[i], b->ev_start[i], b->ev_end[i]));
+    CBMV_CUDA(cudaEventElapsedTime(&done_ms[i], b->t0, b->ev_end[i]));
+    total = std::max(total, done_ms[i]);
+  }
+  *total_ms = total;
+  return CBMV_OK;
 }

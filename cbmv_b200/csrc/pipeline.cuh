@@ -41,7 +41,7 @@ int launch_feature_stats(const double* const* vols, int64_t H, int64_t W, int D,
 int launch_feature_stats_f32(const float* const* vols, int64_t H, int64_t W, int D, float2* statsf,
                              cudaStream_t st);
 int launch_features_mlp(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
-                        const cbmv_mlp* m, float* prob0, cudaStream_t st);
+                        const cbmv_mlp* m, float* prob0, cudaStream_t st, int max_ctas = 0);
 // The 20 features (float32) of the samples idx[i] = (y*W + x)*D + d.
 int launch_features_gather(const double* const* vols, const double* stats, int64_t H, int64_t W,
                            int D, const int64_t* idx, int64_t n, float* out, cudaStream_t st);

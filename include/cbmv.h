@@ -296,6 +296,10 @@ typedef struct cbmv_params {
    * (separable form, rounding differs from the reference's); 1 one running
    * float sum per support in the reference's order (post.cu:415-429). */
   int exact_cbca;
+  /* Most CTAs (one per SM) the learned classifier's kernel may occupy;
+   * 0 = every SM.  Lower values leave SMs to pairs running concurrently
+   * (cbmv_batch). */
+  int mlp_ctas;
 } cbmv_params;
 void cbmv_params_default(cbmv_params* p);
 
@@ -321,9 +325,6 @@ int cbmv_run_rf(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params* p, const u
 int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p, const uint8_t* L,
                  const uint8_t* R, int64_t H, int64_t W, int D, float* disp, float* prob0);
 
-/* Training-sample emission (the GPU counterpart of train.py:100-273): the
- * 20 float32 features of the samples idx[i] = (y*W + x)*D + d of the pair
- * (L, R); idx int64 [n], out float32 [n,20], device memory. */
 /* The four float32 matcher volumes of the learned path (census, NCC,
  * SAD-on-Sobel, ZSAD; the reference's test.py:122-138 costs, [H,W,D]
  * layout) into out float32 [4,H,W,D], device memory.  Census, NCC and
@@ -332,8 +333,37 @@ int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p, const uin
 int cbmv_ctx_volumes_f32(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
                          int64_t H, int64_t W, int D, float* out);
 
+/* Training-sample emission (the GPU counterpart of train.py:100-273): the
+ * 20 float32 features of the samples idx[i] = (y*W + x)*D + d of the pair
+ * (L, R); idx int64 [n], out float32 [n,20], device memory. */
 int cbmv_ctx_features_at(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
                          int64_t H, int64_t W, int D, const int64_t* idx, int64_t n, float* out);
+
+/* ------------------------------------------------------------------ */
+/* batches of pairs of uneven size                                     */
+/* ------------------------------------------------------------------ */
+
+/* A batch of n pairs (H[i] x W[i], D[i] disparities) run by the learned
+ * path as ONE CUDA graph launch: the pairs are spread over `streams`
+ * concurrent contexts (longest first onto the least-loaded context), each
+ * with a workspace sized for its largest pair; the graph holds every pair's
+ * kernels, a fork/join over the contexts and per-pair timing events.  No
+ * counterpart in the reference, which runs one pair per process
+ * (main.py:53-70).  Creation allocates the workspaces. */
+typedef struct cbmv_batch cbmv_batch;
+int cbmv_batch_create(int n, const int64_t* H, const int64_t* W, const int* D, int streams,
+                      cbmv_batch** out);
+int cbmv_batch_destroy(cbmv_batch* b);
+/* Runs the batch on `stream`: L[i], R[i] uint8 [H[i],W[i]], disp[i] float32
+ * [H[i],W[i]], device memory.  The first call (and any call whose pointers,
+ * network or parameters differ from the previous one) captures the graph;
+ * the others replay it.  Asynchronous. */
+int cbmv_batch_run_mlp(cbmv_batch* b, const cbmv_mlp* m, const cbmv_params* p, const uint8_t* const* L,
+                       const uint8_t* const* R, float* const* disp, void* stream);
+/* After the last run has completed: pair_ms[i] = time from pair i's first
+ * kernel to its last, done_ms[i] = time from the graph's start to pair i's
+ * end, *total_ms = the graph's span (all ms). */
+int cbmv_batch_timings(cbmv_batch* b, float* pair_ms, float* done_ms, float* total_ms);
 
 /* Stage timings of the last cbmv_run_* call in milliseconds (CUDA events):
  * [0] matchers, [1] feature statistics, [2] features+classifier, [3] post,
