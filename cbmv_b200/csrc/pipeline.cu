@@ -367,6 +367,27 @@ extern "C" int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p
   return CBMV_OK;
 }
 
+extern "C" int cbmv_run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R, int64_t H,
+                             int64_t W, int D, const float* cost, float* disp) {
+  CBMV_REQUIRE(c && L && R && cost && disp, CBMV_EINVAL, "null pointer argument");
+  cbmv_params def;
+  p = params_or_default(p, &def);
+  RC(check_params(p));
+  CBMV_REQUIRE(H > p->censw && W > p->censw, CBMV_EINVAL, "image %lldx%lld smaller than the census window",
+               (long long)W, (long long)H);
+  CBMV_REQUIRE(H <= 65535 && D >= 1 && D <= 1024, CBMV_ERANGE, "H must be <= 65535 and D in 1..1024");
+  size_t bytes = 0;
+  carve(nullptr, H, W, D, &bytes, true);
+  RC(ensure_workspace(c, bytes));
+  Work w = carve(c->ws, H, W, D, &bytes, true);
+  cudaStream_t st = c->stream;
+  for (int i = 0; i < 4; i++) CBMV_CUDA(cudaEventRecord(c->ev[i], st));
+  CBMV_CUDA(cudaMemcpyAsync(w.volA, cost, sizeof(float) * H * W * D, cudaMemcpyDeviceToDevice, st));
+  RC(run_post(c, p, L, R, H, W, D, w, disp));
+  CBMV_CUDA(cudaEventRecord(c->ev[4], st));
+  return CBMV_OK;
+}
+
 extern "C" int cbmv_ctx_volumes_f32(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
                                     int64_t H, int64_t W, int D, float* out) {
   CBMV_REQUIRE(c && L && R && out, CBMV_EINVAL, "null pointer argument");

@@ -55,6 +55,21 @@ class StereoPipeline:
                   prob_out.data_ptr() if prob_out is not None else None)
         return _dev.result(disp, host)
 
+    def run_post(self, left, right, cost, disp_out=None):
+        """The post-processing alone on a matching cost [H,W,D] float32 (numpy
+        or a CUDA tensor; low = good), e.g. a cost volume saved earlier
+        (cbmv_b200.costvol).  Returns the disparity map."""
+        l, host = _dev.to_device(left, np.uint8)
+        r, _ = _dev.to_device(right, np.uint8)
+        c, _ = _dev.to_device(cost, np.float32)
+        H, W = l.shape
+        if c.dim() != 3 or tuple(c.shape[:2]) != (H, W):
+            raise ValueError("cost must be [H,W,D] for images of %dx%d" % (W, H))
+        disp = disp_out if disp_out is not None else _dev.empty((H, W), np.float32)
+        _lib.call("cbmv_run_post", self.ctx, ctypes.byref(self.params), l.data_ptr(), r.data_ptr(), H, W,
+                  int(c.shape[2]), c.contiguous().data_ptr(), disp.data_ptr())
+        return _dev.result(disp, host)
+
     def volumes_f32(self, left, right, ndisp):
         """The learned path's four float32 matcher volumes (census, NCC,
         SAD-on-Sobel, ZSAD) as a device tensor [4,H,W,D]."""

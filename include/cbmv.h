@@ -325,6 +325,14 @@ int cbmv_run_rf(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params* p, const u
 int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p, const uint8_t* L,
                  const uint8_t* R, int64_t H, int64_t W, int D, float* disp, float* prob0);
 
+/* The post-processing alone (Testing.eval_prob with the _mem chain,
+ * test.py:143-149, 341-449) on a given matching cost: cost float32 [H,W,D]
+ * (low = good, e.g. a saved P(class 0) volume, main.py:56-67), the images L,
+ * R uint8 [H,W] for the cross arms and SGM, disp float32 [H,W]; device
+ * memory.  `cost` is not modified. */
+int cbmv_run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R, int64_t H,
+                  int64_t W, int D, const float* cost, float* disp);
+
 /* The four float32 matcher volumes of the learned path (census, NCC,
  * SAD-on-Sobel, ZSAD; the reference's test.py:122-138 costs, [H,W,D]
  * layout) into out float32 [4,H,W,D], device memory.  Census, NCC and

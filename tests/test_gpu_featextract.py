@@ -70,3 +70,24 @@ def test_fused_features_match_reference_assembly(gpu, oracle_cpu, costs):
     np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-30)
     exact = np.mean(np.all(got == ref, axis=1))
     assert exact > 0.9999, exact
+
+
+def test_gpu_training_samples_equal_the_cpu_path(gpu, oracle_cpu):
+    """Training-sample emission on the GPU (cbmv_b200.train_rf.emit_samples)
+    against the reference's Training.__create_samples_mem restated over the
+    oracle with the same draws: features and labels bit-exact (as the
+    float32 sklearn fits on)."""
+    from cbmv_b200 import synth
+    from cbmv_b200.pipeline import StereoPipeline
+    from cbmv_b200.train_rf import emit_samples
+    from oracle import glue
+    L, R, gt, _ = synth.make_pair(seed=21, width=110, height=70, ndisp=24, planes=4, dmin=2, dmax=19)
+    gt = gt.copy()
+    gt[3, 5:9] = np.inf   # invalid ground truth is skipped, as train.py:105-107 does
+    gt[10, 2] = -1.0
+    X, y = emit_samples(StereoPipeline(), L, R, gt, 24, seed=21)
+    S = glue.create_samples_mem(oracle_cpu.mtc, oracle_cpu.fte, L, R, gt, 24,
+                                lambda g, nd: oracle_cpu.fte.generate_d_indices(g, nd, 1, seed=21))
+    assert X.shape == (S.shape[0], 20)
+    assert np.array_equal(X, S[:, :20].astype(np.float32))
+    assert np.array_equal(y, S[:, 20].astype(np.int32))

@@ -79,3 +79,24 @@ def test_pipeline_repeatable_and_device_io(gpu, small_pair, forest):
     b = pipe.run_rf(l, r, 24)
     assert isinstance(b, torch.Tensor) and b.is_cuda
     assert np.array_equal(a, b.cpu().numpy())  # deterministic
+
+
+def test_saved_cost_volume_gives_the_same_disparity(gpu, small_pair, tmp_path):
+    """--saveCostVolume then --loadCostVolume (main.py:56-67): the post run on
+    the reloaded cost reproduces the fused path's disparity bit for bit."""
+    from cbmv_b200 import costvol
+    from cbmv_b200.mlp import GpuMlp
+    from cbmv_b200.pipeline import StereoPipeline
+    import os
+    L, R, _, _ = small_pair
+    H, W = L.shape
+    D = 24
+    net = GpuMlp.load(os.path.join(os.path.dirname(__file__), "golden", "mlp_694x554.npz"))
+    pipe = StereoPipeline()
+    prob = torch.empty((H, W, D), device="cuda")
+    disp = pipe.run_mlp(net, L, R, D, prob_out=prob)
+    for fmt in costvol.FORMATS:
+        path = str(tmp_path / ("cost_%s.npy" % fmt))
+        costvol.save(path, prob, fmt)
+        cost = costvol.load(path, shape=(H, W, D), fmt=fmt)
+        assert np.array_equal(pipe.run_post(L, R, cost), disp), fmt
