@@ -73,16 +73,17 @@ __global__ void grad_kernel(const float* __restrict__ img, int64_t H, int64_t W,
   }
 }
 
-// sgm2 (post.cu:178-261) for all four scan directions in one launch: one
+// sgm2 (post.cu:178-261) for all four scan directions in one launch (one
+// scan routine, the direction a run-time argument: a single copy of the
+// code keeps the instruction cache warm across the four directions): one
 // warp per scan line (the 2H horizontal and 2W vertical lines run
 // concurrently, each direction writing its path costs to its own volume),
 // lane = d (mod 32), KPL disparities per lane.  The scan runs inside the
 // kernel; the step's costs, D1 and the per-d D2 do not depend on the
 // recursion and are loaded PF steps ahead from a register ring.
-template <int DIR, int KPL, int PF>
-__device__ __forceinline__ void sgm_scan(const SgmGrad& g, const float* __restrict__ in, int H, int W,
-                                         int D, const SgmParams& sp, int line,
-                                         float* __restrict__ out) {
+template <int KPL, int PF>
+__device__ __noinline__ void sgm_scan(const SgmGrad& g, const float* __restrict__ in, int H, int W, int D,
+                                      const SgmParams& sp, int line, float* __restrict__ out, const int DIR) {
   const int lane = threadIdx.x & 31;
   const int nsteps = DIR <= 1 ? W : H;
   const int dx = DIR == 0 ? 1 : DIR == 1 ? -1 : 0;
@@ -187,10 +188,21 @@ template <int KPL, int PF>
 __global__ void __launch_bounds__(128) sgm4_kernel(SgmGrad g, const float* __restrict__ in, int H,
                                                    int W, int D, SgmParams sp, SgmOut o) {
   const int warp = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (warp < H) sgm_scan<0, KPL, PF>(g, in, H, W, D, sp, warp, o.dir[0]);
-  else if (warp < 2 * H) sgm_scan<1, KPL, PF>(g, in, H, W, D, sp, warp - H, o.dir[1]);
-  else if (warp < 2 * H + W) sgm_scan<2, KPL, PF>(g, in, H, W, D, sp, warp - 2 * H, o.dir[2]);
-  else if (warp < 2 * H + 2 * W) sgm_scan<3, KPL, PF>(g, in, H, W, D, sp, warp - 2 * H - W, o.dir[3]);
+  int dir = -1, line = 0;
+  if (warp < H) {
+    dir = 0;
+    line = warp;
+  } else if (warp < 2 * H) {
+    dir = 1;
+    line = warp - H;
+  } else if (warp < 2 * H + W) {
+    dir = 2;
+    line = warp - 2 * H;
+  } else if (warp < 2 * H + 2 * W) {
+    dir = 3;
+    line = warp - 2 * H - W;
+  }
+  if (dir >= 0) sgm_scan<KPL, PF>(g, in, H, W, D, sp, line, o.dir[dir], dir);
 }
 
 // out = base + (((L0 + L1) + L2) + L3) * scale over n elements (base may be
@@ -738,7 +750,9 @@ static void sgm4_launch(const SgmGrad& g, const float* in, int H, int W, int D, 
                         const SgmOut& o, cudaStream_t st) {
   const int lines = 2 * H + 2 * W;
   const int blocks = (lines * 32 + 127) / 128;
-  constexpr int PF = KPL <= 2 ? 8 : KPL <= 4 ? 6 : KPL <= 8 ? 3 : 1;
+  // shallow prefetch keeps the scan at ~80 registers (measured faster than
+  // deeper rings, whose registers cost more occupancy than they hide latency)
+  constexpr int PF = KPL <= 2 ? 4 : KPL <= 8 ? 2 : 1;
   sgm4_kernel<KPL, PF><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
 }
 
