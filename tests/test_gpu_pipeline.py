@@ -100,3 +100,33 @@ def test_saved_cost_volume_gives_the_same_disparity(gpu, small_pair, tmp_path):
         costvol.save(path, prob, fmt)
         cost = costvol.load(path, shape=(H, W, D), fmt=fmt)
         assert np.array_equal(pipe.run_post(L, R, cost), disp), fmt
+
+
+@pytest.mark.parametrize("W,H,D", [(97, 53, 37), (150, 64, 70)])
+def test_learned_path_matches_reference_path(gpu, oracle_cpu, W, H, D):
+    """The learned classifier's whole path at sizes off the tile grids (D not
+    a multiple of 32, widths not multiples of 8 or 16) against the
+    reference's test path restated over the oracle (test_model with the
+    network as its classifier, then eval_prob with the _mem post in the
+    reference's summation order): disparities within 0.5 px on >= 99.5 % of
+    pixels (the device runs tanh.approx and float32 features; the network's
+    cost differs from the oracle's float64 model by ~1e-4 on average)."""
+    import os
+    from oracle import glue, mlp_ref
+    from cbmv_b200 import synth
+    from cbmv_b200.mlp import GpuMlp, MlpParams
+    from cbmv_b200.pipeline import StereoPipeline
+    mlp = os.path.join(os.path.dirname(__file__), "golden", "mlp_694x554.npz")
+    L, R, _, _ = synth.make_pair(seed=W + H + D, width=W, height=H, ndisp=D, planes=4, dmin=2, dmax=D - 4)
+    vec = MlpParams.load(mlp).vec
+
+    def predict(X):
+        p0 = 1.0 / (1.0 + np.exp(mlp_ref.forward_fused(vec, X)))
+        return np.stack([p0, 1 - p0], 1)
+
+    proba = glue.test_model(oracle_cpu.mtc, oracle_cpu.fte, predict, L, R, D)
+    disp_ref = glue.eval_prob(oracle_cpu.post, oracle_cpu.fte, proba, L, R, D)
+    disp = StereoPipeline().run_mlp(GpuMlp.load(mlp), L, R, D)
+    close = np.mean(np.abs(disp - disp_ref) <= 0.5)
+    print("learned path %dx%d D=%d: within 0.5 px %.5f" % (W, H, D, close))
+    assert close >= 0.995, close
