@@ -278,16 +278,24 @@ __global__ void __launch_bounds__(128) matcher_strip_kernel(
     yy = yy < 0 ? 0 : (yy >= H ? H - 1 : yy);
     rowoff[wh] = yy * W;
   }
-  int lw[WIN][WIN], rw[WIN][WIN];  // [ring slot][window row]
+  // ring slot contents, computed when the column is loaded: SAD and NCC
+  // keep the column's sum (of |SL - SR|, of L * R), ZSAD keeps 25 (L - R)
+  // per window row
+  int col[WIN];
+  int dif[MODE == kStripZsad ? WIN : 1][WIN];
   auto load_col = [&](int slot, int64_t c) {
     const int64_t cl = c < 0 ? 0 : (c >= W ? W - 1 : c);
     int64_t cr = c - d;
     cr = cr < 0 ? 0 : (cr >= W ? W - 1 : cr);
+    int sum = 0;
 #pragma unroll
     for (int wh = 0; wh < WIN; wh++) {
-      lw[slot][wh] = (int)__ldg(L + rowoff[wh] + cl);
-      rw[slot][wh] = (int)__ldg(R + rowoff[wh] + cr);
+      const int a = (int)__ldg(L + rowoff[wh] + cl), b = (int)__ldg(R + rowoff[wh] + cr);
+      if (MODE == kStripSadSob) sum += abs(a - b);
+      else if (MODE == kStripNcc) sum += a * b;
+      else dif[MODE == kStripZsad ? slot : 0][wh] = (WIN * WIN) * (a - b);
     }
+    col[slot] = sum;
   };
 #pragma unroll
   for (int j = 0; j < WIN - 1; j++) load_col(j, x0 - r + j);
@@ -303,9 +311,7 @@ __global__ void __launch_bounds__(128) matcher_strip_kernel(
       if (MODE == kStripSadSob) {
         int acc = 0;
 #pragma unroll
-        for (int k = 0; k < WIN; k++)
-#pragma unroll
-          for (int wh = 0; wh < WIN; wh++) acc += abs(lw[(s + k) % WIN][wh] - rw[(s + k) % WIN][wh]);
+        for (int k = 0; k < WIN; k++) acc += col[(s + k) % WIN];
         v = (float)acc;
       } else if (MODE == kStripZsad) {
         const int64_t pl = y * W + x;
@@ -314,16 +320,13 @@ __global__ void __launch_bounds__(128) matcher_strip_kernel(
 #pragma unroll
         for (int k = 0; k < WIN; k++)
 #pragma unroll
-          for (int wh = 0; wh < WIN; wh++)
-            acc += abs((WIN * WIN) * (lw[(s + k) % WIN][wh] - rw[(s + k) % WIN][wh]) - m);
+          for (int wh = 0; wh < WIN; wh++) acc += abs(dif[MODE == kStripZsad ? (s + k) % WIN : 0][wh] - m);
         v = (float)((double)acc / (double)(WIN * WIN));
       } else {
         const int64_t pl = y * W + x, pr = pl - d;
         unsigned acc = 0;
 #pragma unroll
-        for (int k = 0; k < WIN; k++)
-#pragma unroll
-          for (int wh = 0; wh < WIN; wh++) acc += (unsigned)(lw[(s + k) % WIN][wh] * rw[(s + k) % WIN][wh]);
+        for (int k = 0; k < WIN; k++) acc += (unsigned)col[(s + k) % WIN];
         const double cl = Cl[pl], cr = Cr[pr];
         if (isfinite(cl) && isfinite(cr)) {
           const unsigned long long aa = (unsigned long long)Al[pl] * (unsigned long long)Ar[pr];
