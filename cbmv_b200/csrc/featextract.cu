@@ -273,15 +273,35 @@ __global__ void stats_f32_left_kernel(VolsF vols, int64_t HW, int D, float2* __r
   const float inv_sigma = kInvSigmaF32[m];
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const bool vec = (D & 3) == 0 && D <= 512;  // the row as <= 4 float4 per lane, kept in registers
   for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < HW; p += nw) {
     const float* r = vol + p * D;
-    float mn = kRandMaxF;
-    for (int d = lane; d < D; d += 32) mn = fminf(mn, __ldg(r + d));
-    for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-    float den = 0.0f;
-    for (int d = lane; d < D; d += 32) {
-      const float t = __ldg(r + d) - mn;
-      den += __expf(-(t * t) * inv_sigma);
+    float mn = kRandMaxF, den = 0.0f;
+    if (vec) {
+      float4 v[4];
+      const int nq = D >> 2;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int q = lane + 32 * k;
+        v[k] = q < nq ? __ldg(reinterpret_cast<const float4*>(r) + q) : make_float4(kRandMaxF, kRandMaxF, kRandMaxF, kRandMaxF);
+        mn = fminf(mn, fminf(fminf(v[k].x, v[k].y), fminf(v[k].z, v[k].w)));
+      }
+      for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        if (lane + 32 * k < nq) {
+          const float tx = v[k].x - mn, ty = v[k].y - mn, tz = v[k].z - mn, tw = v[k].w - mn;
+          den += (__expf(-(tx * tx) * inv_sigma) + __expf(-(ty * ty) * inv_sigma)) +
+                 (__expf(-(tz * tz) * inv_sigma) + __expf(-(tw * tw) * inv_sigma));
+        }
+      }
+    } else {
+      for (int d = lane; d < D; d += 32) mn = fminf(mn, __ldg(r + d));
+      for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+      for (int d = lane; d < D; d += 32) {
+        const float t = __ldg(r + d) - mn;
+        den += __expf(-(t * t) * inv_sigma);
+      }
     }
     for (int o = 16; o; o >>= 1) den += __shfl_xor_sync(0xffffffffu, den, o);
     if (lane == 0) statsf[(int64_t)(m * 2) * HW + p] = stats_pair(mn, den);

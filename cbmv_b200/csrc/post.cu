@@ -692,11 +692,14 @@ __global__ void f32_to_f64_kernel(const float* __restrict__ in, int64_t n, doubl
 }
 
 // Sums of an image and of its squares in float64 (one block).
-__global__ void moments_kernel(const uint8_t* __restrict__ img, int64_t n, double* __restrict__ mom) {
-  __shared__ double s1[32], s2[32];
-  double a = 0.0, b = 0.0;
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
-    const double v = img[i];
+// Sum and sum of squares of the image as exact 64-bit integers (so the
+// result does not depend on the order of the additions), accumulated by
+// every block into mom[0..1] with integer atomics; mom is zeroed first.
+__global__ void moments_kernel(const uint8_t* __restrict__ img, int64_t n,
+                               unsigned long long* __restrict__ mom) {
+  unsigned long long a = 0, b = 0;
+  GRID_STRIDE(i, n) {
+    const unsigned v = img[i];
     a += v;
     b += v * v;
   }
@@ -705,27 +708,17 @@ __global__ void moments_kernel(const uint8_t* __restrict__ img, int64_t n, doubl
     b += __shfl_xor_sync(0xffffffffu, b, o);
   }
   if ((threadIdx.x & 31) == 0) {
-    s1[threadIdx.x >> 5] = a;
-    s2[threadIdx.x >> 5] = b;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double A = 0.0, B = 0.0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
-      A += s1[k];
-      B += s2[k];
-    }
-    mom[0] = A;
-    mom[1] = B;
+    atomicAdd(mom, a);
+    atomicAdd(mom + 1, b);
   }
 }
 
 // (I - mean) / std in float32 with float32 mean and population std, as
 // test.py:489-492 does with numpy on the float32 image.
 __global__ void normalise_kernel(const uint8_t* __restrict__ img, int64_t n,
-                                 const double* __restrict__ mom, float* __restrict__ out) {
-  const double mean = mom[0] / (double)n;
-  const double var = fmax(mom[1] / (double)n - mean * mean, 0.0);
+                                 const unsigned long long* __restrict__ mom, float* __restrict__ out) {
+  const double mean = (double)mom[0] / (double)n;
+  const double var = fmax((double)mom[1] / (double)n - mean * mean, 0.0);
   const float m = (float)mean, s = (float)sqrt(var);
   GRID_STRIDE(i, n) out[i] = ((float)img[i] - m) / s;
 }
@@ -829,8 +822,10 @@ int launch_mean2d(const float* in, int64_t H, int64_t W, const float* kernel, in
 }
 
 int launch_normalise(const uint8_t* img, int64_t n, double* mom, float* out, cudaStream_t st) {
-  moments_kernel<<<1, 1024, 0, st>>>(img, n, mom);
-  normalise_kernel<<<grid_for(n, 256), 256, 0, st>>>(img, n, mom, out);
+  unsigned long long* m = reinterpret_cast<unsigned long long*>(mom);
+  CBMV_CUDA(cudaMemsetAsync(m, 0, 2 * sizeof(unsigned long long), st));
+  moments_kernel<<<grid_for(n, 256), 256, 0, st>>>(img, n, m);
+  normalise_kernel<<<grid_for(n, 256), 256, 0, st>>>(img, n, m, out);
   return check_launch("normalise");
 }
 
