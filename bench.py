@@ -442,7 +442,8 @@ def run_batch(a, ws, rank, local):
     tune = tune_batch(shapes, net, lefts, rights, log=lambda m: print(m, file=sys.stderr))
     t_tune = time.perf_counter() - t_tune
     b = StereoBatch(shapes, streams=tune["streams"])
-    prm = _lib.default_params(mlp_ctas=tune["mlp_ctas"])
+    prm = _lib.default_params(mlp_ctas=tune["mlp_ctas"], cbca_rows=tune.get("cbca_rows", 32),
+                              sgm_prefetch=tune.get("sgm_prefetch", 0))
     st = torch.cuda.current_stream()
     for _ in range(a.warmup):
         b.run_mlp(net, lefts, rights, prm)
@@ -484,7 +485,9 @@ def run_batch(a, ws, rank, local):
         "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "bf16/f32", "data": "synthetic (seeded uneven pairs, seeds 4000+)",
         "config": {"workload": "%d pairs W~U[320,1500] H~U[240,1000] D in {64,128,192,256}" % len(shapes),
-                   "units": units, "autotune": {k: tune[k] for k in ("streams", "mlp_ctas", "ms", "tried")},
+                   "units": units,
+                   "autotune": {k: tune.get(k) for k in ("streams", "mlp_ctas", "cbca_rows", "sgm_prefetch", "ms",
+                                                         "tried")},
                    "autotune_seconds": t_tune, "parallelism": "pairs over concurrent contexts in one graph"},
         "latency_ms": {"pair_p50": float(np.percentile(pair_ms, 50)), "pair_p99": float(np.percentile(pair_ms, 99)),
                        "done_p50": float(np.percentile(done_ms, 50)), "done_p99": float(np.percentile(done_ms, 99)),

@@ -32,7 +32,7 @@ class cbmv_params(ctypes.Structure):
                 ("alpha1", _flt), ("tau_so", _flt), ("sgm_i", _int), ("L1", _int),
                 ("tau1", _flt), ("cbca_i1", _int), ("cbca_i2", _int), ("median_i", _int),
                 ("median_w", _int), ("blur_sigma", _flt), ("blur_t", _flt), ("direction", _int),
-                ("exact_cbca", _int), ("mlp_ctas", _int)]
+                ("exact_cbca", _int), ("mlp_ctas", _int), ("cbca_rows", _int), ("sgm_prefetch", _int)]
 
 
 # name -> argtypes (all return int status unless listed in _RESTYPE)

@@ -90,13 +90,16 @@ def default_cache_path():
 
 
 def tune_batch(shapes, net, lefts, rights, streams=CANDIDATE_STREAMS, mlp_ctas=(0, None), iters=2,
-               cache_path=None, log=None):
+               cache_path=None, log=None, tile_search=True):
     """Pick the batch's launch shape by timing it: the number of concurrent
     contexts and the classifier kernel's CTA cap (0 = every SM, None = the
-    SM count divided by the number of contexts).  Each candidate is
-    captured, run once untimed and `iters` times timed (graph span, CUDA
-    events); the fastest is cached per (GPU, batch shapes) in a JSON file.
-    Returns {"streams", "mlp_ctas", "ms", "tried": [...]}."""
+    SM count divided by the number of contexts), then (tile_search) the
+    kernel tile shapes, one at a time from the best: rows per CBCA tile
+    (32, 16) and SGM prefetch depth (default, 1, 4).  None of these change
+    the results.  Each candidate is captured, run once untimed and `iters`
+    times timed (graph span, CUDA events); the fastest is cached per (GPU,
+    batch shapes) in a JSON file.  Returns {"streams", "mlp_ctas",
+    "cbca_rows", "sgm_prefetch", "ms", "tried": [...]}."""
     import torch
     shapes = [tuple(int(v) for v in s) for s in shapes]
     cache_path = cache_path or default_cache_path()
@@ -111,6 +114,23 @@ def tune_batch(shapes, net, lefts, rights, streams=CANDIDATE_STREAMS, mlp_ctas=(
         return dict(cache[sig], cached=True)
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     tried = []
+
+    def measure(b, cand):
+        prm = _lib.default_params(mlp_ctas=cand["mlp_ctas"], cbca_rows=cand["cbca_rows"],
+                                  sgm_prefetch=cand["sgm_prefetch"])
+        b.run_mlp(net, lefts, rights, prm)
+        torch.cuda.synchronize()
+        spans = []
+        for _ in range(iters):
+            b.run_mlp(net, lefts, rights, prm)
+            torch.cuda.synchronize()
+            spans.append(b.timings()["total_ms"])
+        cand = dict(cand, ms=float(np.median(spans)))
+        tried.append(cand)
+        if log:
+            log("autotune: " + ", ".join("%s %s" % (k, v) for k, v in cand.items()))
+        return cand
+
     for k in streams:
         if k > len(shapes):
             continue
@@ -119,22 +139,22 @@ def tune_batch(shapes, net, lefts, rights, streams=CANDIDATE_STREAMS, mlp_ctas=(
             c = 0 if cap == 0 else (max(1, sms // k) if cap is None else int(cap))
             if c and c >= sms:
                 continue
-            prm = _lib.default_params(mlp_ctas=c)
-            b.run_mlp(net, lefts, rights, prm)
-            torch.cuda.synchronize()
-            spans = []
-            for _ in range(iters):
-                b.run_mlp(net, lefts, rights, prm)
-                torch.cuda.synchronize()
-                spans.append(b.timings()["total_ms"])
-            ms = float(np.median(spans))
-            tried.append({"streams": k, "mlp_ctas": c, "ms": ms})
-            if log:
-                log("autotune: streams %d, mlp_ctas %d: %.2f ms" % (k, c, ms))
+            measure(b, {"streams": k, "mlp_ctas": c, "cbca_rows": 32, "sgm_prefetch": 0})
         b.close()
         torch.cuda.synchronize()
     best = min(tried, key=lambda t: t["ms"])
-    res = {"streams": best["streams"], "mlp_ctas": best["mlp_ctas"], "ms": best["ms"], "tried": tried,
+    if tile_search:
+        b = StereoBatch(shapes, streams=best["streams"])
+        for key, values in (("cbca_rows", (16,)), ("sgm_prefetch", (1, 4))):
+            for v in values:
+                cand = measure(b, dict({k: best[k] for k in ("streams", "mlp_ctas", "cbca_rows", "sgm_prefetch")},
+                                       **{key: v}))
+                if cand["ms"] < best["ms"]:
+                    best = cand
+        b.close()
+        torch.cuda.synchronize()
+    res = {"streams": best["streams"], "mlp_ctas": best["mlp_ctas"], "cbca_rows": best["cbca_rows"],
+           "sgm_prefetch": best["sgm_prefetch"], "ms": best["ms"], "tried": tried,
            "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
     cache[sig] = res
     try:

@@ -52,6 +52,8 @@ extern "C" void cbmv_params_default(cbmv_params* p) {
   p->direction = -1;  // test.py:501
   p->exact_cbca = 0;
   p->mlp_ctas = 0;
+  p->cbca_rows = 0;
+  p->sgm_prefetch = 0;
 }
 
 struct cbmv_ctx {
@@ -152,6 +154,11 @@ int check_params(const cbmv_params* p) {
                "median window must be odd <= 11");
   CBMV_REQUIRE(p->blur_sigma > 0 && p->blur_sigma <= 5.0f, CBMV_EINVAL, "blur_sigma not in (0, 5]");
   CBMV_REQUIRE(p->direction == 1 || p->direction == -1, CBMV_EINVAL, "direction must be +-1");
+  CBMV_REQUIRE(p->cbca_rows == 0 || p->cbca_rows == 16 || p->cbca_rows == 32, CBMV_EINVAL,
+               "cbca_rows must be 0, 16 or 32");
+  CBMV_REQUIRE(p->sgm_prefetch == 0 || p->sgm_prefetch == 1 || p->sgm_prefetch == 2 || p->sgm_prefetch == 4,
+               CBMV_EINVAL, "sgm_prefetch must be 0, 1, 2 or 4");
+  CBMV_REQUIRE(p->mlp_ctas >= 0, CBMV_EINVAL, "mlp_ctas must be >= 0");
   return CBMV_OK;
 }
 
@@ -239,7 +246,8 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
   float* oth = w.volB;
   auto cbca = [&](const float* in, float* out) {
     return p->exact_cbca ? launch_cbca(w.crossL, w.crossR, in, H, W, D, CBMV_HWD, p->direction, out, st, p->L1 - 1)
-                         : launch_cbca_sep(w.crossL, w.crossR, in, H, W, D, p->direction, out, st, p->L1 - 1);
+                         : launch_cbca_sep(w.crossL, w.crossR, in, H, W, D, p->direction, out, st, p->L1 - 1,
+                                           p->cbca_rows == 16 ? 16 : 32);
   };
   for (int i = 0; i < p->cbca_i1; i++) {
     RC(cbca(cur, oth));
@@ -254,7 +262,7 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
   if (p->sgm_i > 0) RC(launch_sgm_grad(w.imL, w.imR, H, W, &g, st));
   for (int i = 0; i < p->sgm_i; i++) {
     // out = ((L0 + L1 + L2) + L3) / 4   (test.py:379-383)
-    RC(launch_sgm4(g, cur, H, W, D, sp, so, st));
+    RC(launch_sgm4(g, cur, H, W, D, sp, so, st, p->sgm_prefetch));
     RC(launch_sgm_combine(so, V, nullptr, 0.25f, oth, st));
     float* t = cur; cur = oth; oth = t;
   }

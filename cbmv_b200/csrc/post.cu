@@ -357,14 +357,14 @@ __global__ void __launch_bounds__(256) cbca_hwd_tiled_kernel(
 // HALO = L1 - 1 pixels every support element is within the taps.  The
 // result differs from the reference's single running float sum
 // (post.cu:415-429) by rounding only.
-constexpr int CS_TX = 8, CS_TY = 32, CS_TD = 32;
+constexpr int CS_TX = 8, CS_TD = 32;
 
-template <int HALO>
+template <int HALO, int CS_TY>
 constexpr size_t cbca_sep_smem_bytes() {
   return (size_t)(CS_TY + 2 * HALO) * CS_TX * CS_TD * (sizeof(float) + sizeof(uint8_t));
 }
 
-template <int HALO>
+template <int HALO, int CS_TY>
 __global__ void __launch_bounds__(256, 4) cbca_hwd_sep_kernel(
     const float* __restrict__ lc, const float* __restrict__ rc, const float* __restrict__ in, int H, int W,
     int D, int direction, float* __restrict__ out) {
@@ -454,16 +454,23 @@ __global__ void __launch_bounds__(256, 4) cbca_hwd_sep_kernel(
   }
 }
 
+template <int HALO, int TY>
+int launch_cbca_sep_ht(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
+                       int direction, float* out, cudaStream_t st) {
+  constexpr size_t smem = cbca_sep_smem_bytes<HALO, TY>();
+  CBMV_CUDA(cudaFuncSetAttribute(cbca_hwd_sep_kernel<HALO, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  const int64_t tiles = (int64_t)((W + CS_TX - 1) / CS_TX) * ((H + TY - 1) / TY) * ((D + CS_TD - 1) / CS_TD);
+  cbca_hwd_sep_kernel<HALO, TY><<<(unsigned)tiles, 256, smem, st>>>(lc, rc, in, (int)H, (int)W, D, direction, out);
+  return check_launch("cbca_sep");
+}
+
+// tile rows 16 or 32 (the results do not depend on them)
 template <int HALO>
 int launch_cbca_sep_h(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
-                      int direction, float* out, cudaStream_t st) {
-  constexpr size_t smem = cbca_sep_smem_bytes<HALO>();
-  CBMV_CUDA(cudaFuncSetAttribute(cbca_hwd_sep_kernel<HALO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
-  const int64_t tiles = (int64_t)((W + CS_TX - 1) / CS_TX) * ((H + CS_TY - 1) / CS_TY) *
-                        ((D + CS_TD - 1) / CS_TD);
-  cbca_hwd_sep_kernel<HALO><<<(unsigned)tiles, 256, smem, st>>>(lc, rc, in, (int)H, (int)W, D, direction, out);
-  return check_launch("cbca_sep");
+                      int direction, float* out, cudaStream_t st, int rows) {
+  if (rows == 16) return launch_cbca_sep_ht<HALO, 16>(lc, rc, in, H, W, D, direction, out, st);
+  return launch_cbca_sep_ht<HALO, 32>(lc, rc, in, H, W, D, direction, out, st);
 }
 
 // Winner-take-all (first minimum, as np.argmin) and the subpixel parabola
@@ -738,27 +745,32 @@ int launch_sgm_grad(const float* imL, const float* imR, int64_t H, int64_t W, Sg
   return check_launch("sgm_grad");
 }
 
+// prefetch: steps loaded ahead (1, 2 or 4; 0 = the default: shallow
+// prefetch keeps the scan at ~80 registers, measured faster than deeper
+// rings, whose registers cost more occupancy than they hide latency).
+// The results do not depend on it.
 template <int KPL>
 static void sgm4_launch(const SgmGrad& g, const float* in, int H, int W, int D, const SgmParams& sp,
-                        const SgmOut& o, cudaStream_t st) {
+                        const SgmOut& o, cudaStream_t st, int prefetch) {
   const int lines = 2 * H + 2 * W;
   const int blocks = (lines * 32 + 127) / 128;
-  // shallow prefetch keeps the scan at ~80 registers (measured faster than
-  // deeper rings, whose registers cost more occupancy than they hide latency)
-  constexpr int PF = KPL <= 2 ? 4 : KPL <= 8 ? 2 : 1;
-  sgm4_kernel<KPL, PF><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+  constexpr int PF0 = KPL <= 2 ? 4 : KPL <= 8 ? 2 : 1;
+  const int pf = prefetch > 0 && KPL <= 8 ? prefetch : PF0;
+  if (pf >= 4) sgm4_kernel<KPL, KPL <= 8 ? 4 : 1><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+  else if (pf >= 2) sgm4_kernel<KPL, KPL <= 8 ? 2 : 1><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+  else sgm4_kernel<KPL, 1><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
 }
 
 int launch_sgm4(const SgmGrad& g, const float* in, int64_t H, int64_t W, int D, const SgmParams& sp,
-                const SgmOut& o, cudaStream_t st) {
+                const SgmOut& o, cudaStream_t st, int prefetch) {
   const int kpl = (D + 31) / 32;
   const int h = (int)H, w = (int)W;
-  if (kpl <= 1) sgm4_launch<1>(g, in, h, w, D, sp, o, st);
-  else if (kpl <= 2) sgm4_launch<2>(g, in, h, w, D, sp, o, st);
-  else if (kpl <= 4) sgm4_launch<4>(g, in, h, w, D, sp, o, st);
-  else if (kpl <= 8) sgm4_launch<8>(g, in, h, w, D, sp, o, st);
-  else if (kpl <= 16) sgm4_launch<16>(g, in, h, w, D, sp, o, st);
-  else sgm4_launch<32>(g, in, h, w, D, sp, o, st);
+  if (kpl <= 1) sgm4_launch<1>(g, in, h, w, D, sp, o, st, prefetch);
+  else if (kpl <= 2) sgm4_launch<2>(g, in, h, w, D, sp, o, st, prefetch);
+  else if (kpl <= 4) sgm4_launch<4>(g, in, h, w, D, sp, o, st, prefetch);
+  else if (kpl <= 8) sgm4_launch<8>(g, in, h, w, D, sp, o, st, prefetch);
+  else if (kpl <= 16) sgm4_launch<16>(g, in, h, w, D, sp, o, st, prefetch);
+  else sgm4_launch<32>(g, in, h, w, D, sp, o, st, prefetch);
   return check_launch("sgm4");
 }
 
@@ -787,19 +799,19 @@ int launch_cbca(const float* lc, const float* rc, const float* in, int64_t H, in
 }
 
 int launch_cbca_sep(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
-                    int direction, float* out, cudaStream_t st, int halo) {
-  CBMV_REQUIRE(H < (1 << 30) / CS_TY && W < (1 << 30) && (int64_t)((W + CS_TX - 1) / CS_TX) *
-                   ((H + CS_TY - 1) / CS_TY) * ((D + CS_TD - 1) / CS_TD) < ((int64_t)1 << 31),
+                    int direction, float* out, cudaStream_t st, int halo, int rows) {
+  CBMV_REQUIRE(H < (1 << 30) && W < (1 << 30) && (int64_t)((W + CS_TX - 1) / CS_TX) * ((H + 15) / 16) *
+                   ((D + CS_TD - 1) / CS_TD) < ((int64_t)1 << 31),
                CBMV_ERANGE, "cbca: volume too large");
   switch (halo) {
-    case 1: return launch_cbca_sep_h<1>(lc, rc, in, H, W, D, direction, out, st);
-    case 2: return launch_cbca_sep_h<2>(lc, rc, in, H, W, D, direction, out, st);
-    case 3: return launch_cbca_sep_h<3>(lc, rc, in, H, W, D, direction, out, st);
-    case 4: return launch_cbca_sep_h<4>(lc, rc, in, H, W, D, direction, out, st);
-    case 5: return launch_cbca_sep_h<5>(lc, rc, in, H, W, D, direction, out, st);
-    case 6: return launch_cbca_sep_h<6>(lc, rc, in, H, W, D, direction, out, st);
-    case 7: return launch_cbca_sep_h<7>(lc, rc, in, H, W, D, direction, out, st);
-    case 8: return launch_cbca_sep_h<8>(lc, rc, in, H, W, D, direction, out, st);
+    case 1: return launch_cbca_sep_h<1>(lc, rc, in, H, W, D, direction, out, st, rows);
+    case 2: return launch_cbca_sep_h<2>(lc, rc, in, H, W, D, direction, out, st, rows);
+    case 3: return launch_cbca_sep_h<3>(lc, rc, in, H, W, D, direction, out, st, rows);
+    case 4: return launch_cbca_sep_h<4>(lc, rc, in, H, W, D, direction, out, st, rows);
+    case 5: return launch_cbca_sep_h<5>(lc, rc, in, H, W, D, direction, out, st, rows);
+    case 6: return launch_cbca_sep_h<6>(lc, rc, in, H, W, D, direction, out, st, rows);
+    case 7: return launch_cbca_sep_h<7>(lc, rc, in, H, W, D, direction, out, st, rows);
+    case 8: return launch_cbca_sep_h<8>(lc, rc, in, H, W, D, direction, out, st, rows);
     default: return launch_cbca(lc, rc, in, H, W, D, CBMV_HWD, direction, out, st, halo);
   }
 }

@@ -24,7 +24,7 @@ struct SgmOut {
   float* dir[4];
 };
 int launch_sgm4(const SgmGrad& g, const float* in, int64_t H, int64_t W, int D, const SgmParams& sp,
-                const SgmOut& o, cudaStream_t st);
+                const SgmOut& o, cudaStream_t st, int prefetch = 0);
 // out = base + (((L0 + L1) + L2) + L3) * scale; base may be null or out.
 int launch_sgm_combine(const SgmOut& o, int64_t n, const float* base, float scale, float* out,
                        cudaStream_t st);
@@ -35,7 +35,7 @@ int launch_cbca(const float* lc, const float* rc, const float* in, int64_t H, in
 // cbca on [H,W,D] in separable form (row sums, then column sums); arms of
 // at most `halo` pixels (L1 - 1), halo 1..8 (larger: the reference-order kernel)
 int launch_cbca_sep(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
-                    int direction, float* out, cudaStream_t st, int halo);
+                    int direction, float* out, cudaStream_t st, int halo, int rows = 32);
 int launch_wta_subpixel(const float* cost, int64_t H, int64_t W, int D, float* disp_int,
                         float* disp, cudaStream_t st);
 int launch_median(const float* in, int64_t H, int64_t W, int k, float* out, cudaStream_t st);

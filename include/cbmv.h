@@ -300,6 +300,10 @@ typedef struct cbmv_params {
    * 0 = every SM.  Lower values leave SMs to pairs running concurrently
    * (cbmv_batch). */
   int mlp_ctas;
+  /* Launch shapes that do not change the results (picked by the batch
+   * autotuner): rows per CBCA tile, 16 or 32 (0 = 32); SGM steps loaded
+   * ahead, 1, 2 or 4 (0 = the default for the disparity count). */
+  int cbca_rows, sgm_prefetch;
 } cbmv_params;
 void cbmv_params_default(cbmv_params* p);
 

@@ -22,6 +22,20 @@ def _pairs(seed0=50):
     return out
 
 
+def test_tile_shapes_do_not_change_results(gpu):
+    """The autotuner's tile shapes (CBCA tile rows, SGM prefetch depth)
+    leave the disparities bit-identical."""
+    from cbmv_b200 import _lib
+    from cbmv_b200.mlp import GpuMlp
+    from cbmv_b200.pipeline import StereoPipeline
+    net = GpuMlp.load(MLP)
+    (l, r), (_, _, d) = _pairs()[3], SHAPES[3]
+    ref = StereoPipeline().run_mlp(net, l, r, d).cpu().numpy()
+    for rows, pf in ((16, 0), (32, 1), (16, 4), (32, 2)):
+        got = StereoPipeline(params=_lib.default_params(cbca_rows=rows, sgm_prefetch=pf)).run_mlp(net, l, r, d)
+        assert np.array_equal(got.cpu().numpy(), ref), (rows, pf)
+
+
 def test_batch_graph_matches_single_pairs(gpu):
     from cbmv_b200.batch import StereoBatch
     from cbmv_b200.mlp import GpuMlp
@@ -56,8 +70,10 @@ def test_autotuner_picks_and_caches(gpu, tmp_path):
     cache = str(tmp_path / "autotune.json")
     res = tune_batch(SHAPES, net, [p[0] for p in pairs], [p[1] for p in pairs], streams=(1, 2), mlp_ctas=(0, None),
                      iters=1, cache_path=cache)
-    # one context: "SMs / contexts" is every SM, the same candidate as 0, tried once
-    assert not res["cached"] and res["streams"] in (1, 2) and len(res["tried"]) == 3
+    # one context: "SMs / contexts" is every SM, the same candidate as 0, tried once;
+    # then the tile search: CBCA rows 16, SGM prefetch 1 and 4
+    assert not res["cached"] and res["streams"] in (1, 2) and len(res["tried"]) == 6
+    assert res["cbca_rows"] in (16, 32) and res["sgm_prefetch"] in (0, 1, 4)
     assert res["ms"] == min(t["ms"] for t in res["tried"])
     again = tune_batch(SHAPES, net, [p[0] for p in pairs], [p[1] for p in pairs], cache_path=cache)
     assert again["cached"] and again["streams"] == res["streams"]
