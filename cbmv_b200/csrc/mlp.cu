@@ -710,7 +710,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   unsigned char* sW3 = sW2 + kSmW2i;
   unsigned char* sW4 = sW3 + kSmW3i;
   unsigned char* sTiles = sW4 + kSmW4i;
-  __shared__ __align__(16) float s_norm[kNormN];
+  __shared__ float4 s_nrm[kF];  // per feature column: cap, mu, inv_sd
   __shared__ __align__(16) float s_b2[kH2];
   __shared__ __align__(16) float s_b3[kH3];
   __shared__ float s_b4;
@@ -722,7 +722,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   if (tid < 32) umma::tmem_alloc(&tmem_base, 128 * kGroups);
   if (tid < kGroups) umma::mbar_init(&bars[tid], 1);
   stage_inference_weights(P, sW1, sW2, sW3, sW4);
-  for (int i = tid; i < kNormN; i += kInfThreads) s_norm[i] = P[i];
+  for (int i = tid; i < kF; i += kInfThreads) s_nrm[i] = make_float4(P[i], P[kF + i], P[2 * kF + i], 0.0f);
   for (int i = tid; i < kH2; i += kInfThreads) s_b2[i] = P[kOffB2 + i];
   for (int i = tid; i < kH3; i += kInfThreads) s_b3[i] = P[kOffB3 + i];
   if (tid == 0) s_b4 = P[kOffB4];
@@ -757,6 +757,9 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   uint32_t phase = 0;
   bool ok = true;
 
+  // this thread's two matchers' ratio epsilon and likelihood 1/sigma
+  const float eps0 = kEpsF[2 * half], eps1 = kEpsF[2 * half + 1];
+  const float isg0 = kInvSigmaF[2 * half], isg1 = kInvSigmaF[2 * half + 1];
   for (; tile < tiles; tile += tstride) {
     // 1. features of sample t, matchers 2*half and 2*half+1 -> row of X0 (the first atom of the tile)
     {
@@ -772,16 +775,18 @@ __global__ void __launch_bounds__(kInfThreads, 1)
         const float c = __ldg(vol + tv);
         const float2 sl = statsf[(int64_t)(m * 2) * HW + pv];
         const float2 sr = has_right ? statsf[(int64_t)(m * 2 + 1) * HW + pv - dv] : make_float2(kRandMaxF, 0.0f);
-        const float inv_ce = __fdividef(1.0f, c + kEpsF[m]);
+        const float eps = i ? eps1 : eps0, isg = i ? isg1 : isg0;
+        const float inv_ce = __fdividef(1.0f, c + eps);
         f[i] = c;
-        conf_f32(c, inv_ce, sl, kEpsF[m], kInvSigmaF[m], &f[2 + i], &f[4 + i]);
-        conf_f32(c, inv_ce, sr, kEpsF[m], kInvSigmaF[m], &f[6 + i], &f[8 + i]);
+        conf_f32(c, inv_ce, sl, eps, isg, &f[2 + i], &f[4 + i]);
+        conf_f32(c, inv_ce, sr, eps, isg, &f[6 + i], &f[8 + i]);
       }
 #pragma unroll
       for (int q = 0; q < 5; q++) {
         const int k = 4 * q + 2 * half;  // reference column of f[2q]
-        const float a = (fminf(f[2 * q], s_norm[k]) - s_norm[kF + k]) * s_norm[2 * kF + k];
-        const float b = (fminf(f[2 * q + 1], s_norm[k + 1]) - s_norm[kF + k + 1]) * s_norm[2 * kF + k + 1];
+        const float4 na = s_nrm[k], nb = s_nrm[k + 1];
+        const float a = (fminf(f[2 * q], na.x) - na.y) * na.z;
+        const float b = (fminf(f[2 * q + 1], nb.x) - nb.y) * nb.z;
         *reinterpret_cast<uint32_t*>(sA + umma::sw128_offset(128, row, k)) = pack_bf16x2(a, b);
       }
       if (half) {  // columns 20, 21: the bias inputs; 22..31: zero
