@@ -55,6 +55,22 @@ class StereoPipeline:
                   prob_out.data_ptr() if prob_out is not None else None)
         return _dev.result(disp, host)
 
+    def run_classified(self, left, right, ndisp, net=None, disp_out=None, prob_out=None):
+        """The learned classifier with the random forest as its fallback:
+        runs `net` (cbmv_b200.mlp.GpuMlp) when given; if that call fails or
+        the network reports a tensor-core wait timeout, the pair is run again
+        with the pipeline's forest.  Returns (disparity, "mlp" or "rf")."""
+        if net is not None:
+            try:
+                disp = self.run_mlp(net, left, right, ndisp, disp_out=disp_out, prob_out=prob_out)
+                if net.status() == 0:
+                    return disp, "mlp"
+            except _lib.CbmvError:
+                pass
+        if self.forest is None:
+            raise RuntimeError("the learned classifier failed and the pipeline has no forest to fall back on")
+        return self.run_rf(left, right, ndisp, disp_out=disp_out, prob_out=prob_out), "rf"
+
     def run_post(self, left, right, cost, disp_out=None):
         """The post-processing alone on a matching cost [H,W,D] float32 (numpy
         or a CUDA tensor; low = good), e.g. a cost volume saved earlier

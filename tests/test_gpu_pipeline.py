@@ -130,3 +130,18 @@ def test_learned_path_matches_reference_path(gpu, oracle_cpu, W, H, D):
     close = np.mean(np.abs(disp - disp_ref) <= 0.5)
     print("learned path %dx%d D=%d: within 0.5 px %.5f" % (W, H, D, close))
     assert close >= 0.995, close
+
+
+def test_run_classified_uses_the_network(gpu, small_pair, forest):
+    """On a clean run the learned classifier answers, not its fallback."""
+    import os
+    from cbmv_b200.forest_gpu import GpuForest
+    from cbmv_b200.mlp import GpuMlp
+    from cbmv_b200.pipeline import StereoPipeline
+    L, R, _, _ = small_pair
+    net = GpuMlp.load(os.path.join(os.path.dirname(__file__), "golden", "mlp_694x554.npz"))
+    pipe = StereoPipeline(GpuForest(forest))
+    disp, which = pipe.run_classified(L, R, 24, net=net)
+    assert which == "mlp" and np.array_equal(disp, pipe.run_mlp(net, L, R, 24))
+    disp_rf, which_rf = pipe.run_classified(L, R, 24)
+    assert which_rf == "rf" and np.array_equal(disp_rf, pipe.run_rf(L, R, 24))

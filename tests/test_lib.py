@@ -45,6 +45,31 @@ def test_host_side_argument_checks():
     assert abs(p.pi1 - 1.3) < 1e-6 and abs(p.blur_t - 1.3) < 1e-6
 
 
+def test_argument_checks_of_the_fused_entry_points():
+    """The batch, post-only, separable CBCA and parameter checks reject bad
+    arguments on the host, before any device work."""
+    import numpy as np
+    from cbmv_b200 import _lib
+    L = _lib.lib()
+    buf = ctypes.c_void_p(16)
+    h = ctypes.c_void_p()
+    Hs, Ws, Ds = (np.array(v, dt) for v, dt in (([64, 8], np.int64), ([64, 64], np.int64), ([32, 32], np.int32)))
+    assert L.cbmv_batch_create(0, Hs.ctypes.data, Ws.ctypes.data, Ds.ctypes.data, 2, ctypes.byref(h)) == -1
+    assert L.cbmv_batch_create(2, Hs.ctypes.data, Ws.ctypes.data, Ds.ctypes.data, 2, ctypes.byref(h)) == -1
+    assert b"pair 1" in L.cbmv_last_error()                               # an 8-row image
+    assert L.cbmv_batch_create(1, Hs.ctypes.data, Ws.ctypes.data, Ds.ctypes.data, 0, ctypes.byref(h)) == -1
+    assert L.cbmv_batch_run_mlp(None, buf, None, buf, buf, buf, None) == -1
+    assert L.cbmv_cbca_separable(buf, buf, buf, 10, 10, 4, 12, -1, buf, None) == -1   # L1 > 9
+    assert L.cbmv_cbca_separable(buf, buf, buf, 10, 10, 4, 6, -1, buf, None) == -1    # in == out
+    assert L.cbmv_run_post(None, None, buf, buf, 10, 10, 4, buf, buf) == -1
+    prm = _lib.default_params(cbca_rows=24)
+    assert L.cbmv_run_mlp(buf, buf, ctypes.byref(prm), buf, buf, 64, 64, 32, buf, None) != 0
+    assert b"cbca_rows" in L.cbmv_last_error()
+    prm = _lib.default_params(sgm_prefetch=3)
+    assert L.cbmv_run_mlp(buf, buf, ctypes.byref(prm), buf, buf, 64, 64, 32, buf, None) != 0
+    assert b"sgm_prefetch" in L.cbmv_last_error()
+
+
 def test_forest_upload_validation():
     import numpy as np
     from cbmv_b200 import _lib
@@ -69,3 +94,36 @@ def test_forest_upload_validation():
     bad[0, 3] = 25
     assert L.cbmv_forest_create(bad.ctypes.data, 1, leafv.ctypes.data, 2, offs.ctypes.data, 1, 20,
                                 ctypes.byref(h)) == -1
+
+
+def test_learned_classifier_falls_back_to_the_forest():
+    """StereoPipeline.run_classified: the network's result when it ran
+    cleanly, the forest's when the network call failed or reported a
+    tensor-core timeout (the pipeline's calls stubbed: host logic only)."""
+    import pytest
+    from cbmv_b200 import _lib
+    from cbmv_b200.pipeline import StereoPipeline
+
+    class Net:
+        def __init__(self, status):
+            self.s = status
+
+        def status(self):
+            return self.s
+
+    p = StereoPipeline.__new__(StereoPipeline)  # no device context needed for the stubs
+    p.forest = object()
+    p.run_rf = lambda *a, **k: "rf-disparity"
+    p.run_mlp = lambda net, *a, **k: "mlp-disparity"
+    assert p.run_classified(None, None, 8, net=Net(0)) == ("mlp-disparity", "mlp")
+    assert p.run_classified(None, None, 8, net=Net(1)) == ("rf-disparity", "rf")
+    assert p.run_classified(None, None, 8) == ("rf-disparity", "rf")
+
+    def fail(*a, **k):
+        raise _lib.CbmvError("cbmv_run_mlp", -2, "injected")
+    p.run_mlp = fail
+    assert p.run_classified(None, None, 8, net=Net(0)) == ("rf-disparity", "rf")
+    p.forest = None
+    with pytest.raises(RuntimeError):
+        p.run_classified(None, None, 8, net=Net(0))
+    p.ctx = None  # nothing to release
