@@ -533,15 +533,16 @@ extern "C" int cbmv_mlp_status(const cbmv_mlp* n, int* status) {
 // Fused inference: features of 128 consecutive (pixel, d) samples -> the
 // network on the tensor cores -> matching cost 1 - P(correct), float32.
 //
-// One persistent CTA per SM, four independent groups of 256 threads; each
+// One persistent CTA per SM, four independent groups of 128 threads; each
 // group owns a 128-row tile in flight (its activation buffer in shared
 // memory and 128 tensor-memory columns), so while one group's MMAs run the
-// others compute features or epilogues.  Threads r and r + 128 of a group
-// share row r of its tile: each forms the features of two matchers of
-// sample r, then handles half of that row's columns in each epilogue.  The
-// group's first thread issues its MMAs, commits them to the group's
-// mbarrier and alone polls it; the others wait on the group's named barrier
-// (no issue slots spent spinning), which also hands them the poll's result.
+// others compute features or epilogues.  Thread r of a group owns row r of
+// its tile: it forms the 20 features of sample r (their inputs for the
+// next tile are loaded while this one runs through the network), then
+// that row's columns in each epilogue.  The group's first thread issues
+// its MMAs, commits them to the group's mbarrier and alone polls it; the
+// others wait on the group's named barrier (no issue slots spent
+// spinning), which also hands them the poll's result.
 //
 // Arithmetic, per layer (the float32 accumulator in tensor memory):
 //   layer 1  K = 32: 20 normalised features, two constant-one columns whose
@@ -569,7 +570,7 @@ struct FeatVolsF {
 };
 
 constexpr int kGroups = 4;                        // tiles in flight per CTA
-constexpr int kGroupThreads = 256;               // two threads per tile row
+constexpr int kGroupThreads = 128;               // one thread per tile row
 constexpr int kInfThreads = kGroupThreads * kGroups;
 constexpr size_t kSmW1i = 128 * 128;      // [128 x 64] SW128, K = 32 used
 constexpr size_t kSmW2i = 2 * 128 * 128;  // [128 x 128]
@@ -577,7 +578,7 @@ constexpr size_t kSmW3i = 2 * 64 * 128;   // [64 x 128]
 constexpr size_t kSmW4i = 16 * 128;       // [16 x 64]
 constexpr size_t kSmTile = 2 * 128 * 128; // a group's activation tile [128 x 128]
 constexpr size_t kSmInf = 1024 + kSmW1i + kSmW2i + kSmW3i + kSmW4i + kGroups * kSmTile;
-constexpr uint16_t kBf16One = 0x3F80;
+constexpr uint32_t kBf16OneOne = 0x3F803F80u;  // two bf16 ones
 
 static __constant__ float kEpsF[4] = {0.01f, 1.01f, 0.01f, 0.01f};
 static __constant__ float kInvSigmaF[4] = {(float)(1.0 / (2.0 * 8 * 8)), (float)(1.0 / 0.02),
@@ -598,15 +599,6 @@ __device__ __forceinline__ bool group_all(int g, bool v) {
       : "r"((uint32_t)v), "r"(g + 1), "n"(kGroupThreads)
       : "memory");
   return r != 0;
-}
-
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
-          taddr),
-      "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]),
-      "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15])
-      : "memory");
 }
 
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
@@ -670,34 +662,80 @@ __device__ void stage_inference_weights(const float* __restrict__ P, unsigned ch
   }
 }
 
-// One hidden-layer epilogue of row `row`, this thread's NC accumulator
-// columns from c_begin: 2*GELU as bf16 into the activation tile; the first
-// `nprefill` of these columns then receive the next layer's bias.
-template <int NC>
-__device__ __forceinline__ void epilogue_hidden(uint32_t tlane, unsigned char* sA, int row, int c_begin,
-                                                const float* next_bias, int nprefill) {
+// Row `row` of a K-major SW128 activation tile: 16-byte chunk j (columns
+// 8j .. 8j+7 of a 64-column atom) of atom a sits at
+// rowp + a * 128 * 128 + ((j << 4) ^ r7s), r7s = (row % 8) << 4.
+__device__ __forceinline__ uint4* tile_chunk(unsigned char* rowp, int r7s, int a, int j) {
+  return reinterpret_cast<uint4*>(rowp + a * 128 * 128 + ((j << 4) ^ r7s));
+}
+
+// One hidden-layer epilogue of this thread's row: accumulator columns
+// 0 .. NC-1 -> 2*GELU as bf16 into the activation tile; the first
+// `nprefill` columns then receive the next layer's bias.
+// 2*GELU of 32 loaded accumulator columns c .. c+31 -> the activation tile;
+// then the next layer's bias into those columns if c < nprefill
+__device__ __forceinline__ void epilogue_chunk(uint32_t tlane, unsigned char* rowp, int r7s, int c, uint32_t* v,
+                                               const float* next_bias, int nprefill) {
+  uint32_t h[16];
 #pragma unroll
-  for (int c = c_begin; c < c_begin + NC; c += 16) {
-    float v[16];
-    umma::tmem_ld16(tlane + c, v);
-    uint32_t h[8];
+  for (int i = 0; i < 16; i++) h[i] = gelu2x_bf16(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
 #pragma unroll
-    for (int i = 0; i < 8; i++) h[i] = gelu2x_bf16(v[2 * i], v[2 * i + 1]);
-    *reinterpret_cast<uint4*>(sA + umma::sw128_offset(128, row, c)) = make_uint4(h[0], h[1], h[2], h[3]);
-    *reinterpret_cast<uint4*>(sA + umma::sw128_offset(128, row, c + 8)) = make_uint4(h[4], h[5], h[6], h[7]);
-    if (c - c_begin < nprefill) {
+  for (int q = 0; q < 4; q++)
+    *tile_chunk(rowp, r7s, c >> 6, ((c & 63) >> 3) + q) = make_uint4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);
+  if (c < nprefill) {
 #pragma unroll
-      for (int i = 0; i < 16; i += 4) {
-        const float4 q = *reinterpret_cast<const float4*>(next_bias + c + i);
-        v[i] = q.x;
-        v[i + 1] = q.y;
-        v[i + 2] = q.z;
-        v[i + 3] = q.w;
-      }
-      tmem_st16(tlane + c, v);
+    for (int i = 0; i < 32; i += 4) {
+      const uint4 q = *reinterpret_cast<const uint4*>(next_bias + c + i);
+      v[i] = q.x;
+      v[i + 1] = q.y;
+      v[i + 2] = q.z;
+      v[i + 3] = q.w;
     }
+    umma::tmem_st32(tlane + c, v);
+  }
+}
+
+// One hidden-layer epilogue of this thread's row: accumulator columns
+// 0 .. NC-1 -> 2*GELU as bf16 into the activation tile; the first
+// `nprefill` columns then receive the next layer's bias.  The load of the
+// next 32 columns is in flight while the current ones are computed.
+template <int NC>
+__device__ __forceinline__ void epilogue_hidden(uint32_t tlane, unsigned char* rowp, int r7s,
+                                                const float* next_bias, int nprefill) {
+  uint32_t va[32], vb[32];
+  umma::tmem_ld32_issue(tlane, va);
+  umma::tmem_ld32_wait(va);
+#pragma unroll 1
+  for (int c = 0; c < NC; c += 64) {
+    umma::tmem_ld32_issue(tlane + c + 32, vb);
+    epilogue_chunk(tlane, rowp, r7s, c, va, next_bias, nprefill);
+    umma::tmem_ld32_wait(vb);
+    if (c + 64 < NC) umma::tmem_ld32_issue(tlane + c + 64, va);
+    epilogue_chunk(tlane, rowp, r7s, c + 32, vb, next_bias, nprefill);
+    if (c + 64 < NC) umma::tmem_ld32_wait(va);
   }
   if (nprefill > 0) tmem_wait_st();
+}
+
+// Inputs of the four matchers' features of one sample: its costs and the
+// row statistics (min, 1/den) of its left and right views.
+struct FeatIn {
+  float c[4];
+  float2 sl[4], sr[4];
+};
+
+__device__ __forceinline__ void load_feat_in(const FeatVolsF& fv, const float2* __restrict__ statsf, int64_t HW,
+                                             int64_t N, int64_t t, int64_t p, int d, int64_t x, FeatIn& in) {
+  const bool valid = t < N;
+  const int64_t tv = valid ? t : 0, pv = valid ? p : 0;
+  const int dv = valid ? d : 0;
+  const bool has_right = valid && x >= d;
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    in.c[m] = __ldg(fv.v[m] + tv);
+    in.sl[m] = __ldg(statsf + (int64_t)(2 * m) * HW + pv);
+    in.sr[m] = has_right ? __ldg(statsf + (int64_t)(2 * m + 1) * HW + pv - dv) : make_float2(kRandMaxF, 0.0f);
+  }
 }
 
 __global__ void __launch_bounds__(kInfThreads, 1)
@@ -716,8 +754,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   __shared__ float s_b4;
   __shared__ uint64_t bars[kGroups];
   __shared__ uint32_t tmem_base;
-  const int tid = threadIdx.x, g = tid / kGroupThreads, gt = tid % kGroupThreads;
-  const int row = gt & 127, half = gt >> 7, wq = (gt >> 5) & 3;
+  const int tid = threadIdx.x, g = tid / kGroupThreads, row = tid % kGroupThreads, wq = row >> 5;
 
   if (tid < 32) umma::tmem_alloc(&tmem_base, 128 * kGroups);
   if (tid < kGroups) umma::mbar_init(&bars[tid], 1);
@@ -732,10 +769,12 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   umma::tc_fence_after();
 
   unsigned char* sA = sTiles + g * kSmTile;
+  unsigned char* rowp = sA + (row >> 3) * 1024 + (row & 7) * 128;
+  const int r7s = (row & 7) << 4;
   uint64_t* bar = &bars[g];
   const uint32_t tacc = tmem_base + (uint32_t)(g * 128);
   const uint32_t tlane = tacc + ((uint32_t)(wq * 32) << 16);
-  const bool leader = gt == 0;
+  const bool leader = row == 0;
   constexpr uint32_t id128 = umma::idesc_bf16(128, 128), id64 = umma::idesc_bf16(128, 64),
                      id16 = umma::idesc_bf16(128, 16);
   // operand descriptors, formed where the leader issues (keeps them out of the other threads' registers)
@@ -757,44 +796,42 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   uint32_t phase = 0;
   bool ok = true;
 
-  // this thread's two matchers' ratio epsilon and likelihood 1/sigma
-  const float eps0 = kEpsF[2 * half], eps1 = kEpsF[2 * half + 1];
-  const float isg0 = kInvSigmaF[2 * half], isg1 = kInvSigmaF[2 * half + 1];
+  FeatIn in;
+  load_feat_in(fv, statsf, HW, N, t, p, d, x, in);
   for (; tile < tiles; tile += tstride) {
-    // 1. features of sample t, matchers 2*half and 2*half+1 -> row of X0 (the first atom of the tile)
+    // 1. the 20 features of sample t -> row of X0 (the first atom of the tile):
+    //    columns 0..19 in the reference's order, 20 and 21 the bias inputs, 22..31 zero
     {
-      const bool valid = t < N;
-      const int64_t tv = valid ? t : 0, pv = valid ? p : 0;
-      const int dv = valid ? d : 0;
-      const bool has_right = valid && x >= d;
-      float f[10];  // f[2q + i]: feature group q of matcher 2*half + i
+      float f[20];
 #pragma unroll
-      for (int i = 0; i < 2; i++) {
-        const int m = 2 * half + i;
-        const float* vol = i == 0 ? (half ? fv.v[2] : fv.v[0]) : (half ? fv.v[3] : fv.v[1]);
-        const float c = __ldg(vol + tv);
-        const float2 sl = statsf[(int64_t)(m * 2) * HW + pv];
-        const float2 sr = has_right ? statsf[(int64_t)(m * 2 + 1) * HW + pv - dv] : make_float2(kRandMaxF, 0.0f);
-        const float eps = i ? eps1 : eps0, isg = i ? isg1 : isg0;
-        const float inv_ce = __fdividef(1.0f, c + eps);
-        f[i] = c;
-        conf_f32(c, inv_ce, sl, eps, isg, &f[2 + i], &f[4 + i]);
-        conf_f32(c, inv_ce, sr, eps, isg, &f[6 + i], &f[8 + i]);
+      for (int m = 0; m < 4; m++) {
+        const float c = in.c[m];
+        const float inv_ce = __fdividef(1.0f, c + kEpsF[m]);
+        f[m] = c;
+        conf_f32(c, inv_ce, in.sl[m], kEpsF[m], kInvSigmaF[m], &f[4 + m], &f[8 + m]);
+        conf_f32(c, inv_ce, in.sr[m], kEpsF[m], kInvSigmaF[m], &f[12 + m], &f[16 + m]);
       }
+      uint32_t u[10];
 #pragma unroll
-      for (int q = 0; q < 5; q++) {
-        const int k = 4 * q + 2 * half;  // reference column of f[2q]
+      for (int k = 0; k < 20; k += 2) {
         const float4 na = s_nrm[k], nb = s_nrm[k + 1];
-        const float a = (fminf(f[2 * q], na.x) - na.y) * na.z;
-        const float b = (fminf(f[2 * q + 1], nb.x) - nb.y) * nb.z;
-        *reinterpret_cast<uint32_t*>(sA + umma::sw128_offset(128, row, k)) = pack_bf16x2(a, b);
+        u[k >> 1] = pack_bf16x2((fminf(f[k], na.x) - na.y) * na.z, (fminf(f[k + 1], nb.x) - nb.y) * nb.z);
       }
-      if (half) {  // columns 20, 21: the bias inputs; 22..31: zero
-        *reinterpret_cast<uint2*>(sA + umma::sw128_offset(128, row, 20)) =
-            make_uint2((uint32_t)kBf16One | ((uint32_t)kBf16One << 16), 0u);
-        *reinterpret_cast<uint4*>(sA + umma::sw128_offset(128, row, 24)) = make_uint4(0u, 0u, 0u, 0u);
-      }
+      *tile_chunk(rowp, r7s, 0, 0) = make_uint4(u[0], u[1], u[2], u[3]);
+      *tile_chunk(rowp, r7s, 0, 1) = make_uint4(u[4], u[5], u[6], u[7]);
+      *tile_chunk(rowp, r7s, 0, 2) = make_uint4(u[8], u[9], kBf16OneOne, 0u);
+      *tile_chunk(rowp, r7s, 0, 3) = make_uint4(0u, 0u, 0u, 0u);
     }
+    // the next sample's inputs, in flight while this tile runs through the network
+    int64_t tn = t + step, pn = p + sp, xn = x + sx;
+    int dn = d + sd;
+    if (dn >= D) {
+      dn -= D;
+      pn += 1;
+      xn += 1;
+    }
+    if (xn >= W) xn -= W;
+    if (tile + tstride < tiles) load_feat_in(fv, statsf, HW, N, tn, pn, dn, xn, in);
     umma::fence_async_smem();
     umma::tc_fence_before();
     group_sync(g);
@@ -810,7 +847,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
-    epilogue_hidden<64>(tlane, sA, row, 64 * half, s_b2, 64);
+    epilogue_hidden<128>(tlane, rowp, r7s, s_b2, 128);
     umma::fence_async_smem();
     umma::tc_fence_before();
     group_sync(g);
@@ -828,8 +865,8 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
-    // b3 goes to columns 0..63, which only the first half has read
-    epilogue_hidden<64>(tlane, sA, row, 64 * half, s_b3, half ? 0 : 64);
+    // b3 goes to columns 0..63 once they are read
+    epilogue_hidden<128>(tlane, rowp, r7s, s_b3, 64);
     umma::fence_async_smem();
     umma::tc_fence_before();
     group_sync(g);
@@ -847,7 +884,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
-    epilogue_hidden<32>(tlane, sA, row, 32 * half, nullptr, 0);
+    epilogue_hidden<64>(tlane, rowp, r7s, nullptr, 0);
     umma::fence_async_smem();
     umma::tc_fence_before();
     group_sync(g);
@@ -863,27 +900,20 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
-    if (half == 0) {
+    {
       uint32_t z2[2];
       asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];"
                    : "=r"(z2[0]), "=r"(z2[1])
                    : "r"(tlane + 64));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(z2[0]), "+r"(z2[1]) : : "memory");
       const float z = (__uint_as_float(z2[0]) + __uint_as_float(z2[1])) + s_b4;
       if (t < N) prob0[t] = 1.0f / (1.0f + __expf(z));
     }
     umma::tc_fence_before();
-    // advance this thread's sample by tstride tiles
-    t += step;
-    p += sp;
-    d += sd;
-    x += sx;
-    if (d >= D) {
-      d -= D;
-      p += 1;
-      x += 1;
-    }
-    if (x >= W) x -= W;
+    t = tn;
+    p = pn;
+    d = dn;
+    x = xn;
   }
   if (!ok) {
     // let this group's MMAs still in flight finish (bounded) before the memory is freed
