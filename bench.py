@@ -43,8 +43,9 @@ METRIC = "pixel·disparities/s end-to-end at 694×554, D=128; MLP vs RF at match
 BYTES_PER_UNIT_FUSED = 4.0  # algorithmic HBM bytes of matchers+features+classifier per (p,d)
 # dense flops of the 20-128-128-64-1 network per (p,d): 2*(20*128 + 128*128 + 128*64 + 64)
 FLOPS_PER_UNIT_MLP = 2.0 * (20 * 128 + 128 * 128 + 128 * 64 + 64)
-MUFU_PER_UNIT_MLP = 128 + 128 + 64  # one tanh per hidden activation
-MUFU_PER_CLK_SM = 16                # special-function results per clock per SM (measured)
+# MMA work the fused kernel issues per (pixel, d): layer 1 K = 32 (20 inputs + 2 bias ones + padding),
+# the K = 16 bias MMAs of layers 2 and 3, layer 4 as N = 16 (w4 high + low rows and padding)
+MMA_FLOPS_PER_UNIT_MLP = 2 * (32 * 128 + 16 * 128 + 128 * 128 + 16 * 64 + 128 * 64 + 64 * 16)
 
 
 def peaks():
@@ -257,9 +258,6 @@ def run_cbmv(a, ws, rank, local):
 
     hbm, hbm_kind = peaks()
     tc, tc_kind = tensor_peak()
-    props = torch.cuda.get_device_properties(dev)
-    sms = props.multi_processor_count
-    sm_hz = (clk.summary().get("sm_mhz") or 1965.0) * 1e6
     traffic = {}
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
@@ -274,15 +272,15 @@ def run_cbmv(a, ws, rank, local):
     if "mlp" in res:
         mlp_tflops = FLOPS_PER_UNIT_MLP * units / (res["mlp"]["stage_ms"]["classify"] / 1e3) / 1e12
         t_cls = res["mlp"]["stage_ms"]["classify"]
-        mufu_floor_ms = MUFU_PER_UNIT_MLP * units / (MUFU_PER_CLK_SM * sms * sm_hz) * 1e3
+        mma_floor_ms = MMA_FLOPS_PER_UNIT_MLP * units / (tc * 1e12) * 1e3
         roof_mlp = {"bound": "tensor", "kernel": "features_mlp_kernel", "achieved": mlp_tflops,
                     "peak": tc, "unit": "TFLOP/s", "frac": mlp_tflops / tc,
                     "traffic": traffic.get("features_mlp_kernel"), "peak_kind": tc_kind,
                     "flops_per_unit": FLOPS_PER_UNIT_MLP,
-                    "mufu": {"tanh_per_unit": MUFU_PER_UNIT_MLP, "floor_ms": mufu_floor_ms,
-                             "frac": mufu_floor_ms / t_cls,
-                             "note": "GELU's tanh runs on the 16-per-clock-per-SM special-function "
-                                     "unit (packed bf16 tanh costs two issues): the kernel's real bound"},
+                    "mma_issued": {"flops_per_unit": MMA_FLOPS_PER_UNIT_MLP, "floor_ms": mma_floor_ms,
+                                   "frac": mma_floor_ms / t_cls,
+                                   "note": "tensor time of the MMAs as issued (padding and bias MMAs "
+                                           "included) at the measured peak"},
                     "note": "dense flops of 20-128-128-64-1 per (pixel,d); the kernel also builds "
                             "the 20 features from the four float32 cost volumes"}
         res["mlp"]["roofline"] = roof_mlp

@@ -129,7 +129,7 @@ extern "C" int cbmv_gemm_bf16(const uint16_t* A, const uint16_t* B, float* C, in
 }
 
 // ====================================================================
-// MLP: 20 -> 128 -> 128 -> 64 -> 1, GELU (tanh form), sigmoid output.
+// MLP: 20 -> 128 -> 128 -> 64 -> 1, ReLU, sigmoid output.
 // Parameter vector (float32, host order):
 //   cap[20] mu[20] inv_sd[20]        input transform x' = (min(x,cap)-mu)*inv_sd
 //   W1[128x20] b1[128] W2[128x128] b2[128] W3[64x128] b3[64] w4[64] b4[1]
@@ -146,12 +146,10 @@ constexpr int kOffW1 = kNormN, kOffB1 = kOffW1 + kH1 * kF, kOffW2 = kOffB1 + kH1
               kOffB2 = kOffW2 + kH2 * kH1, kOffW3 = kOffB2 + kH2, kOffB3 = kOffW3 + kH3 * kH2,
               kOffW4 = kOffB3 + kH3, kOffB4 = kOffW4 + kH3, kNParams = kOffB4 + 1;
 
-__device__ __forceinline__ float gelu_t(float x, float* dgelu) {
-  const float k0 = 0.7978845608028654f, k1 = 0.044715f;
-  const float u = k0 * (x + k1 * x * x * x);
-  const float t = tanhf(u);
-  if (dgelu) *dgelu = 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * k0 * (1.0f + 3.0f * k1 * x * x);
-  return 0.5f * x * (1.0f + t);
+// ReLU and its derivative (0 at x = 0)
+__device__ __forceinline__ float relu_t(float x, float* drelu) {
+  if (drelu) *drelu = x > 0.0f ? 1.0f : 0.0f;
+  return x > 0.0f ? x : 0.0f;
 }
 
 __device__ __forceinline__ uint16_t to_bf16(float x) {
@@ -173,15 +171,15 @@ __global__ void mlp_prep_kernel(const float* __restrict__ X, int B, const float*
   }
 }
 
-// S = Z + b; A = gelu(S) as bf16 [B,N] and [N,B]; Af = gelu(S) float (optional)
-__global__ void mlp_bias_gelu_kernel(const float* __restrict__ Z, const float* __restrict__ bias, int B,
+// S = Z + b; A = relu(S) as bf16 [B,N] and [N,B]; Af = relu(S) float (optional)
+__global__ void mlp_bias_relu_kernel(const float* __restrict__ Z, const float* __restrict__ bias, int B,
                                      int N, float* __restrict__ S, uint16_t* __restrict__ A,
                                      uint16_t* __restrict__ AT, float* __restrict__ Af) {
   GS(t, (int64_t)B * N) {
     const int b = (int)(t / N), n = (int)(t % N);
     const float s = Z[t] + bias[n];
     S[t] = s;
-    const float a = gelu_t(s, nullptr);
+    const float a = relu_t(s, nullptr);
     if (A) A[t] = to_bf16(a);
     if (AT) AT[(int64_t)n * B + b] = to_bf16(a);
     if (Af) Af[t] = a;
@@ -190,7 +188,7 @@ __global__ void mlp_bias_gelu_kernel(const float* __restrict__ Z, const float* _
 
 // output layer, loss and the first backward step, one warp per sample:
 // z = A3 . w4 + b4, p = sigmoid(z), loss_i = BCE; dz = (p - y) / B;
-// dS3 = dz * w4 * gelu'(S3) -> bf16 [B,64] and [64,B]; per-sample dz and
+// dS3 = dz * w4 * relu'(S3) -> bf16 [B,64] and [64,B]; per-sample dz and
 // dz*A3 kept for the (ordered) reductions of dw4 / db4.
 __global__ void mlp_head_kernel(const float* __restrict__ A3f, const float* __restrict__ S3,
                                 const float* __restrict__ y, const float* __restrict__ P, int B,
@@ -215,7 +213,7 @@ __global__ void mlp_head_kernel(const float* __restrict__ A3f, const float* __re
     }
     for (int k = lane; k < kH3; k += 32) {
       float dg;
-      gelu_t(S3[(int64_t)b * kH3 + k], &dg);
+      relu_t(S3[(int64_t)b * kH3 + k], &dg);
       const float d = g * P[kOffW4 + k] * dg;
       dS3[(int64_t)b * kH3 + k] = to_bf16(d);
       dS3T[(int64_t)k * B + b] = to_bf16(d);
@@ -225,14 +223,14 @@ __global__ void mlp_head_kernel(const float* __restrict__ A3f, const float* __re
   }
 }
 
-// dS = dA * gelu'(S) -> bf16 [B,N], [N,B] and float [B,N]
-__global__ void mlp_dgelu_kernel(const float* __restrict__ dA, const float* __restrict__ S, int B, int N,
+// dS = dA * relu'(S) -> bf16 [B,N], [N,B] and float [B,N]
+__global__ void mlp_drelu_kernel(const float* __restrict__ dA, const float* __restrict__ S, int B, int N,
                                  uint16_t* __restrict__ dS, uint16_t* __restrict__ dST,
                                  float* __restrict__ dSf) {
   GS(t, (int64_t)B * N) {
     const int b = (int)(t / N), n = (int)(t % N);
     float dg;
-    gelu_t(S[t], &dg);
+    relu_t(S[t], &dg);
     const float d = dA[t] * dg;
     dS[t] = to_bf16(d);
     dST[(int64_t)n * B + b] = to_bf16(d);
@@ -461,11 +459,11 @@ int mlp_fwd_bwd(cbmv_mlp* n, const float* X, const float* y, cudaStream_t st) {
   int rc;
   mlp_prep_kernel<<<g, 256, 0, st>>>(X, B, n->P, n->X0, n->X0T);
   if ((rc = launch_gemm_bf16(n->X0, n->W1b, n->Z, B, kH1, kK1, n->status, st))) return rc;
-  mlp_bias_gelu_kernel<<<g, 256, 0, st>>>(n->Z, n->P + kOffB1, B, kH1, n->S1, n->A1, n->A1T, nullptr);
+  mlp_bias_relu_kernel<<<g, 256, 0, st>>>(n->Z, n->P + kOffB1, B, kH1, n->S1, n->A1, n->A1T, nullptr);
   if ((rc = launch_gemm_bf16(n->A1, n->W2b, n->Z, B, kH2, kH1, n->status, st))) return rc;
-  mlp_bias_gelu_kernel<<<g, 256, 0, st>>>(n->Z, n->P + kOffB2, B, kH2, n->S2, n->A2, n->A2T, nullptr);
+  mlp_bias_relu_kernel<<<g, 256, 0, st>>>(n->Z, n->P + kOffB2, B, kH2, n->S2, n->A2, n->A2T, nullptr);
   if ((rc = launch_gemm_bf16(n->A2, n->W3b, n->Z, B, kH3, kH2, n->status, st))) return rc;
-  mlp_bias_gelu_kernel<<<g, 256, 0, st>>>(n->Z, n->P + kOffB3, B, kH3, n->S3, nullptr, nullptr, n->A3f);
+  mlp_bias_relu_kernel<<<g, 256, 0, st>>>(n->Z, n->P + kOffB3, B, kH3, n->S3, nullptr, nullptr, n->A3f);
   mlp_head_kernel<<<grid_for((int64_t)B * 32, 256), 256, 0, st>>>(n->A3f, n->S3, y, n->P, B, n->loss_i,
                                                                   n->dz, n->dw4_i, n->dS3, n->dS3T, n->dSf);
   mlp_colsum_kernel<<<1, 64, 0, st>>>(n->dw4_i, B, kH3, n->dw4);
@@ -475,12 +473,12 @@ int mlp_fwd_bwd(cbmv_mlp* n, const float* X, const float* y, cudaStream_t st) {
   // layer 3: dW3^T = A2^T dS3, dA2 = dS3 W3
   if ((rc = launch_gemm_bf16(n->A2T, n->dS3T, n->dW3T, kH2, kH3, B, n->status, st))) return rc;
   if ((rc = launch_gemm_bf16(n->dS3, n->W3T, n->dA, B, kH2, kH3, n->status, st))) return rc;
-  mlp_dgelu_kernel<<<g, 256, 0, st>>>(n->dA, n->S2, B, kH2, n->dS2, n->dS2T, n->dSf);
+  mlp_drelu_kernel<<<g, 256, 0, st>>>(n->dA, n->S2, B, kH2, n->dS2, n->dS2T, n->dSf);
   mlp_colsum_kernel<<<1, 128, 0, st>>>(n->dSf, B, kH2, n->db2);
   // layer 2: dW2 = dS2^T A1, dA1 = dS2 W2
   if ((rc = launch_gemm_bf16(n->dS2T, n->A1T, n->dW2, kH2, kH1, B, n->status, st))) return rc;
   if ((rc = launch_gemm_bf16(n->dS2, n->W2T, n->dA, B, kH1, kH2, n->status, st))) return rc;
-  mlp_dgelu_kernel<<<g, 256, 0, st>>>(n->dA, n->S1, B, kH1, n->dS1, n->dS1T, n->dSf);
+  mlp_drelu_kernel<<<g, 256, 0, st>>>(n->dA, n->S1, B, kH1, n->dS1, n->dS1T, n->dSf);
   mlp_colsum_kernel<<<1, 128, 0, st>>>(n->dSf, B, kH1, n->db1);
   // layer 1: dW1 = dS1^T X0
   if ((rc = launch_gemm_bf16(n->dS1T, n->X0T, n->dW1, kH1, kK1, B, n->status, st))) return rc;
@@ -544,18 +542,19 @@ extern "C" int cbmv_mlp_status(const cbmv_mlp* n, int* status) {
 // others wait on the group's named barrier (no issue slots spent
 // spinning), which also hands them the poll's result.
 //
-// Arithmetic, per layer (the float32 accumulator in tensor memory):
+// Arithmetic, per layer (the float32 accumulator in tensor memory); every
+// bias enters as bf16 high + low parts multiplied by constant ones:
 //   layer 1  K = 32: 20 normalised features, two constant-one columns whose
-//            weights are b1 split into bf16 high and low parts, zeros;
-//   layers 2, 3: the bias is stored into the accumulator (tcgen05.st)
-//            before the MMA, which accumulates onto it;
-//   hidden activations are kept as 2 * GELU(s) in bf16 -- computed as
-//            x * (1 + tanh(k0 * x * (1 + k1 * x^2))) on packed bf16 pairs --
-//            and the following layer's weights are staged times 0.5 (an
-//            exact scaling), so the products are unchanged;
+//            weights are b1's parts, zeros;
+//   layers 2, 3: a first K = 16 MMA of a constant tile (ones in columns 0
+//            and 1) against b2's / b3's parts (stored in the unused K
+//            columns 32..63 of layer 1's weight tile) initialises the
+//            accumulator, the layer's MMAs accumulate onto it;
+//   hidden activations: ReLU and the bf16 rounding in one instruction
+//            (cvt.rn.relu.bf16x2.f32) per pair of columns;
 //   output   layer 4 is an MMA too: N = 16, rows 0 and 1 of its weight tile
-//            are the high and low bf16 parts of 0.5 * w4, z = D[0] + D[1] +
-//            b4, cost = 1 - sigmoid(z) = 1 / (1 + exp(z)).
+//            are the high and low bf16 parts of w4, z = D[0] + D[1] + b4,
+//            cost = 1 - sigmoid(z) = 1 / (1 + exp(z)).
 // The features themselves are formed in float32 (they enter the network as
 // bf16), from float32 cost volumes and float32 row statistics (min, 1/den),
 // with one reciprocal 1/(c + e) shared by the left and right ratio.
@@ -576,8 +575,10 @@ constexpr size_t kSmW1i = 128 * 128;      // [128 x 64] SW128, K = 32 used
 constexpr size_t kSmW2i = 2 * 128 * 128;  // [128 x 128]
 constexpr size_t kSmW3i = 2 * 64 * 128;   // [64 x 128]
 constexpr size_t kSmW4i = 16 * 128;       // [16 x 64]
+constexpr size_t kSmOne = 128 * 128;      // [128 x 64], ones in columns 0 and 1
 constexpr size_t kSmTile = 2 * 128 * 128; // a group's activation tile [128 x 128]
-constexpr size_t kSmInf = 1024 + kSmW1i + kSmW2i + kSmW3i + kSmW4i + kGroups * kSmTile;
+constexpr size_t kSmInf = 1024 + kSmW1i + kSmW2i + kSmW3i + kSmW4i + kSmOne + kGroups * kSmTile;
+constexpr int kColB2 = 32, kColB3 = 48;  // K columns of layer 1's weight tile holding b2, b3
 constexpr uint32_t kBf16OneOne = 0x3F803F80u;  // two bf16 ones
 
 static __constant__ float kEpsF[4] = {0.01f, 1.01f, 0.01f, 0.01f};
@@ -601,26 +602,18 @@ __device__ __forceinline__ bool group_all(int g, bool v) {
   return r != 0;
 }
 
-__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
-
 // Two float32 values as a packed bf16 pair (low = a), round to nearest even
 __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
   const __nv_bfloat162 x = __floats2bfloat162_rn(a, b);
   return *reinterpret_cast<const uint32_t*>(&x);
 }
 
-// 2 * GELU of two float32 pre-activations, as a packed bf16 pair (low = a)
-__device__ __forceinline__ uint32_t gelu2x_bf16(float a, float b) {
-  const uint32_t xb = pack_bf16x2(a, b);
-  const __nv_bfloat162 x = *reinterpret_cast<const __nv_bfloat162*>(&xb);
-  const __nv_bfloat162 c0 = __float2bfloat162_rn(0.7978845608028654f);
-  const __nv_bfloat162 c1 = __float2bfloat162_rn(0.7978845608028654f * 0.044715f);
-  const __nv_bfloat162 u = __hmul2(x, __hfma2(__hmul2(x, x), c1, c0));
-  uint32_t ub = *reinterpret_cast<const uint32_t*>(&u), tb;
-  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(tb) : "r"(ub));
-  const __nv_bfloat162 t = *reinterpret_cast<const __nv_bfloat162*>(&tb);
-  const __nv_bfloat162 r = __hfma2(x, t, x);
-  return *reinterpret_cast<const uint32_t*>(&r);
+// ReLU of two float32 pre-activations, as a packed bf16 pair (low = a),
+// round to nearest even
+__device__ __forceinline__ uint32_t relu_bf16x2(float a, float b) {
+  uint32_t r;
+  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+  return r;
 }
 
 // ratio and likelihood of cost c (featextract.cpp:333 and :440) in float32
@@ -632,33 +625,47 @@ __device__ __forceinline__ void conf_f32(float c, float inv_ce, float2 st, float
   *lik = __expf(-(t * t) * inv_sigma) * st.y;  // 1/den = 0 on sentinel rows
 }
 
-// Stage the inference weights from the float32 parameter vector.
+// bf16 high part of x and the bf16 rounding of the rest: x ~ hi + lo
+__device__ __forceinline__ void split_bf16(float x, float* hi, float* lo) {
+  *hi = __bfloat162float(__float2bfloat16_rn(x));
+  *lo = x - *hi;
+}
+
+// Stage the inference weights from the float32 parameter vector, and the
+// constant tile of the bias MMAs.
 __device__ void stage_inference_weights(const float* __restrict__ P, unsigned char* sW1, unsigned char* sW2,
-                                        unsigned char* sW3, unsigned char* sW4) {
+                                        unsigned char* sW3, unsigned char* sW4, unsigned char* sOne) {
   for (int q = threadIdx.x; q < 128 * 64; q += blockDim.x) {
     const int r = q >> 6, k = q & 63;
-    const float b = P[kOffB1 + r];
-    const float bh = __bfloat162float(__float2bfloat16_rn(b));
-    float v = 0.0f;
-    if (k < kF) v = P[kOffW1 + r * kF + k];
-    else if (k == kF) v = bh;
-    else if (k == kF + 1) v = b - bh;
+    float v = 0.0f, hi, lo;
+    if (k < kF) {
+      v = P[kOffW1 + r * kF + k];
+    } else if (k == kF || k == kF + 1) {
+      split_bf16(P[kOffB1 + r], &hi, &lo);
+      v = k == kF ? hi : lo;
+    } else if (k == kColB2 || k == kColB2 + 1) {
+      split_bf16(P[kOffB2 + r], &hi, &lo);
+      v = k == kColB2 ? hi : lo;
+    } else if (r < kH3 && (k == kColB3 || k == kColB3 + 1)) {
+      split_bf16(P[kOffB3 + r], &hi, &lo);
+      v = k == kColB3 ? hi : lo;
+    }
     *reinterpret_cast<uint16_t*>(sW1 + umma::sw128_offset(128, r, k)) = to_bf16(v);
+    *reinterpret_cast<uint16_t*>(sOne + umma::sw128_offset(128, r, k)) = to_bf16(k < 2 ? 1.0f : 0.0f);
   }
   for (int q = threadIdx.x; q < 128 * 128; q += blockDim.x) {
     const int r = q >> 7, k = q & 127;
-    *reinterpret_cast<uint16_t*>(sW2 + umma::sw128_offset(128, r, k)) = to_bf16(0.5f * P[kOffW2 + q]);
+    *reinterpret_cast<uint16_t*>(sW2 + umma::sw128_offset(128, r, k)) = to_bf16(P[kOffW2 + q]);
   }
   for (int q = threadIdx.x; q < 64 * 128; q += blockDim.x) {
     const int r = q >> 7, k = q & 127;
-    *reinterpret_cast<uint16_t*>(sW3 + umma::sw128_offset(64, r, k)) = to_bf16(0.5f * P[kOffW3 + q]);
+    *reinterpret_cast<uint16_t*>(sW3 + umma::sw128_offset(64, r, k)) = to_bf16(P[kOffW3 + q]);
   }
   for (int q = threadIdx.x; q < 16 * 64; q += blockDim.x) {
     const int r = q >> 6, k = q & 63;
-    const float w = 0.5f * P[kOffW4 + k];
-    const float wh = __bfloat162float(__float2bfloat16_rn(w));
-    const float v = r == 0 ? wh : r == 1 ? w - wh : 0.0f;
-    *reinterpret_cast<uint16_t*>(sW4 + umma::sw128_offset(16, r, k)) = to_bf16(v);
+    float hi, lo;
+    split_bf16(P[kOffW4 + k], &hi, &lo);
+    *reinterpret_cast<uint16_t*>(sW4 + umma::sw128_offset(16, r, k)) = to_bf16(r == 0 ? hi : r == 1 ? lo : 0.0f);
   }
 }
 
@@ -669,52 +676,33 @@ __device__ __forceinline__ uint4* tile_chunk(unsigned char* rowp, int r7s, int a
   return reinterpret_cast<uint4*>(rowp + a * 128 * 128 + ((j << 4) ^ r7s));
 }
 
-// One hidden-layer epilogue of this thread's row: accumulator columns
-// 0 .. NC-1 -> 2*GELU as bf16 into the activation tile; the first
-// `nprefill` columns then receive the next layer's bias.
-// 2*GELU of 32 loaded accumulator columns c .. c+31 -> the activation tile;
-// then the next layer's bias into those columns if c < nprefill
-__device__ __forceinline__ void epilogue_chunk(uint32_t tlane, unsigned char* rowp, int r7s, int c, uint32_t* v,
-                                               const float* next_bias, int nprefill) {
+// ReLU of 32 loaded accumulator columns c .. c+31 -> the activation tile
+__device__ __forceinline__ void epilogue_chunk(unsigned char* rowp, int r7s, int c, const uint32_t* v) {
   uint32_t h[16];
 #pragma unroll
-  for (int i = 0; i < 16; i++) h[i] = gelu2x_bf16(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
+  for (int i = 0; i < 16; i++) h[i] = relu_bf16x2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
 #pragma unroll
   for (int q = 0; q < 4; q++)
     *tile_chunk(rowp, r7s, c >> 6, ((c & 63) >> 3) + q) = make_uint4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);
-  if (c < nprefill) {
-#pragma unroll
-    for (int i = 0; i < 32; i += 4) {
-      const uint4 q = *reinterpret_cast<const uint4*>(next_bias + c + i);
-      v[i] = q.x;
-      v[i + 1] = q.y;
-      v[i + 2] = q.z;
-      v[i + 3] = q.w;
-    }
-    umma::tmem_st32(tlane + c, v);
-  }
 }
 
 // One hidden-layer epilogue of this thread's row: accumulator columns
-// 0 .. NC-1 -> 2*GELU as bf16 into the activation tile; the first
-// `nprefill` columns then receive the next layer's bias.  The load of the
+// 0 .. NC-1 -> ReLU as bf16 into the activation tile.  The load of the
 // next 32 columns is in flight while the current ones are computed.
 template <int NC>
-__device__ __forceinline__ void epilogue_hidden(uint32_t tlane, unsigned char* rowp, int r7s,
-                                                const float* next_bias, int nprefill) {
+__device__ __forceinline__ void epilogue_hidden(uint32_t tlane, unsigned char* rowp, int r7s) {
   uint32_t va[32], vb[32];
   umma::tmem_ld32_issue(tlane, va);
   umma::tmem_ld32_wait(va);
-#pragma unroll 1
+#pragma unroll
   for (int c = 0; c < NC; c += 64) {
     umma::tmem_ld32_issue(tlane + c + 32, vb);
-    epilogue_chunk(tlane, rowp, r7s, c, va, next_bias, nprefill);
+    epilogue_chunk(rowp, r7s, c, va);
     umma::tmem_ld32_wait(vb);
     if (c + 64 < NC) umma::tmem_ld32_issue(tlane + c + 64, va);
-    epilogue_chunk(tlane, rowp, r7s, c + 32, vb, next_bias, nprefill);
+    epilogue_chunk(rowp, r7s, c + 32, vb);
     if (c + 64 < NC) umma::tmem_ld32_wait(va);
   }
-  if (nprefill > 0) tmem_wait_st();
 }
 
 // Inputs of the four matchers' features of one sample: its costs and the
@@ -747,10 +735,9 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   unsigned char* sW2 = sW1 + kSmW1i;
   unsigned char* sW3 = sW2 + kSmW2i;
   unsigned char* sW4 = sW3 + kSmW3i;
-  unsigned char* sTiles = sW4 + kSmW4i;
+  unsigned char* sOne = sW4 + kSmW4i;
+  unsigned char* sTiles = sOne + kSmOne;
   __shared__ float4 s_nrm[kF];  // per feature column: cap, mu, inv_sd
-  __shared__ __align__(16) float s_b2[kH2];
-  __shared__ __align__(16) float s_b3[kH3];
   __shared__ float s_b4;
   __shared__ uint64_t bars[kGroups];
   __shared__ uint32_t tmem_base;
@@ -758,10 +745,8 @@ __global__ void __launch_bounds__(kInfThreads, 1)
 
   if (tid < 32) umma::tmem_alloc(&tmem_base, 128 * kGroups);
   if (tid < kGroups) umma::mbar_init(&bars[tid], 1);
-  stage_inference_weights(P, sW1, sW2, sW3, sW4);
+  stage_inference_weights(P, sW1, sW2, sW3, sW4, sOne);
   for (int i = tid; i < kF; i += kInfThreads) s_nrm[i] = make_float4(P[i], P[kF + i], P[2 * kF + i], 0.0f);
-  for (int i = tid; i < kH2; i += kInfThreads) s_b2[i] = P[kOffB2 + i];
-  for (int i = tid; i < kH3; i += kInfThreads) s_b3[i] = P[kOffB3 + i];
   if (tid == 0) s_b4 = P[kOffB4];
   umma::fence_async_smem();
   umma::tc_fence_before();
@@ -822,16 +807,20 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       *tile_chunk(rowp, r7s, 0, 2) = make_uint4(u[8], u[9], kBf16OneOne, 0u);
       *tile_chunk(rowp, r7s, 0, 3) = make_uint4(0u, 0u, 0u, 0u);
     }
-    // the next sample's inputs, in flight while this tile runs through the network
-    int64_t tn = t + step, pn = p + sp, xn = x + sx;
-    int dn = d + sd;
-    if (dn >= D) {
-      dn -= D;
-      pn += 1;
-      xn += 1;
+    // advance to this thread's next sample (tile + tstride) and load its
+    // inputs, in flight while this tile runs through the network
+    const int64_t t_cur = t;
+    t += step;
+    p += sp;
+    d += sd;
+    x += sx;
+    if (d >= D) {
+      d -= D;
+      p += 1;
+      x += 1;
     }
-    if (xn >= W) xn -= W;
-    if (tile + tstride < tiles) load_feat_in(fv, statsf, HW, N, tn, pn, dn, xn, in);
+    if (x >= W) x -= W;
+    if (tile + tstride < tiles) load_feat_in(fv, statsf, HW, N, t, p, d, x, in);
     umma::fence_async_smem();
     umma::tc_fence_before();
     group_sync(g);
@@ -847,7 +836,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
-    epilogue_hidden<128>(tlane, rowp, r7s, s_b2, 128);
+    epilogue_hidden<128>(tlane, rowp, r7s);
     umma::fence_async_smem();
     umma::tc_fence_before();
     group_sync(g);
@@ -855,6 +844,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     // 3. layer 2 (K = 128) onto the bias b2
     if (leader) {
       const uint64_t dA0 = DESC(sA), dA1 = DESC(sA + 128 * 128), dW20 = DESC(sW2), dW21 = DESC(sW2 + 128 * 128);
+      umma::mma_bf16(tacc, DESC(sOne), DESC(sW1) + 2 * (kColB2 / 16), id128, false);
 #pragma unroll
       for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA0 + 2 * kk, dW20 + 2 * kk, id128, true);
 #pragma unroll
@@ -865,8 +855,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
-    // b3 goes to columns 0..63 once they are read
-    epilogue_hidden<128>(tlane, rowp, r7s, s_b3, 64);
+    epilogue_hidden<128>(tlane, rowp, r7s);
     umma::fence_async_smem();
     umma::tc_fence_before();
     group_sync(g);
@@ -874,6 +863,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     // 4. layer 3 (N = 64) onto the bias b3
     if (leader) {
       const uint64_t dA0 = DESC(sA), dA1 = DESC(sA + 128 * 128), dW30 = DESC(sW3), dW31 = DESC(sW3 + 64 * 128);
+      umma::mma_bf16(tacc, DESC(sOne), DESC(sW1) + 2 * (kColB3 / 16), id64, false);
 #pragma unroll
       for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA0 + 2 * kk, dW30 + 2 * kk, id64, true);
 #pragma unroll
@@ -884,7 +874,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     phase ^= 1u;
     umma::tc_fence_after();
     if (!ok) break;
-    epilogue_hidden<64>(tlane, rowp, r7s, nullptr, 0);
+    epilogue_hidden<64>(tlane, rowp, r7s);
     umma::fence_async_smem();
     umma::tc_fence_before();
     group_sync(g);
@@ -907,13 +897,9 @@ __global__ void __launch_bounds__(kInfThreads, 1)
                    : "r"(tlane + 64));
       asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(z2[0]), "+r"(z2[1]) : : "memory");
       const float z = (__uint_as_float(z2[0]) + __uint_as_float(z2[1])) + s_b4;
-      if (t < N) prob0[t] = 1.0f / (1.0f + __expf(z));
+      if (t_cur < N) prob0[t_cur] = 1.0f / (1.0f + __expf(z));
     }
     umma::tc_fence_before();
-    t = tn;
-    p = pn;
-    d = dn;
-    x = xn;
   }
   if (!ok) {
     // let this group's MMAs still in flight finish (bounded) before the memory is freed

@@ -6,8 +6,8 @@ forest (test.py:603-620) as the per-(pixel, d) matching-probability model.
     loss = tr.step(X, y, lr)                 # X [B,20] float32, y [B] (1 = correct)
     net = tr.params()
 
-Architecture 20 -> 128 -> 128 -> 64 -> 1 with GELU (tanh form) and a sigmoid
-output P(correct); the matching cost handed to the post-processing is
+Architecture 20 -> 128 -> 128 -> 64 -> 1 with ReLU and a sigmoid output
+P(correct); the matching cost handed to the post-processing is
 1 - P, as the reference hands it P(class 0) of the forest.  The parameter
 vector layout is documented in include/cbmv.h (cbmv_mlp_*).
 """
@@ -54,7 +54,8 @@ class MlpParams:
         v["mu"][:] = mu
         v["inv_sd"][:] = 1.0 / np.maximum(sd, 1e-12)
         for (n, k), name in zip(LAYERS + [(1, 64)], ["W1", "W2", "W3", "w4"]):
-            lim = np.sqrt(6.0 / (k + n))  # Glorot-uniform
+            # He-uniform into the ReLU layers, Glorot-uniform into the output
+            lim = np.sqrt(6.0 / k) if n > 1 else np.sqrt(6.0 / (k + n))
             v[name][...] = rng.uniform(-lim, lim, v[name].shape).astype(np.float32)
         return p
 

@@ -198,8 +198,8 @@ int cbmv_forest_predict(const cbmv_forest* f, const float* X, int64_t N, double*
 int cbmv_gemm_bf16(const uint16_t* A, const uint16_t* B, float* C, int64_t M, int64_t N, int64_t K,
                    int* status, void* stream);
 
-/* The classifier network: 20 -> 128 -> 128 -> 64 -> 1, GELU (tanh form),
- * sigmoid output = P(correct match); its matching cost is 1 - P.  Its
+/* The classifier network: 20 -> 128 -> 128 -> 64 -> 1, ReLU, sigmoid
+ * output = P(correct match); its matching cost is 1 - P.  Its
  * parameter vector (float32, cbmv_mlp_num_params() values) is, in order:
  * cap[20], mu[20], inv_sd[20] (input transform x' = (min(x,cap)-mu)*inv_sd),
  * W1[128x20], b1[128], W2[128x128], b2[128], W3[64x128], b3[64], w4[64],

@@ -20,11 +20,9 @@ def bf16(x):
     return r.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-def gelu(x):
-    k0, k1 = 0.7978845608028654, 0.044715
-    t = np.tanh(k0 * (x + k1 * x ** 3))
-    d = 0.5 * (1 + t) + 0.5 * x * (1 - t * t) * k0 * (1 + 3 * k1 * x * x)
-    return 0.5 * x * (1 + t), d
+def relu(x):
+    """ReLU and its derivative (0 at x = 0)."""
+    return np.maximum(x, 0.0), (x > 0).astype(np.float64)
 
 
 def unpack(vec):
@@ -46,11 +44,11 @@ def forward(vec, X):
     c32, m32, s32 = (np.float32(p[k]) for k in ("cap", "mu", "inv_sd"))
     X0 = bf16((np.minimum(np.asarray(X, np.float32), c32) - m32) * s32)
     S1 = X0 @ bf16(p["W1"]).T + p["b1"]
-    A1, d1 = gelu(S1)
+    A1, d1 = relu(S1)
     S2 = bf16(A1) @ bf16(p["W2"]).T + p["b2"]
-    A2, d2 = gelu(S2)
+    A2, d2 = relu(S2)
     S3 = bf16(A2) @ bf16(p["W3"]).T + p["b3"]
-    A3, d3 = gelu(S3)
+    A3, d3 = relu(S3)
     z = A3 @ p["w4"] + p["b4"][0]
     return dict(X0=X0, S1=S1, A1=A1, d1=d1, S2=S2, A2=A2, d2=d2, S3=S3, A3=A3, d3=d3, z=z, p=p)
 
@@ -81,37 +79,26 @@ def loss_and_grads(vec, X, y):
     return loss, g, prob
 
 
-def gelu2_bf16(s):
-    """2 * GELU(s) as the fused inference kernel forms it on packed bf16
-    pairs: x = bf16(s), u = x * (c0 + c1 * x^2),
-    t = tanh(u), r = x * t + x, every operation rounded to bf16 (fma: once)."""
-    c0 = bf16(np.float32(0.7978845608028654))
-    c1 = bf16(np.float32(0.7978845608028654) * np.float32(0.044715))
-    x = bf16(np.asarray(s, np.float32))
-    sq = bf16(x * x)
-    u = bf16(x * bf16(sq * c1 + c0))
-    t = bf16(np.tanh(u))
-    return bf16(x * t + x)
+def split_bf16(x):
+    """bf16 high part of float32 x and the bf16 rounding of the rest."""
+    x = np.asarray(x, np.float32)
+    hi = bf16(x)
+    return hi, bf16(x - np.float32(hi))
 
 
 def forward_fused(vec, X):
     """The network as the fused inference kernel evaluates it (test
-    infrastructure): b1 enters through two constant-one inputs as bf16
-    high + low parts; hidden activations are kept as bf16 2*GELU with the
-    next weights halved (exact); the output layer runs on bf16 activations
-    against the high + low bf16 parts of w4/2.  Returns z."""
+    infrastructure): every bias (and w4) enters as its bf16 high + low
+    parts; hidden activations are ReLU rounded to bf16 (cvt.rn.relu); the
+    output layer runs on those bf16 activations.  Returns z."""
     p = unpack(vec)
     c32, m32, s32 = (np.float32(p[k]) for k in ("cap", "mu", "inv_sd"))
     X0 = bf16((np.minimum(np.asarray(X, np.float32), c32) - m32) * s32)
-    b1h = bf16(p["b1"])
-    b1l = bf16(np.float32(p["b1"]) - np.float32(b1h))
-    S1 = X0 @ bf16(p["W1"]).T + (b1h + b1l)
-    A1 = gelu2_bf16(S1)
-    S2 = A1 @ bf16(0.5 * p["W2"]).T + p["b2"]
-    A2 = gelu2_bf16(S2)
-    S3 = A2 @ bf16(0.5 * p["W3"]).T + p["b3"]
-    A3 = gelu2_bf16(S3)
-    w = np.float32(0.5 * p["w4"])
-    wh = bf16(w)
-    wl = bf16(w - np.float32(wh))
+    b1h, b1l = split_bf16(p["b1"])
+    b2h, b2l = split_bf16(p["b2"])
+    b3h, b3l = split_bf16(p["b3"])
+    wh, wl = split_bf16(p["w4"])
+    A1 = bf16(np.maximum(X0 @ bf16(p["W1"]).T + (b1h + b1l), 0))
+    A2 = bf16(np.maximum(A1 @ bf16(p["W2"]).T + (b2h + b2l), 0))
+    A3 = bf16(np.maximum(A2 @ bf16(p["W3"]).T + (b3h + b3l), 0))
     return A3 @ (wh + wl) + p["b4"][0]

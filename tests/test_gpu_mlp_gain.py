@@ -5,7 +5,7 @@ features, classifier, MC-CNN `_mem` post) is run three ways:
 
 - with the trained bf16 MLP (tests/golden/mlp_694x554.npz, trained by
   cbmv_b200/train_mlp.py on GPU-emitted samples of pairs 2000..2199);
-- with the same network before training (its Glorot initialisation, same
+- with the same network before training (its random initialisation, same
   input transform): the learned weights alone are what differs;
 - without a classifier: the post-processing applied to the normalised census
   cost, the best single matcher (test.py:341-449 driven with that volume),

@@ -109,8 +109,9 @@ def test_learned_path_matches_reference_path(gpu, oracle_cpu, W, H, D):
     reference's test path restated over the oracle (test_model with the
     network as its classifier, then eval_prob with the _mem post in the
     reference's summation order): disparities within 0.5 px on >= 99.5 % of
-    pixels (the device runs tanh.approx and float32 features; the network's
-    cost differs from the oracle's float64 model by ~1e-4 on average)."""
+    pixels (the device forms the features in float32 and rounds activations
+    to bf16; the network's cost differs from the oracle's float64 model by
+    ~1e-4 on average)."""
     import os
     from oracle import glue, mlp_ref
     from cbmv_b200 import synth
