@@ -244,11 +244,18 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
   RC(launch_cross(w.imR, H, W, p->L1, p->tau1, w.crossR, st));
   float* cur = w.volA;
   float* oth = w.volB;
+  // the separable form's supports, shared by a run of passes, in the first
+  // matcher volume (dead during the post; the SGM reuses it in between)
+  const bool masked = !p->exact_cbca && p->L1 - 1 <= kCbcaMaskMaxHalo;
+  uint32_t* masks = reinterpret_cast<uint32_t*>(w.vol[0]);
   auto cbca = [&](const float* in, float* out) {
-    return p->exact_cbca ? launch_cbca(w.crossL, w.crossR, in, H, W, D, CBMV_HWD, p->direction, out, st, p->L1 - 1)
-                         : launch_cbca_sep(w.crossL, w.crossR, in, H, W, D, p->direction, out, st, p->L1 - 1,
-                                           p->cbca_rows == 16 ? 16 : 32);
+    const int rows = p->cbca_rows == 16 ? 16 : 32;
+    if (p->exact_cbca)
+      return launch_cbca(w.crossL, w.crossR, in, H, W, D, CBMV_HWD, p->direction, out, st, p->L1 - 1);
+    if (masked) return launch_cbca_masked(masks, in, H, W, D, out, st, rows);
+    return launch_cbca_sep(w.crossL, w.crossR, in, H, W, D, p->direction, out, st, p->L1 - 1, rows);
   };
+  if (masked && p->cbca_i1 > 0) RC(launch_cbca_mask_build(w.crossL, w.crossR, H, W, D, p->direction, masks, st));
   for (int i = 0; i < p->cbca_i1; i++) {
     RC(cbca(cur, oth));
     float* t = cur; cur = oth; oth = t;
@@ -266,6 +273,7 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
     RC(launch_sgm_combine(so, V, nullptr, 0.25f, oth, st));
     float* t = cur; cur = oth; oth = t;
   }
+  if (masked && p->cbca_i2 > 0) RC(launch_cbca_mask_build(w.crossL, w.crossR, H, W, D, p->direction, masks, st));
   for (int i = 0; i < p->cbca_i2; i++) {
     RC(cbca(cur, oth));
     float* t = cur; cur = oth; oth = t;

@@ -473,6 +473,165 @@ int launch_cbca_sep_h(const float* lc, const float* rc, const float* in, int64_t
   return launch_cbca_sep_ht<HALO, 32>(lc, rc, in, H, W, D, direction, out, st);
 }
 
+// The separable CBCA with its supports precomputed: the support of every
+// (y, x, d) depends on the cross arms only, so the cbca_i2 passes of one
+// post share it.  One 32-bit word per (y, x, d), for arms of at most
+// kMaskHalo pixels:
+//   bits  0..10  taps k = -5..5 of its support row (bit k + 5),
+//   bits 11..21  taps of its support column,
+//   bits 22..28  the number of pixels in its support (at most 121),
+//   bit  31      x + d*direction is outside the image (the input is copied).
+// The passes then sum the same taps in the same ascending order as
+// cbca_hwd_sep_kernel, so the results are bit-identical to it.
+constexpr int kMaskHalo = kCbcaMaskMaxHalo;
+constexpr uint32_t kMaskCopy = 1u << 31;
+
+template <int CS_TY>
+__global__ void __launch_bounds__(256) cbca_mask_build_kernel(const float* __restrict__ lc,
+                                                              const float* __restrict__ rc, int H, int W, int D,
+                                                              int direction, uint32_t* __restrict__ mask) {
+  constexpr int HALO = kMaskHalo;
+  constexpr int SR = CS_TY + 2 * HALO;
+  __shared__ uint8_t sC[SR][CS_TX][CS_TD];     // support-row lengths
+  __shared__ uint16_t sH[CS_TY][CS_TX][CS_TD];  // support-row taps of the tile's own rows
+  const int ntd = (D + CS_TD - 1) / CS_TD, ntx = (W + CS_TX - 1) / CS_TX;
+  const int64_t t = blockIdx.x;
+  const int td = (int)(t % ntd), tx = (int)((t / ntd) % ntx), ty = (int)(t / ((int64_t)ntd * ntx));
+  const int X0 = tx * CS_TX, Y0 = ty * CS_TY;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int d = td * CS_TD + lane, dd = d * direction;
+  const bool dok = d < D;
+  const int64_t HW = (int64_t)H * W;
+  // 1. support rows of the tile's rows and HALO rows above and below
+  for (int r = warp; r < SR; r += 8) {
+    const int yy = Y0 - HALO + r;
+    const bool rok = yy >= 0 && yy < H && dok;
+    const int64_t o = (int64_t)(rok ? yy : 0) * W;
+#pragma unroll
+    for (int c = 0; c < CS_TX; c++) {
+      const int x = X0 + c, xm = x + dd;
+      int cnt = 0;
+      uint32_t hm = 0;
+      if (rok && x < W && xm >= 0 && xm < W) {
+        const int ks = max((int)__ldg(lc + o + x), (int)__ldg(rc + o + xm) - dd) - x;
+        const int kt = min((int)__ldg(lc + HW + o + x), (int)__ldg(rc + HW + o + xm) - dd) - x;
+        cnt = max(kt - ks - 1, 0);
+        const int lo = max(ks + 1, -HALO), hi = min(kt - 1, HALO);
+        if (hi >= lo) hm = ((1u << (hi - lo + 1)) - 1u) << (lo + HALO);
+      }
+      sC[r][c][lane] = (uint8_t)cnt;
+      if (r >= HALO && r < HALO + CS_TY) sH[r - HALO][c][lane] = (uint16_t)hm;
+    }
+  }
+  __syncthreads();
+  // 2. support columns: warp c owns tile column c
+  const int c = warp, x = X0 + c, xm = x + dd;
+  if (x >= W || !dok) return;
+  const bool xok = xm >= 0 && xm < W;
+  for (int cy = 0; cy < CS_TY; cy++) {
+    const int y = Y0 + cy;
+    if (y >= H) break;
+    const int64_t o = (int64_t)y * W;
+    const int64_t id = (o + x) * D + d;
+    if (!xok) {
+      mask[id] = kMaskCopy;
+      continue;
+    }
+    const int ks = max((int)__ldg(lc + 2 * HW + o + x), (int)__ldg(rc + 2 * HW + o + xm)) - y;
+    const int kt = min((int)__ldg(lc + 3 * HW + o + x), (int)__ldg(rc + 3 * HW + o + xm)) - y;
+    uint32_t vm = 0, cnt = 0;
+#pragma unroll
+    for (int k = -HALO; k <= HALO; k++)
+      if (k > ks && k < kt) {
+        vm |= 1u << (k + HALO);
+        cnt += sC[cy + HALO + k][c][lane];
+      }
+    mask[id] = (uint32_t)sH[cy][c][lane] | (vm << 11) | ((cnt & 0x7Fu) << 22);
+  }
+}
+
+// One CBCA pass from the precomputed supports (same tiling and summation
+// order as cbca_hwd_sep_kernel<kMaskHalo>).
+template <int CS_TY>
+__global__ void __launch_bounds__(256, 4) cbca_hwd_mask_kernel(const uint32_t* __restrict__ mask,
+                                                               const float* __restrict__ in, int H, int W,
+                                                               int D, float* __restrict__ out) {
+  constexpr int HALO = kMaskHalo;
+  constexpr int SR = CS_TY + 2 * HALO;
+  constexpr int NV = CS_TX + 2 * HALO;
+  constexpr int G = 8;
+  static_assert(CS_TX == 8 && CS_TY % G == 0, "one warp per tile column");
+  extern __shared__ float sR[];  // [SR][CS_TX][CS_TD]
+  const int ntd = (D + CS_TD - 1) / CS_TD, ntx = (W + CS_TX - 1) / CS_TX;
+  const int64_t t = blockIdx.x;
+  const int td = (int)(t % ntd), tx = (int)((t / ntd) % ntx), ty = (int)(t / ((int64_t)ntd * ntx));
+  const int X0 = tx * CS_TX, Y0 = ty * CS_TY;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int d = td * CS_TD + lane;
+  const bool dok = d < D;
+  // 1. row sums over each (yy, x, d)'s support-row taps
+  for (int r = warp; r < SR; r += 8) {
+    const int yy = Y0 - HALO + r;
+    const bool rok = yy >= 0 && yy < H && dok;
+    const int64_t o = (int64_t)(rok ? yy : 0) * W;
+    const float* row = in + o * D + d;
+    const uint32_t* mrow = mask + o * D + d;
+    float v[NV];
+#pragma unroll
+    for (int j = 0; j < NV; j++) {
+      const int xx = X0 - HALO + j;
+      v[j] = (rok && xx >= 0 && xx < W) ? __ldg(row + (int64_t)xx * D) : 0.0f;
+    }
+#pragma unroll
+    for (int c = 0; c < CS_TX; c++) {
+      const int x = X0 + c;
+      const uint32_t hm = (rok && x < W) ? __ldg(mrow + (int64_t)x * D) : 0u;
+      float sum = 0.0f;
+#pragma unroll
+      for (int k = -HALO; k <= HALO; k++)
+        if (hm & (1u << (k + HALO))) sum += v[c + HALO + k];
+      sR[(r * CS_TX + c) * CS_TD + lane] = sum;
+    }
+  }
+  __syncthreads();
+  // 2. column sums: warp c owns tile column c; G output rows at a time from
+  //    a register window of G + 2*HALO row sums
+  const int c = warp, x = X0 + c;
+  if (x >= W || !dok) return;
+#pragma unroll 1
+  for (int g0 = 0; g0 < CS_TY; g0 += G) {
+    float wr[G + 2 * HALO];
+#pragma unroll
+    for (int j = 0; j < G + 2 * HALO; j++) wr[j] = sR[((g0 + j) * CS_TX + c) * CS_TD + lane];
+#pragma unroll
+    for (int cy = 0; cy < G; cy++) {
+      const int y = Y0 + g0 + cy;
+      if (y >= H) break;
+      const int64_t id = ((int64_t)y * W + x) * D + d;
+      const uint32_t w = __ldg(mask + id);
+      if (w & kMaskCopy) {
+        out[id] = __ldg(in + id);
+        continue;
+      }
+      float sum = 0.0f;
+#pragma unroll
+      for (int k = -HALO; k <= HALO; k++)
+        if (w & (1u << (k + HALO + 11))) sum += wr[cy + HALO + k];
+      out[id] = sum / (float)((w >> 22) & 0x7Fu);
+    }
+  }
+}
+
+template <int TY>
+int launch_cbca_masked_t(const uint32_t* mask, const float* in, int64_t H, int64_t W, int D, float* out,
+                         cudaStream_t st) {
+  constexpr size_t smem = (size_t)(TY + 2 * kMaskHalo) * CS_TX * CS_TD * sizeof(float);
+  const int64_t tiles = (int64_t)((W + CS_TX - 1) / CS_TX) * ((H + TY - 1) / TY) * ((D + CS_TD - 1) / CS_TD);
+  cbca_hwd_mask_kernel<TY><<<(unsigned)tiles, 256, smem, st>>>(mask, in, (int)H, (int)W, D, out);
+  return check_launch("cbca_masked");
+}
+
+
 // Winner-take-all (first minimum, as np.argmin) and the subpixel parabola
 // (post.cu:453-483).  One warp per pixel on [H,W,D] volumes.
 __global__ void wta_subpixel_hwd_kernel(const float* __restrict__ c, int64_t HW, int D,
@@ -816,6 +975,29 @@ int launch_cbca_sep(const float* lc, const float* rc, const float* in, int64_t H
   }
 }
 
+int launch_cbca_mask_build(const float* lc, const float* rc, int64_t H, int64_t W, int D, int direction,
+                           uint32_t* mask, cudaStream_t st) {
+  CBMV_REQUIRE(H < (1 << 30) && W < (1 << 30) &&
+                   (int64_t)((W + CS_TX - 1) / CS_TX) * ((H + 15) / 16) * ((D + CS_TD - 1) / CS_TD) <
+                       ((int64_t)1 << 31),
+               CBMV_ERANGE, "cbca: volume too large");
+  constexpr int TY = 32;
+  const int64_t tiles = (int64_t)((W + CS_TX - 1) / CS_TX) * ((H + TY - 1) / TY) * ((D + CS_TD - 1) / CS_TD);
+  cbca_mask_build_kernel<TY><<<(unsigned)tiles, 256, 0, st>>>(lc, rc, (int)H, (int)W, D, direction, mask);
+  return check_launch("cbca_mask_build");
+}
+
+// tile rows 16 or 32 (the results do not depend on them)
+int launch_cbca_masked(const uint32_t* mask, const float* in, int64_t H, int64_t W, int D, float* out,
+                       cudaStream_t st, int rows) {
+  CBMV_REQUIRE(H < (1 << 30) && W < (1 << 30) &&
+                   (int64_t)((W + CS_TX - 1) / CS_TX) * ((H + 15) / 16) * ((D + CS_TD - 1) / CS_TD) <
+                       ((int64_t)1 << 31),
+               CBMV_ERANGE, "cbca: volume too large");
+  if (rows == 16) return launch_cbca_masked_t<16>(mask, in, H, W, D, out, st);
+  return launch_cbca_masked_t<32>(mask, in, H, W, D, out, st);
+}
+
 int launch_wta_subpixel(const float* cost, int64_t H, int64_t W, int D, float* disp_int,
                         float* disp, cudaStream_t st) {
   wta_subpixel_hwd_kernel<<<grid_for(H * W * 32, 256), 256, 0, st>>>(cost, H * W, D, disp_int, disp);
@@ -914,7 +1096,15 @@ extern "C" int cbmv_cbca_separable(const float* crossL, const float* crossR, con
   CBMV_REQUIRE(in != out, CBMV_EINVAL, "cbca: in and out must differ");
   CBMV_REQUIRE(direction == 1 || direction == -1, CBMV_EINVAL, "direction must be +-1");
   CBMV_REQUIRE(L1 >= 2 && L1 <= 9, CBMV_EINVAL, "cbca_separable: L1 must be in 2..9");
-  return launch_cbca_sep(crossL, crossR, in, H, W, D, direction, out, as_stream(stream), L1 - 1);
+  cudaStream_t st = as_stream(stream);
+  if (L1 - 1 > kCbcaMaskMaxHalo) return launch_cbca_sep(crossL, crossR, in, H, W, D, direction, out, st, L1 - 1);
+  // the pipeline's form: supports precomputed into a stream-ordered scratch buffer
+  uint32_t* mask = nullptr;
+  CBMV_CUDA(cudaMallocAsync(&mask, sizeof(uint32_t) * H * W * D, st));
+  int rc = launch_cbca_mask_build(crossL, crossR, H, W, D, direction, mask, st);
+  if (rc == CBMV_OK) rc = launch_cbca_masked(mask, in, H, W, D, out, st);
+  CBMV_CUDA(cudaFreeAsync(mask, st));
+  return rc;
 }
 
 extern "C" int cbmv_wta(const float* cost, int64_t H, int64_t W, int D, int layout, float* disp,

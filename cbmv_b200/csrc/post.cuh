@@ -36,6 +36,14 @@ int launch_cbca(const float* lc, const float* rc, const float* in, int64_t H, in
 // at most `halo` pixels (L1 - 1), halo 1..8 (larger: the reference-order kernel)
 int launch_cbca_sep(const float* lc, const float* rc, const float* in, int64_t H, int64_t W, int D,
                     int direction, float* out, cudaStream_t st, int halo, int rows = 32);
+// the separable cbca with its supports precomputed (arms of at most 5
+// pixels, L1 <= 6): one 32-bit word per (p,d) in `mask`, built once per
+// cross, then any number of passes; bit-identical to launch_cbca_sep
+int launch_cbca_mask_build(const float* lc, const float* rc, int64_t H, int64_t W, int D, int direction,
+                           uint32_t* mask, cudaStream_t st);
+int launch_cbca_masked(const uint32_t* mask, const float* in, int64_t H, int64_t W, int D, float* out,
+                       cudaStream_t st, int rows = 32);
+constexpr int kCbcaMaskMaxHalo = 5;
 int launch_wta_subpixel(const float* cost, int64_t H, int64_t W, int D, float* disp_int,
                         float* disp, cudaStream_t st);
 int launch_median(const float* in, int64_t H, int64_t W, int k, float* out, cudaStream_t st);

@@ -154,10 +154,12 @@ def test_dropin_post_module_runs_reference_driver(gpu, oracle_cpu, scene):
     assert np.mean(np.abs(got_i - ref_i) <= 0.5) >= 0.99
 
 
-@pytest.mark.parametrize("direction", [-1, 1])
-def test_cbca_separable_matches_model_exactly(gpu, oracle_cpu, scene, direction):
-    """cbmv_cbca_separable (the fused pipeline's default CBCA) against the
-    oracle's float32 model of its summation order: bit-exact; against the
+@pytest.mark.parametrize("direction,L1", [(-1, 6), (1, 6), (-1, 9)])
+def test_cbca_separable_matches_model_exactly(gpu, oracle_cpu, scene, direction, L1):
+    """cbmv_cbca_separable (the fused pipeline's default CBCA: with L1 <= 6
+    its supports precomputed once and read by the pass, with L1 = 9 taps
+    reaching 8 pixels tested on the arms themselves) against the oracle's
+    float32 model of its summation order: bit-exact; against the
     reference-order cbca: relative 1e-5."""
     from cbmv_b200 import _lib
     from oracle import post_model
@@ -166,7 +168,7 @@ def test_cbca_separable_matches_model_exactly(gpu, oracle_cpu, scene, direction)
     H, W = imgl.shape
     tl, tr, ts = _t(lc), _t(rc), _t(vol)
     out = torch.empty_like(ts)
-    _lib.call("cbmv_cbca_separable", tl.data_ptr(), tr.data_ptr(), ts.data_ptr(), H, W, D, 6,
+    _lib.call("cbmv_cbca_separable", tl.data_ptr(), tr.data_ptr(), ts.data_ptr(), H, W, D, L1,
               direction, out.data_ptr(), None)
     ref_order = torch.empty_like(ts)
     _lib.call("cbmv_cbca", tl.data_ptr(), tr.data_ptr(), ts.data_ptr(), H, W, D, _lib.HWD, direction,
