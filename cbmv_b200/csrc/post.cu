@@ -81,7 +81,7 @@ __global__ void grad_kernel(const float* __restrict__ img, int64_t H, int64_t W,
 // lane = d (mod 32), KPL disparities per lane.  The scan runs inside the
 // kernel; the step's costs, D1 and the per-d D2 do not depend on the
 // recursion and are loaded PF steps ahead from a register ring.
-template <int KPL, int PF>
+template <int KPL, int PF, bool FULL>
 __device__ __noinline__ void sgm_scan(const SgmGrad& g, const float* __restrict__ in, int H, int W, int D,
                                       const SgmParams& sp, int line, float* __restrict__ out, const int DIR) {
   const int lane = threadIdx.x & 31;
@@ -103,33 +103,36 @@ __device__ __noinline__ void sgm_scan(const SgmGrad& g, const float* __restrict_
   // the difference to the previous pixel of the scan sits at the later of
   // the two pixels in the neighbour-difference images
   const int gshift = DIR == 1 ? 1 : DIR == 3 ? W : 0;
+  // step s visits pixel p0 + s * pstep, column x0 + s * dx
+  const int64_t p0 = DIR == 0 ? (int64_t)line * W
+                   : DIR == 1 ? (int64_t)line * W + W - 1
+                   : DIR == 2 ? (int64_t)line
+                              : (int64_t)(H - 1) * W + line;
+  const int64_t pstep = DIR == 0 ? 1 : DIR == 1 ? -1 : DIR == 2 ? (int64_t)W : -(int64_t)W;
+  const int x0 = DIR == 0 ? 0 : DIR == 1 ? W - 1 : line;
+  // post.cu:232-237: D2 = 10 when the matching pixel xx = x + d*direction
+  // or its predecessor xx - dx leaves the image, i.e. unless
+  // max(0, dx) <= xx < min(W, W + dx)
+  const int s = sp.direction;
+  const int xlo = max(0, dx);
+  const unsigned xspan = (unsigned)(min(W, W + dx) - xlo);
 
   struct Step {
     float cost[KPL], d2[KPL];
     float d1;
   };
-  auto pix = [&](int step) -> int64_t {
-    if (DIR == 0) return (int64_t)line * W + step;
-    if (DIR == 1) return (int64_t)line * W + (W - 1 - step);
-    if (DIR == 2) return (int64_t)step * W + line;
-    return (int64_t)(H - 1 - step) * W + line;
-  };
-  auto load = [&](int step, Step& s) {
-    const int64_t ind2 = pix(step);
-    const int x = DIR <= 1 ? (DIR == 0 ? step : W - 1 - step) : line;
-    const float* src = in + ind2 * D;
-    s.d1 = step > 0 ? gl[ind2 + gshift] : 0.0f;
+  auto load = [&](int step, Step& st) {
+    const int64_t ind2 = p0 + step * pstep;
+    const int xl = x0 + step * dx + lane * s - xlo;  // xx - xlo of this lane's d = lane
+    const float* src = in + ind2 * D + lane;
+    const float* grp = gr + ind2 + gshift + lane * s;
+    st.d1 = step > 0 ? gl[ind2 + gshift] : 0.0f;
 #pragma unroll
     for (int k = 0; k < KPL; k++) {
-      const int d = lane + 32 * k;
-      s.cost[k] = d < D ? src[d] : inf;
-      const int xx = x + d * sp.direction;
-      // post.cu:232-237: D2 = 10 when the matching pixel or its predecessor
-      // leaves the image
-      if (step == 0 || d >= D || xx < 0 || xx >= W || xx - dx < 0 || xx - dx >= W)
-        s.d2[k] = 10.0f;
-      else
-        s.d2[k] = gr[ind2 + d * sp.direction + gshift];
+      const bool dk = FULL || lane + 32 * k < D;
+      st.cost[k] = dk ? src[32 * k] : inf;
+      const bool inside = (unsigned)(xl + 32 * k * s) < xspan;
+      st.d2[k] = (step > 0 && dk && inside) ? grp[32 * k * s] : 10.0f;
     }
   };
   float prev[KPL];
@@ -155,36 +158,39 @@ __device__ __noinline__ void sgm_scan(const SgmGrad& g, const float* __restrict_
 #pragma unroll
         for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
         const bool d1lo = cur.d1 < sp.tau_so, d1hi = cur.d1 > sp.tau_so;
+        // class 0 (both gradients below tau) or 1 (both above) when the step's
+        // D1 allows it and D2 agrees, else class 2
+        const float a2 = d1lo ? p2[0] : p2[1], a1lo = d1lo ? p1lo[0] : p1lo[1],
+                    a1hi = d1lo ? p1hi[0] : p1hi[1];
 #pragma unroll
         for (int k = 0; k < KPL; k++) {
           const int d = lane + 32 * k;
-          // neighbours d-1 and d+1 of the previous step
-          float lo = __shfl_up_sync(0xffffffffu, prev[k], 1);
-          float hi = __shfl_down_sync(0xffffffffu, prev[k], 1);
-          const float lo_w = __shfl_sync(0xffffffffu, prev[k > 0 ? k - 1 : 0], 31);
-          const float hi_w = __shfl_sync(0xffffffffu, prev[k + 1 < KPL ? k + 1 : k], 0);
-          if (lane == 0) lo = lo_w;
-          if (lane == 31) hi = hi_w;
+          // neighbours d-1 and d+1 of the previous step: lane 31 hands lane 0
+          // its value of the previous disparity block, lane 0 hands lane 31
+          // its value of the next one
+          const float up = lane == 31 ? prev[k > 0 ? k - 1 : 0] : prev[k];
+          const float dn = lane == 0 ? prev[k + 1 < KPL ? k + 1 : k] : prev[k];
+          const float lo = __shfl_sync(0xffffffffu, up, (lane + 31) & 31);
+          const float hi = __shfl_sync(0xffffffffu, dn, (lane + 1) & 31);
           const float D2 = cur.d2[k];
-          const int c = (d1lo && D2 < sp.tau_so) ? 0 : (d1hi && D2 > sp.tau_so) ? 1 : 2;
-          float cost = fminf(prev[k], mn + p2[c]);
-          if (d - 1 >= 0) cost = fminf(cost, lo + p1lo[c]);
-          if (d + 1 < D) cost = fminf(cost, hi + p1hi[c]);
-          L[k] = d < D ? cur.cost[k] + cost - mn : inf;
+          const bool ca = d1lo ? D2 < sp.tau_so : (d1hi && D2 > sp.tau_so);
+          float cost = fminf(prev[k], mn + (ca ? a2 : p2[2]));
+          if (d - 1 >= 0) cost = fminf(cost, lo + (ca ? a1lo : p1lo[2]));
+          if (d + 1 < D) cost = fminf(cost, hi + (ca ? a1hi : p1hi[2]));
+          L[k] = (FULL || d < D) ? cur.cost[k] + cost - mn : inf;
         }
       }
-      float* dst = out + pix(step) * D;
+      float* dst = out + (p0 + step * pstep) * D + lane;
 #pragma unroll
       for (int k = 0; k < KPL; k++) {
-        const int d = lane + 32 * k;
-        if (d < D) dst[d] = L[k];
+        if (FULL || lane + 32 * k < D) dst[32 * k] = L[k];
         prev[k] = L[k];
       }
     }
   }
 }
 
-template <int KPL, int PF>
+template <int KPL, int PF, bool FULL>
 __global__ void __launch_bounds__(128) sgm4_kernel(SgmGrad g, const float* __restrict__ in, int H,
                                                    int W, int D, SgmParams sp, SgmOut o) {
   const int warp = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -202,7 +208,7 @@ __global__ void __launch_bounds__(128) sgm4_kernel(SgmGrad g, const float* __res
     dir = 3;
     line = warp - 2 * H - W;
   }
-  if (dir >= 0) sgm_scan<KPL, PF>(g, in, H, W, D, sp, line, o.dir[dir], dir);
+  if (dir >= 0) sgm_scan<KPL, PF, FULL>(g, in, H, W, D, sp, line, o.dir[dir], dir);
 }
 
 // out = base + (((L0 + L1) + L2) + L3) * scale over n elements (base may be
@@ -915,9 +921,15 @@ static void sgm4_launch(const SgmGrad& g, const float* in, int H, int W, int D, 
   const int blocks = (lines * 32 + 127) / 128;
   constexpr int PF0 = KPL <= 2 ? 4 : KPL <= 8 ? 2 : 1;
   const int pf = prefetch > 0 && KPL <= 8 ? prefetch : PF0;
-  if (pf >= 4) sgm4_kernel<KPL, KPL <= 8 ? 4 : 1><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
-  else if (pf >= 2) sgm4_kernel<KPL, KPL <= 8 ? 2 : 1><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
-  else sgm4_kernel<KPL, 1><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+  if (D == 32 * KPL) {  // every lane's disparities exist: no bounds tests on d
+    if (pf >= 4) sgm4_kernel<KPL, KPL <= 8 ? 4 : 1, true><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+    else if (pf >= 2) sgm4_kernel<KPL, KPL <= 8 ? 2 : 1, true><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+    else sgm4_kernel<KPL, 1, true><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+  } else {
+    if (pf >= 4) sgm4_kernel<KPL, KPL <= 8 ? 4 : 1, false><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+    else if (pf >= 2) sgm4_kernel<KPL, KPL <= 8 ? 2 : 1, false><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+    else sgm4_kernel<KPL, 1, false><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+  }
 }
 
 int launch_sgm4(const SgmGrad& g, const float* in, int64_t H, int64_t W, int D, const SgmParams& sp,
