@@ -266,21 +266,58 @@ __device__ __forceinline__ float2 stats_pair(float mn, float den) {
   return mn == kRandMaxF ? make_float2(kRandMaxF, 0.0f) : make_float2(mn, 1.0f / den);
 }
 
-// Both views in one pass: a CTA owns RS_PIX pixels of one row of one
-// matcher.  For each 32-wide disparity chunk it stages, coalesced along d,
-// the block its pixels' left rows cross (view 0: C[y, x, d]) and the block
-// their right diagonals cross (view 1: right pixel x' of row y sees
-// C[y, x' + d, d], the fill C[0,0,0] where x' + d >= W,
-// featextract.cpp:115-152); pass 0 forms both minima, pass 1 both sums of
-// exp(-(c - min)^2 / sigma), each in ascending d.
-constexpr int RS_PIX = 256;
-constexpr size_t kStatsSmem = (size_t)(2 * RS_PIX + 32) * 33 * sizeof(float);
+// view 0: one warp per pixel, the pixel's D costs are contiguous
+__global__ void stats_f32_left_kernel(VolsF vols, int64_t HW, int D, float2* __restrict__ statsf) {
+  const int m = blockIdx.y;
+  const float* __restrict__ vol = vols.v[m];
+  const float inv_sigma = kInvSigmaF32[m];
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const bool vec = (D & 3) == 0 && D <= 512;  // the row as <= 4 float4 per lane, kept in registers
+  for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < HW; p += nw) {
+    const float* r = vol + p * D;
+    float mn = kRandMaxF, den = 0.0f;
+    if (vec) {
+      float4 v[4];
+      const int nq = D >> 2;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int q = lane + 32 * k;
+        v[k] = q < nq ? __ldg(reinterpret_cast<const float4*>(r) + q) : make_float4(kRandMaxF, kRandMaxF, kRandMaxF, kRandMaxF);
+        mn = fminf(mn, fminf(fminf(v[k].x, v[k].y), fminf(v[k].z, v[k].w)));
+      }
+      for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        if (lane + 32 * k < nq) {
+          const float tx = v[k].x - mn, ty = v[k].y - mn, tz = v[k].z - mn, tw = v[k].w - mn;
+          den += (__expf(-(tx * tx) * inv_sigma) + __expf(-(ty * ty) * inv_sigma)) +
+                 (__expf(-(tz * tz) * inv_sigma) + __expf(-(tw * tw) * inv_sigma));
+        }
+      }
+    } else {
+      for (int d = lane; d < D; d += 32) mn = fminf(mn, __ldg(r + d));
+      for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+      for (int d = lane; d < D; d += 32) {
+        const float t = __ldg(r + d) - mn;
+        den += __expf(-(t * t) * inv_sigma);
+      }
+    }
+    for (int o = 16; o; o >>= 1) den += __shfl_xor_sync(0xffffffffu, den, o);
+    if (lane == 0) statsf[(int64_t)(m * 2) * HW + p] = stats_pair(mn, den);
+  }
+}
 
-__global__ void __launch_bounds__(RS_PIX) stats_f32_kernel(VolsF vols, int64_t H, int64_t W, int D,
-                                                           float2* __restrict__ statsf) {
-  extern __shared__ float sm_stats[];
-  float* tl = sm_stats;                // [RS_PIX][33]: C[y, X0 + i, d0 + j]
-  float* tr = sm_stats + RS_PIX * 33;  // [RS_PIX + 32][33]: C[y, X0 + d0 + i, d0 + j]
+// view 1: right pixel x' of row y sees C[y, x' + d, d] (the fill C[0,0,0]
+// where x' + d >= W, featextract.cpp:115-152).  A CTA owns RS_PIX right
+// pixels of one row; for each 32-wide disparity chunk it stages the
+// (RS_PIX + 32) x 32 block of the volume the chunk's diagonals cross
+// (coalesced along d) and each thread walks its diagonal in shared memory.
+constexpr int RS_PIX = 256;
+
+__global__ void __launch_bounds__(RS_PIX) stats_f32_right_kernel(VolsF vols, int64_t H, int64_t W, int D,
+                                                                 float2* __restrict__ statsf) {
+  __shared__ float tile[(RS_PIX + 32) * 33];
   const int m = blockIdx.y;
   const float* __restrict__ vol = vols.v[m];
   const float fill = __ldg(vol);
@@ -290,55 +327,45 @@ __global__ void __launch_bounds__(RS_PIX) stats_f32_kernel(VolsF vols, int64_t H
   const int64_t X0 = (blockIdx.x % nxb) * RS_PIX;
   const int tid = threadIdx.x;
   const int64_t xr = X0 + tid;
-  const float* row = vol + y * W * D;
-  float mnl = kRandMaxF, denl = 0.0f, mnr = kRandMaxF, denr = 0.0f;
+  float mn = kRandMaxF, den = 0.0f;
   for (int pass = 0; pass < 2; pass++) {
     for (int d0 = 0; d0 < D; d0 += 32) {
       __syncthreads();
-      for (int q = tid; q < RS_PIX * 32; q += RS_PIX) {
-        const int i = q >> 5, j = q & 31;
-        const int64_t x = X0 + i;
-        const int d = d0 + j;
-        tl[i * 33 + j] = (x < W && d < D) ? __ldg(row + x * D + d) : kRandMaxF;
-      }
       for (int q = tid; q < (RS_PIX + 32) * 32; q += RS_PIX) {
         const int i = q >> 5, j = q & 31;
         const int64_t x = X0 + d0 + i;
         const int d = d0 + j;
-        tr[i * 33 + j] = (x < W && d < D) ? __ldg(row + x * D + d) : fill;
+        float v = fill;
+        if (x < W && d < D) v = __ldg(vol + (y * W + x) * D + d);
+        tile[i * 33 + j] = v;
       }
       __syncthreads();
       if (xr < W) {
         const int nj = D - d0 < 32 ? D - d0 : 32;
         if (pass == 0) {
-          for (int j = 0; j < nj; j++) {
-            mnl = fminf(mnl, tl[tid * 33 + j]);
-            mnr = fminf(mnr, tr[(tid + j) * 33 + j]);
-          }
+          for (int j = 0; j < nj; j++) mn = fminf(mn, tile[(tid + j) * 33 + j]);
         } else {
           for (int j = 0; j < nj; j++) {
-            const float a = tl[tid * 33 + j] - mnl, b = tr[(tid + j) * 33 + j] - mnr;
-            denl += __expf(-(a * a) * inv_sigma);
-            denr += __expf(-(b * b) * inv_sigma);
+            const float t = tile[(tid + j) * 33 + j] - mn;
+            den += __expf(-(t * t) * inv_sigma);
           }
         }
       }
     }
   }
-  if (xr < W) {
-    const int64_t HW = H * W;
-    statsf[(int64_t)(m * 2) * HW + y * W + xr] = stats_pair(mnl, denl);
-    statsf[(int64_t)(m * 2 + 1) * HW + y * W + xr] = stats_pair(mnr, denr);
-  }
+  if (xr < W) statsf[(int64_t)(m * 2 + 1) * H * W + y * W + xr] = stats_pair(mn, den);
 }
 
 int launch_feature_stats_f32(const float* const* vols, int64_t H, int64_t W, int D, float2* statsf,
                              cudaStream_t st) {
   const VolsF v = {{vols[0], vols[1], vols[2], vols[3]}};
-  const int64_t blocks = H * ((W + RS_PIX - 1) / RS_PIX);
-  CBMV_REQUIRE(blocks < ((int64_t)1 << 31), CBMV_ERANGE, "image too large for the statistics grid");
-  CBMV_CUDA(cudaFuncSetAttribute(stats_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStatsSmem));
-  stats_f32_kernel<<<dim3((unsigned)blocks, 4), RS_PIX, kStatsSmem, st>>>(v, H, W, D, statsf);
+  const int64_t HW = H * W;
+  const int64_t lblocks = (HW + 7) / 8;  // 8 warps per block, one pixel each
+  stats_f32_left_kernel<<<dim3((unsigned)(lblocks < 65535 * 16 ? lblocks : 65535 * 16), 4), 256, 0, st>>>(
+      v, HW, D, statsf);
+  const int64_t rblocks = H * ((W + RS_PIX - 1) / RS_PIX);
+  CBMV_REQUIRE(rblocks < ((int64_t)1 << 31), CBMV_ERANGE, "image too large for the statistics grid");
+  stats_f32_right_kernel<<<dim3((unsigned)rblocks, 4), RS_PIX, 0, st>>>(v, H, W, D, statsf);
   return check_launch("feature_stats_f32");
 }
 
