@@ -26,3 +26,24 @@ def test_oracle_backward_matches_finite_differences(monkeypatch):
         lm, _, _ = mlp_ref.loss_and_grads(vec - e, X, y)
         fd = (lp - lm) / 2e-6
         assert abs(fd - g[j - 60]) < 1e-6 + 1e-4 * abs(fd), (j, fd, g[j - 60])
+
+
+def test_fused_model_close_to_float64_network():
+    """The oracle's model of the fused inference kernel (bf16 inputs,
+    weights and ReLU activations, biases as bf16 high + low parts) stays
+    within bf16 rounding of the float64 network, and the high + low split
+    reproduces each bias to 2^-16 relative."""
+    from oracle import mlp_ref
+    rng = np.random.default_rng(1)
+    sizes = [20, 20, 20, 128 * 20, 128, 128 * 128, 128, 64 * 128, 64, 64, 1]
+    vec = np.concatenate([np.full(20, 1e9), np.zeros(20), np.ones(20),
+                          rng.normal(scale=0.2, size=sum(sizes) - 60)])
+    X = rng.normal(size=(500, 20)).astype(np.float32)
+    z_model = mlp_ref.forward_fused(vec, X)
+    z_exact = mlp_ref.forward(vec, X)["z"]
+    scale = np.abs(z_exact).max()
+    assert np.abs(z_model - z_exact).max() < 0.05 * scale
+    assert np.abs(z_model - z_exact).mean() < 0.01 * scale
+    b = mlp_ref.unpack(vec)["b2"].astype(np.float32)
+    hi, lo = mlp_ref.split_bf16(b)
+    assert np.all(np.abs((hi + lo) - b) <= 2.0 ** -16 * np.abs(b) + 1e-30)
