@@ -244,7 +244,10 @@ int cbmv_cbca(const float* crossL, const float* crossR, const float* in, int64_t
 /* cbca of the same arms and volume in separable form (row sums, then column
  * sums of each support; the fused pipeline's default): [H,W,D] layout only,
  * arms from cbmv_cross with the same L1 (2..9); in != out.  Equal to
- * cbmv_cbca up to float rounding. */
+ * cbmv_cbca up to float rounding.  With L1 <= 6 the supports are first
+ * stored as one 32-bit word per (p,d) in a stream-ordered scratch buffer
+ * (cudaMallocAsync / cudaFreeAsync on `stream`, 4 B per (p,d)); the result
+ * is bit-identical either way. */
 int cbmv_cbca_separable(const float* crossL, const float* crossR, const float* in, int64_t H,
                         int64_t W, int D, int L1, int direction, float* out, void* stream);
 /* np.argmin over d (test.py:408-409), first minimum; disp float32 [H,W]. */
