@@ -172,3 +172,31 @@ def test_separable_cbca_model_close_to_reference_order(oracle_cpu):
         rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-30)
         assert rel.max() <= 1e-5, rel.max()
         assert np.mean(got == ref) > 0.5
+
+
+def test_support_words_reproduce_separable_model(oracle_cpu):
+    """The pipeline's CBCA runs from precomputed support words (row taps,
+    column taps, pixel count, copy flag); restated on the CPU, a pass from
+    the words equals the separable model bit for bit, in both directions,
+    and the words' counts equal the support sizes."""
+    from oracle import glue, post_model
+    from cbmv_b200 import synth
+    L, R, _, _ = synth.make_pair(seed=9, width=70, height=40, ndisp=20, planes=4, dmin=2, dmax=16)
+    imgl, imgr = glue.normalise_images(L, R)
+    o = oracle_cpu.post
+    a, b = o.CUDA_float_array(imgl), o.CUDA_float_array(imgr)
+    lc, rc = o.CUDA_float_array(np.zeros(1)), o.CUDA_float_array(np.zeros(1))
+    o.cross(a, lc, 6, .07)
+    o.cross(b, rc, 6, .07)
+    H, W, D = 40, 70, 20
+    vol = np.random.default_rng(5).random((H, W, D)).astype(np.float32)
+    for direction in (-1, 1):
+        words = post_model.cbca_support_words(lc.a, rc.a, H, W, D, direction)
+        copy = (words >> 31) == 1
+        x = np.arange(W)[None, :, None] + np.arange(D)[None, None, :] * direction
+        assert np.array_equal(copy, np.broadcast_to((x < 0) | (x >= W), copy.shape))
+        cnt = (words >> 22) & 0x7F
+        assert cnt[~copy].min() >= 1 and cnt.max() <= 121
+        got = post_model.cbca_from_words(words, vol)
+        ref = post_model.cbca_separable(lc.a, rc.a, vol, direction, 5)
+        assert np.array_equal(got, ref)
