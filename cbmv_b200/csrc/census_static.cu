@@ -28,7 +28,10 @@ __device__ __align__(256) ulonglong2 g_census_scratch[2 * kStaticCensusMaxPixels
 
 // The array's device address, looked up once per device: in host code the
 // symbol g_census_scratch names a host-side stand-in, not device memory, so
-// it must never be passed to a kernel directly.
+// it must never be passed to a kernel directly.  The cache lives as long as
+// the process: after cudaDeviceReset the module (and the array) is loaded
+// anew at another address, so a process that resets a device must not call
+// cbmv_census_static again.
 std::mutex g_mu;
 void* g_addr[64] = {};
 
@@ -58,19 +61,15 @@ extern "C" int64_t cbmv_census_static_max_pixels(void) { return kStaticCensusMax
 
 extern "C" int cbmv_census_static(const uint8_t* L, const uint8_t* R, int64_t H, int64_t W, int D,
                                   int wsize, void* out, int dtype, int layout, void* stream) {
-  CBMV_REQUIRE(L && R && out, CBMV_EINVAL, "null pointer argument");
-  CBMV_REQUIRE(H > 0 && W > 0 && D > 0 && D <= 65535 && H <= 65535, CBMV_EINVAL,
-               "bad size H=%lld W=%lld D=%d", (long long)H, (long long)W, D);
-  CBMV_REQUIRE(wsize >= 1 && (wsize & 1) && wsize <= 11, CBMV_EINVAL,
-               "window %d must be odd and <= 11", wsize);
-  CBMV_REQUIRE(dtype == CBMV_F32 || dtype == CBMV_F64, CBMV_EINVAL, "bad dtype %d", dtype);
-  CBMV_REQUIRE(layout == CBMV_HWD || layout == CBMV_DHW, CBMV_EINVAL, "bad layout %d", layout);
-  CBMV_REQUIRE(H * W <= kStaticCensusMaxPixels, CBMV_ERANGE,
-               "cbmv_census_static: image of %lld pixels exceeds its fixed scratch of %lld pixels "
+  int rc = check_common(L, R, out, H, W, D, wsize, dtype, layout, 11);  // as cbmv_census
+  if (rc) return rc;
+  // W <= max / H first, so that H * W cannot overflow
+  CBMV_REQUIRE(W <= kStaticCensusMaxPixels / H, CBMV_ERANGE,
+               "cbmv_census_static: image of %lld x %lld pixels exceeds its fixed scratch of %lld pixels "
                "(use cbmv_census)",
-               (long long)(H * W), (long long)kStaticCensusMaxPixels);
+               (long long)W, (long long)H, (long long)kStaticCensusMaxPixels);
   ulonglong2* dl = nullptr;
-  int rc = scratch_address(&dl);
+  rc = scratch_address(&dl);
   if (rc) return rc;
   ulonglong2* dr = dl + kStaticCensusMaxPixels;
   cudaStream_t st = as_stream(stream);

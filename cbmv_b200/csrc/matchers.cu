@@ -341,6 +341,9 @@ __global__ void __launch_bounds__(128) matcher_strip_kernel(
   }
 }
 
+}  // namespace
+
+// Argument checks shared by the matcher entry points (also cbmv_census_static).
 int check_common(const void* a, const void* b, const void* out, int64_t H, int64_t W, int D, int w,
                  int dtype, int layout, int wmax) {
   CBMV_REQUIRE(a && b && out, CBMV_EINVAL, "null pointer argument");
@@ -354,6 +357,8 @@ int check_common(const void* a, const void* b, const void* out, int64_t H, int64
   CBMV_REQUIRE(layout == CBMV_HWD || layout == CBMV_DHW, CBMV_EINVAL, "bad layout %d", layout);
   return CBMV_OK;
 }
+
+namespace {
 
 // Scratch allocation for the stand-alone matcher entry points (the fused
 // pipeline keeps its scratch in its context instead).

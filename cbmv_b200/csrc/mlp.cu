@@ -617,12 +617,15 @@ __device__ __forceinline__ uint32_t relu_bf16x2(float a, float b) {
 }
 
 // ratio and likelihood of cost c (featextract.cpp:333 and :440) in float32
-// against its row statistics st = (min, 1/den); inv_ce = 1 / (c + e)
+// against its row statistics st = (min, 1/den); inv_ce = 1 / (c + e).
+// expf (about 1 ulp over the whole range) rather than the approximate
+// exponential, whose error grows with the argument (large for the census
+// and NCC likelihoods far from the row minimum).
 __device__ __forceinline__ void conf_f32(float c, float inv_ce, float2 st, float e, float inv_sigma,
                                          float* ratio, float* lik) {
   const float t = c - st.x;
   *ratio = st.x == kRandMaxF ? 0.0f : (st.x + e) * inv_ce;
-  *lik = __expf(-(t * t) * inv_sigma) * st.y;  // 1/den = 0 on sentinel rows
+  *lik = expf(-(t * t) * inv_sigma) * st.y;  // 1/den = 0 on sentinel rows
 }
 
 // bf16 high part of x and the bf16 rounding of the rest: x ~ hi + lo
@@ -726,6 +729,37 @@ __device__ __forceinline__ void load_feat_in(const FeatVolsF& fv, const float2* 
   }
 }
 
+// The 20 features of one sample in the reference's column order
+// (test.py:521-595): 0-3 the costs, 4-7 ratio, 8-11 likelihood, 12-19 the
+// same two of the right view warped to the left, all in float32.
+__device__ __forceinline__ void features_f32(const FeatIn& in, float* f) {
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    const float c = in.c[m];
+    const float inv_ce = __fdividef(1.0f, c + kEpsF[m]);
+    f[m] = c;
+    conf_f32(c, inv_ce, in.sl[m], kEpsF[m], kInvSigmaF[m], &f[4 + m], &f[8 + m]);
+    conf_f32(c, inv_ce, in.sr[m], kEpsF[m], kInvSigmaF[m], &f[12 + m], &f[16 + m]);
+  }
+}
+
+// The learned path's float32 features of the samples idx[i] = (y*W + x)*D + d,
+// through the same code as the fused kernel below; out [n, 20].
+__global__ void features_f32_gather_kernel(FeatVolsF fv, const float2* __restrict__ statsf, int64_t H, int64_t W,
+                                           int D, const int64_t* __restrict__ idx, int64_t n, float* __restrict__ out) {
+  const int64_t HW = H * W, N = HW * D;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = idx[i];
+    const int64_t p = t / D;
+    FeatIn in;
+    load_feat_in(fv, statsf, HW, N, t, p, (int)(t - p * D), p % W, in);
+    float f[20];
+    features_f32(in, f);
+#pragma unroll
+    for (int k = 0; k < 20; k++) out[i * 20 + k] = f[k];
+  }
+}
+
 __global__ void __launch_bounds__(kInfThreads, 1)
     features_mlp_kernel(FeatVolsF fv, const float2* __restrict__ statsf, int64_t H, int64_t W, int D,
                         const float* __restrict__ P, float* __restrict__ prob0, int* __restrict__ status) {
@@ -788,14 +822,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     //    columns 0..19 in the reference's order, 20 and 21 the bias inputs, 22..31 zero
     {
       float f[20];
-#pragma unroll
-      for (int m = 0; m < 4; m++) {
-        const float c = in.c[m];
-        const float inv_ce = __fdividef(1.0f, c + kEpsF[m]);
-        f[m] = c;
-        conf_f32(c, inv_ce, in.sl[m], kEpsF[m], kInvSigmaF[m], &f[4 + m], &f[8 + m]);
-        conf_f32(c, inv_ce, in.sr[m], kEpsF[m], kInvSigmaF[m], &f[12 + m], &f[16 + m]);
-      }
+      features_f32(in, f);
       uint32_t u[10];
 #pragma unroll
       for (int k = 0; k < 20; k += 2) {
@@ -915,6 +942,15 @@ __global__ void __launch_bounds__(kInfThreads, 1)
 }
 
 }  // namespace
+
+int launch_features_f32_gather(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
+                               const int64_t* idx, int64_t n, float* out, cudaStream_t st) {
+  FeatVolsF fv = {{vols[0], vols[1], vols[2], vols[3]}};
+  const int64_t blocks = (n + 255) / 256;
+  features_f32_gather_kernel<<<(unsigned)(blocks < 65535 * 16 ? blocks : 65535 * 16), 256, 0, st>>>(
+      fv, statsf, H, W, D, idx, n, out);
+  return check_launch("features_f32_gather");
+}
 
 int launch_features_mlp(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
                         const cbmv_mlp* m, float* prob0, cudaStream_t st, int max_ctas) {

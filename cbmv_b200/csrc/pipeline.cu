@@ -430,6 +430,19 @@ extern "C" int cbmv_ctx_features_at(cbmv_ctx* c, const cbmv_params* p, const uin
   return launch_features_gather(vols, w.stats, H, W, D, idx, n, out, c->stream);
 }
 
+extern "C" int cbmv_ctx_features_f32_at(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L,
+                                        const uint8_t* R, int64_t H, int64_t W, int D, const int64_t* idx,
+                                        int64_t n, float* out) {
+  CBMV_REQUIRE(c && L && R && idx && out, CBMV_EINVAL, "null pointer argument");
+  CBMV_REQUIRE(n > 0, CBMV_EINVAL, "n must be positive");
+  cbmv_params def;
+  p = params_or_default(p, &def);
+  Work w;
+  RC(run_front(c, p, L, R, H, W, D, &w, true));
+  const float* vols[4] = {(float*)w.vol[0], (float*)w.vol[1], (float*)w.vol[2], (float*)w.vol[3]};
+  return launch_features_f32_gather(vols, w.statsf, H, W, D, idx, n, out, c->stream);
+}
+
 // ====================================================================
 // Batches: many pairs of uneven size in one CUDA graph launch.
 // ====================================================================

@@ -7,6 +7,10 @@
 
 namespace cbmv {
 
+// Matcher arguments: non-null pointers, 0 < H <= 65535, 0 < D <= 65535
+// (CBMV_ERANGE beyond), W > 0, window odd and <= wmax, dtype and layout.
+int check_common(const void* a, const void* b, const void* out, int64_t H, int64_t W, int D, int w,
+                 int dtype, int layout, int wmax);
 int launch_census_desc(const uint8_t* img, int64_t H, int64_t W, int w, ulonglong2* desc,
                        cudaStream_t st);
 template <class T>
@@ -42,6 +46,10 @@ int launch_feature_stats_f32(const float* const* vols, int64_t H, int64_t W, int
                              cudaStream_t st);
 int launch_features_mlp(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
                         const cbmv_mlp* m, float* prob0, cudaStream_t st, int max_ctas = 0);
+// The learned path's float32 features of the samples idx[i] = (y*W + x)*D + d
+// (the fused network kernel's own feature code), out [n, 20].
+int launch_features_f32_gather(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
+                               const int64_t* idx, int64_t n, float* out, cudaStream_t st);
 // The 20 features (float32) of the samples idx[i] = (y*W + x)*D + d.
 int launch_features_gather(const double* const* vols, const double* stats, int64_t H, int64_t W,
                            int D, const int64_t* idx, int64_t n, float* out, cudaStream_t st);

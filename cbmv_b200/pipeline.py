@@ -98,8 +98,11 @@ class StereoPipeline:
                   H, W, int(ndisp), out.data_ptr())
         return out
 
-    def features_at(self, left, right, ndisp, idx):
-        """20 float32 features of the samples idx = (y*W + x)*D + d (device tensor [n,20])."""
+    def features_at(self, left, right, ndisp, idx, learned=False):
+        """20 float32 features of the samples idx = (y*W + x)*D + d (device
+        tensor [n,20]): the reference's float64 features rounded to float32
+        (what the random forest reads), or with learned=True the learned
+        path's own float32 features (what its network reads)."""
         import torch
         l, _ = _dev.to_device(left, np.uint8)
         r, _ = _dev.to_device(right, np.uint8)
@@ -108,7 +111,8 @@ class StereoPipeline:
         if ix.numel() and (int(ix.min()) < 0 or int(ix.max()) >= H * W * int(ndisp)):
             raise ValueError("sample index outside the H*W*D volume")
         out = torch.empty((ix.numel(), 20), dtype=torch.float32, device="cuda")
-        _lib.call("cbmv_ctx_features_at", self.ctx, ctypes.byref(self.params), l.data_ptr(), r.data_ptr(),
+        fn = "cbmv_ctx_features_f32_at" if learned else "cbmv_ctx_features_at"
+        _lib.call(fn, self.ctx, ctypes.byref(self.params), l.data_ptr(), r.data_ptr(),
                   H, W, int(ndisp), ix.data_ptr(), ix.numel(), out.data_ptr())
         return out
 

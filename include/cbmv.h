@@ -77,6 +77,8 @@ int cbmv_census(const uint8_t* L, const uint8_t* R, int64_t H, int64_t W, int D,
  * images are rejected with CBMV_ERANGE; use cbmv_census for them.
  *  - The first call on each device looks up the array's device address
  *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *    The address is kept for the life of the process: a process that calls
+ *    cudaDeviceReset on a device must not call this entry point afterwards.
  *  - All calls on a device share the one array: calls whose work overlaps on
  *    the GPU (different streams, or threads without ordering) race and
  *    corrupt each other's results; serialise them on one stream.
@@ -353,6 +355,14 @@ int cbmv_ctx_volumes_f32(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, co
  * (L, R); idx int64 [n], out float32 [n,20], device memory. */
 int cbmv_ctx_features_at(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
                          int64_t H, int64_t W, int D, const int64_t* idx, int64_t n, float* out);
+
+/* The learned path's own 20 features of the samples idx[i] = (y*W + x)*D + d
+ * (the float32 arithmetic the fused network kernel of cbmv_run_mlp forms
+ * them with, from its float32 volumes and row statistics; the reference's
+ * are float64, test.py:521-595): idx int64 [n], out float32 [n,20], device
+ * memory. */
+int cbmv_ctx_features_f32_at(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
+                             int64_t H, int64_t W, int D, const int64_t* idx, int64_t n, float* out);
 
 /* ------------------------------------------------------------------ */
 /* batches of pairs of uneven size                                     */

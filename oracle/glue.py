@@ -152,9 +152,14 @@ def postprocessing_mem(post, imgl, imgr, cost, direction, p=PARAMS):
     return disp_d.get_array()
 
 
-def postprocessing_mem_interp(post, fte, imgl, imgr, cost, direction, p=PARAMS):
+def postprocessing_mem_interp(post, fte, imgl, imgr, cost, direction, p=PARAMS, check_outlier=None):
     """Testing.__postprocessing_mem_interp, test.py:153-338 (adds the
-    right-reference chain and the left-right check)."""
+    right-reference chain and the left-right check).
+
+    check_outlier(outlier) (optional) sees the outlier map before
+    interpolate_mismatch runs; a backend with device-side asserts in that
+    kernel (post.cu:810) needs every mismatch pixel to see a non-mismatch
+    pixel along one of its 16 rays, and the caller checks that there."""
     r_cost = fte.get_right_cost(cost)
     post.InitCUDA()
     cross_array_init = np.zeros((4, imgl.shape[0], imgl.shape[1])).astype(np.float32)
@@ -224,6 +229,8 @@ def postprocessing_mem_interp(post, fte, imgl, imgr, cost, direction, p=PARAMS):
     outlier = np.zeros((r_disp.shape[0], r_disp.shape[1])).astype(np.float32)
     outlier_d = post.CUDA_float_array(outlier)
     post.outlier_detection(disp_d, r_disp_d, outlier_d, out_s)
+    if check_outlier is not None:
+        check_outlier(outlier_d.get_array())
     post.interpolate_mismatch(disp_d, outlier_d, disp_temp)
     post.CUDA_copy_float(disp_temp, disp_d)
     post.interpolate_occlusion(disp_d, outlier_d, disp_temp)
@@ -237,7 +244,7 @@ def postprocessing_mem_interp(post, fte, imgl, imgr, cost, direction, p=PARAMS):
     return disp_d.get_array()
 
 
-def eval_prob(post, fte, prob, iml, imr, d, interpolate=False, p=PARAMS):
+def eval_prob(post, fte, prob, iml, imr, d, interpolate=False, p=PARAMS, check_outlier=None):
     """Testing.eval_prob + do_post, test.py:143-149 and 485-504 (the
     graph-cut branch is out of scope).  Returns the disparity map."""
     h, w = iml.shape
@@ -246,7 +253,7 @@ def eval_prob(post, fte, prob, iml, imr, d, interpolate=False, p=PARAMS):
     fte.get_right_cost(prob)  # computed by the reference, unused by _mem
     imgl, imgr = normalise_images(iml, imr)
     if interpolate:
-        return postprocessing_mem_interp(post, fte, imgl, imgr, prob, -1, p)
+        return postprocessing_mem_interp(post, fte, imgl, imgr, prob, -1, p, check_outlier)
     return postprocessing_mem(post, imgl, imgr, prob, -1, p)
 
 

@@ -69,6 +69,28 @@ def test_pipeline_matches_reference_path(gpu, oracle_cpu, small_pair, forest):
     assert close_x >= 0.999, close_x
 
 
+def test_pipeline_long_arms_matches_reference_path(gpu, oracle_cpu, small_pair, forest):
+    """Cross arms of up to 8 pixels (L1 = 9; the fused post then aggregates
+    from the arms themselves, past the 5-pixel reach of its precomputed
+    support words) against the reference path with the same L1."""
+    from oracle import glue
+    from cbmv_b200 import _lib
+    from cbmv_b200.forest_gpu import GpuForest
+    from cbmv_b200.pipeline import StereoPipeline
+    L, R, _, _ = small_pair
+    D = 24
+    proba = glue.test_model(oracle_cpu.mtc, oracle_cpu.fte,
+                            lambda X: np.stack([oracle_cpu.rf_predict(forest, X),
+                                                1 - oracle_cpu.rf_predict(forest, X)], 1), L, R, D)
+    disp_ref = glue.eval_prob(oracle_cpu.post, oracle_cpu.fte, proba, L, R, D, p=dict(glue.PARAMS, L1=9))
+    prm = _lib.default_params()
+    prm.L1 = 9
+    disp = StereoPipeline(GpuForest(forest), params=prm).run_rf(L, R, D)
+    close = np.mean(np.abs(disp - disp_ref) <= 0.5)
+    print("L1 = 9: disparity within 0.5 px %.5f" % close)
+    assert close >= 0.999, close
+
+
 def test_pipeline_repeatable_and_device_io(gpu, small_pair, forest):
     from cbmv_b200.forest_gpu import GpuForest
     from cbmv_b200.pipeline import StereoPipeline
@@ -108,10 +130,10 @@ def test_learned_path_matches_reference_path(gpu, oracle_cpu, W, H, D):
     a multiple of 32, widths not multiples of 8 or 16) against the
     reference's test path restated over the oracle (test_model with the
     network as its classifier, then eval_prob with the _mem post in the
-    reference's summation order): disparities within 0.5 px on >= 99.5 % of
-    pixels (the device forms the features in float32 and rounds activations
-    to bf16; the network's cost differs from the oracle's float64 model by
-    ~1e-4 on average)."""
+    reference's summation order): disparities within 0.5 px on >= 99.9 % of
+    pixels, the bar for final disparity maps (the device forms the features
+    in float32 and rounds activations to bf16; the network's cost differs
+    from the oracle's float64 model by ~1e-4 on average)."""
     import os
     from oracle import glue, mlp_ref
     from cbmv_b200 import synth
@@ -130,7 +152,7 @@ def test_learned_path_matches_reference_path(gpu, oracle_cpu, W, H, D):
     disp = StereoPipeline().run_mlp(GpuMlp.load(mlp), L, R, D)
     close = np.mean(np.abs(disp - disp_ref) <= 0.5)
     print("learned path %dx%d D=%d: within 0.5 px %.5f" % (W, H, D, close))
-    assert close >= 0.995, close
+    assert close >= 0.999, close
 
 
 def test_run_classified_uses_the_network(gpu, small_pair, forest):

@@ -25,12 +25,12 @@ def _t(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-def _crosses(oracle_cpu, imgl, imgr):
+def _crosses(oracle_cpu, imgl, imgr, L1=6):
     o = oracle_cpu.post
     a, b = o.CUDA_float_array(imgl), o.CUDA_float_array(imgr)
     lc, rc = o.CUDA_float_array(np.zeros(1)), o.CUDA_float_array(np.zeros(1))
-    o.cross(a, lc, 6, .07)
-    o.cross(b, rc, 6, .07)
+    o.cross(a, lc, L1, .07)
+    o.cross(b, rc, L1, .07)
     return lc.a, rc.a
 
 
@@ -147,25 +147,31 @@ def test_dropin_post_module_runs_reference_driver(gpu, oracle_cpu, scene):
     ref = glue.postprocessing_mem(oracle_cpu.post, imgl, imgr, cost, -1)
     got = glue.postprocessing_mem(post, imgl, imgr, cost, -1)
     close = np.mean(np.abs(got - ref) <= 0.5)
-    assert close >= 0.995, close
+    print("drop-in post module vs oracle post, _mem chain: within 0.5 px %.5f" % close)
+    assert close >= 0.999, close
     ref_i = glue.postprocessing_mem_interp(oracle_cpu.post, oracle_cpu.fte, imgl, imgr, cost, -1)
     from cbmv_b200 import libfeatextract as fte
     got_i = glue.postprocessing_mem_interp(post, fte, imgl, imgr, cost, -1)
-    assert np.mean(np.abs(got_i - ref_i) <= 0.5) >= 0.99
+    close_i = np.mean(np.abs(got_i - ref_i) <= 0.5)
+    print("drop-in post module vs oracle post, _interp chain: within 0.5 px %.5f" % close_i)
+    assert close_i >= 0.999, close_i
 
 
 @pytest.mark.parametrize("direction,L1", [(-1, 6), (1, 6), (-1, 9)])
 def test_cbca_separable_matches_model_exactly(gpu, oracle_cpu, scene, direction, L1):
     """cbmv_cbca_separable (the fused pipeline's default CBCA: with L1 <= 6
-    its supports precomputed once and read by the pass, with L1 = 9 taps
-    reaching 8 pixels tested on the arms themselves) against the oracle's
-    float32 model of its summation order: bit-exact; against the
-    reference-order cbca: relative 1e-5."""
+    its supports precomputed once and read by the pass; with L1 = 9 the
+    arms are built with L1 = 9, reach up to 8 pixels and the pass reads the
+    arms themselves) against the oracle's float32 model of its summation
+    order with a halo of L1 - 1: bit-exact; against the reference-order
+    cbca: relative 1e-5."""
     from cbmv_b200 import _lib
     from oracle import post_model
     imgl, imgr, vol, D = scene
-    lc, rc = _crosses(oracle_cpu, imgl, imgr)
+    lc, rc = _crosses(oracle_cpu, imgl, imgr, L1)
     H, W = imgl.shape
+    reach = max(int(np.max(np.abs(lc[0] - np.arange(W)[None, :]))), int(np.max(np.abs(lc[2] - np.arange(H)[:, None]))))
+    assert reach == L1, reach  # the longest arm ends L1 pixels away (its last pixel at L1 - 1)
     tl, tr, ts = _t(lc), _t(rc), _t(vol)
     out = torch.empty_like(ts)
     _lib.call("cbmv_cbca_separable", tl.data_ptr(), tr.data_ptr(), ts.data_ptr(), H, W, D, L1,
@@ -174,6 +180,6 @@ def test_cbca_separable_matches_model_exactly(gpu, oracle_cpu, scene, direction,
     _lib.call("cbmv_cbca", tl.data_ptr(), tr.data_ptr(), ts.data_ptr(), H, W, D, _lib.HWD, direction,
               ref_order.data_ptr(), None)
     got = out.cpu().numpy()
-    assert np.array_equal(got, post_model.cbca_separable(lc, rc, vol, direction, 5))
+    assert np.array_equal(got, post_model.cbca_separable(lc, rc, vol, direction, L1 - 1))
     ro = ref_order.cpu().numpy()
     assert np.max(np.abs(got - ro) / np.maximum(np.abs(ro), 1e-30)) <= 1e-5

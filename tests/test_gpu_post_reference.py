@@ -1,0 +1,275 @@
+"""The oracle's CPU restatement of the post-processing (oracle/oracle.c,
+orc_cross ... orc_interpolate_occlusion) pinned to the reference's own
+cpp/post/post.cu, compiled unmodified for sm_100a into
+oracle/_ref/libcbmv_ref_post.so and run on the GPU through oracle.ref.post
+(the reference's boost.python surface, post.cu:905-933); then the fused
+device post of this package held to that pinned chain.
+
+Kernel by kernel (post.cu line ranges in each test), on the same inputs:
+cross, sgm (one full sgm_w call), cbca in both directions, subpixel,
+median2d and the LR check (outlier_detection, interpolate_mismatch,
+interpolate_occlusion) must equal the oracle bit for bit; mean2d within
+1e-6 relative (the reference build contracts `sum += img * kernel` into
+fused multiply-adds, the oracle multiplies and adds).  The whole `_mem`
+and `_interp` chains of test.py:153-449 (Testing.eval_prob) over the
+reference's post and over the oracle's agree to the same 1e-6; the
+package's fused post (cbmv_run_post, separable and reference-order CBCA)
+agrees with the reference's chain on >= 99.9 % of pixels within 0.5 px.
+
+Inputs the reference's kernels need, checked here before they are called:
+  * W >= H: sgm2 keeps its scan-line state in tmp[d * W + blockIdx.x]
+    (post.cu:213, 219, 260) over a [W, D] buffer (test.py:384), so the
+    horizontal scans (blockIdx.x = row) stay inside it and apart from each
+    other only when no row index reaches W.  Every configuration of this
+    path has W > H.
+  * H*W a multiple of 64: swap_axis_back (post.cu:630-640) reads 64 pixels
+    per block with only the block's first pixel checked against H*W.
+  * every mismatch pixel of the outlier map reaches a non-mismatch pixel on
+    one of its 16 rays (the device assert at post.cu:810).
+Cases: a 128x64 pair with D=24 and a 694x160 band of the 694x554 pair with
+D=128 (the headline width and disparity count); costs are the census
+volume of the pair (the kernel tests) and the random forest's P(class 0)
+of the fused path (the chains).
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+# Testing.__init__ defaults, test.py:46-47
+PI1, PI2, TAU_SO, ALPHA1, Q1, Q2 = 1.3, 10.0, 0.12, 1.4, 2.2, 3.0
+
+# interpolate_mismatch's ray directions (dx, dy), post.cu:759-776
+_RAYS = [(0, 1), (-0.5, 1), (-1, 1), (-1, 0.5), (-1, 0), (-1, -0.5), (-1, -1), (-0.5, -1),
+         (0, -1), (0.5, -1), (1, -1), (1, -0.5), (1, 0), (1, 0.5), (1, 1), (0.5, 1)]
+
+
+def _cround(v):
+    """C round() of float32 values: halves away from zero."""
+    return (np.sign(v) * np.floor(np.abs(v) + np.float32(0.5))).astype(np.int64)
+
+
+def mismatch_rays_ok(outlier):
+    """True when every mismatch pixel (2) of `outlier` meets a pixel that is
+    not a mismatch inside the image along at least one of the 16 rays that
+    interpolate_mismatch walks (float32 steps, C rounding)."""
+    H, W = outlier.shape
+    ys, xs = np.nonzero(outlier == 2)
+    found = np.zeros(len(ys), bool)
+    for dx, dy in _RAYS:
+        xx, yy = xs.astype(np.float32), ys.astype(np.float32)
+        active = np.ones(len(ys), bool)
+        while active.any():
+            xx[active] += np.float32(dx)
+            yy[active] += np.float32(dy)
+            xi, yi = _cround(xx), _cround(yy)
+            inside = (xi >= 0) & (xi < W) & (yi >= 0) & (yi < H)
+            is2 = np.zeros(len(ys), bool)
+            is2[inside] = outlier[yi[inside], xi[inside]] == 2
+            found |= active & inside & ~is2
+            active &= inside & is2
+    return bool(found.all())
+
+
+def _require_ref():
+    from oracle import ref
+    assert ref.post_available(), "oracle/_ref/libcbmv_ref_post.so is not built (make -C oracle ref)"
+    assert ref.cpu_available(), "oracle/_ref/libcbmv_ref_cpu.so is not built (make -C oracle ref)"
+    ref.post.InitCUDA()
+    return ref
+
+
+def _check_shape(H, W):
+    assert W >= H, "the reference's SGM needs W >= H (post.cu:213)"
+    assert (H * W) % 64 == 0, "the reference's swap_axis_back needs H*W % 64 == 0 (post.cu:630)"
+
+
+@pytest.fixture(scope="module", params=["128x64_D24", "694x160_D128"])
+def case(request, oracle_cpu):
+    from oracle import glue
+    from cbmv_b200 import synth
+    if request.param == "128x64_D24":
+        L, R, _, _ = synth.make_pair(seed=5, width=128, height=64, ndisp=24, planes=5, dmin=2, dmax=20)
+        D = 24
+    else:
+        L, R, _, _ = synth.pair_694x554(seed=0)
+        L, R = L[:160].copy(), R[:160].copy()
+        D = 128
+    H, W = L.shape
+    _check_shape(H, W)
+    imgl, imgr = glue.normalise_images(L, R)
+    census = oracle_cpu.mtc.census(L, R, D, 11) / 121.0  # [H,W,D], sentinel entries stay large
+    return dict(L=L, R=R, D=D, H=H, W=W, imgl=imgl, imgr=imgr, hwd=census,
+                dhw=np.ascontiguousarray(np.transpose(census, (2, 0, 1))))
+
+
+def _crosses_ref(ref, c, L1=6):
+    out = []
+    for img in (c["imgl"], c["imgr"]):
+        a = ref.post.CUDA_float_array(img)
+        o = ref.post.CUDA_float_array(np.zeros((4, c["H"], c["W"]), np.float32))
+        ref.post.cross(a, o, L1, .07)
+        out.append(o.get_array())
+    return out
+
+
+@pytest.mark.parametrize("L1", [6, 9])
+def test_cross_equals_reference(gpu, oracle_cpu, case, L1):
+    """cross, post.cu:336-396."""
+    ref = _require_ref()
+    got = _crosses_ref(ref, case, L1)
+    for img, g in zip((case["imgl"], case["imgr"]), got):
+        want = np.empty((4, case["H"], case["W"]), np.float32)
+        oracle_cpu.lib().orc_cross(img.ctypes.data, case["H"], case["W"], L1, np.float32(.07), want.ctypes.data)
+        assert np.array_equal(g, want)
+
+
+@pytest.mark.parametrize("direction", [-1, 1])
+def test_cbca_equals_reference(gpu, oracle_cpu, case, direction):
+    """cbca, post.cu:399-450, on a [D,H,W] volume, both match directions."""
+    ref = _require_ref()
+    lc, rc = _crosses_ref(ref, case)
+    vol = case["dhw"]
+    lcd, rcd = ref.post.CUDA_float_array(lc), ref.post.CUDA_float_array(rc)
+    vd, od = ref.post.CUDA_double_array(vol), ref.post.CUDA_double_array(vol)
+    ref.post.cbca(lcd, rcd, vd, od, direction)
+    got = od.get_array()
+    want = np.empty_like(vol)
+    D, H, W = vol.shape
+    oracle_cpu.lib().orc_cbca(lc.ctypes.data, rc.ctypes.data, vol.ctypes.data, D, H, W, direction,
+                              want.ctypes.data)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("direction", [-1, 1])
+def test_sgm_equals_reference(gpu, oracle_cpu, case, direction):
+    """One full sgm_w call (post.cu:178-333: the four directions one after
+    another into one output, from a zeroed output and state, test.py:379-382)
+    on the [H,W,D] volume."""
+    ref = _require_ref()
+    H, W, D = case["H"], case["W"], case["D"]
+    vol = np.ascontiguousarray(case["hwd"])
+    l, r = ref.post.CUDA_float_array(case["imgl"]), ref.post.CUDA_float_array(case["imgr"])
+    cin = ref.post.CUDA_double_array(vol)
+    cout = ref.post.CUDA_double_array(np.zeros_like(vol))
+    tmp = ref.post.CUDA_double_array(np.zeros((W, D)))
+    ref.post.sgm(l, r, cin, cout, tmp, PI1, PI2, TAU_SO, ALPHA1, Q1, Q2, direction)
+    got = cout.get_array()
+    want = np.zeros((H, W, D))
+    oracle_cpu.lib().orc_sgm(case["imgl"].ctypes.data, case["imgr"].ctypes.data, vol.ctypes.data, H, W, D,
+                             PI1, PI2, TAU_SO, ALPHA1, Q1, Q2, direction, want.ctypes.data)
+    diff = np.abs(got - want)
+    print("sgm %dx%d D=%d direction %d: max |ref - oracle| %.3g, equal %.6f"
+          % (W, H, D, direction, diff.max(), np.mean(got == want)))
+    assert np.array_equal(got, want)
+
+
+def test_subpixel_median_mean2d_equal_reference(gpu, oracle_cpu, case):
+    """subpixel_enchancement (post.cu:453-483), median2d (:486-518),
+    mean2d (:520-566) with Testing.__gaussian (test.py:108-118)."""
+    from oracle import glue
+    ref = _require_ref()
+    H, W, D = case["H"], case["W"], case["D"]
+    vol = case["dhw"]
+    d0 = np.argmin(vol, axis=0).astype(np.float32)
+    P = ref.post
+    dd, cd, od = P.CUDA_float_array(d0), P.CUDA_double_array(vol), P.CUDA_float_array(d0)
+    P.subpixel_enchancement(dd, cd, od)
+    sub = od.get_array()
+    want = np.empty((H, W), np.float32)
+    oracle_cpu.lib().orc_subpixel(d0.ctypes.data, vol.ctypes.data, H, W, D, want.ctypes.data)
+    assert np.array_equal(sub, want)
+    assert np.mean(sub != d0) > 0.1  # the refinement moved most pixels
+    sd, md = P.CUDA_float_array(sub), P.CUDA_float_array(sub)
+    P.median2d(sd, md, 3)
+    med = md.get_array()
+    want_m = np.empty((H, W), np.float32)
+    oracle_cpu.lib().orc_median2d(sub.ctypes.data, H, W, 3, want_m.ctypes.data)
+    assert np.array_equal(med, want_m)
+    k = glue.gaussian(2.2)
+    ind, outd = P.CUDA_float_array(med), P.CUDA_float_array(med)
+    P.mean2d(ind, outd, k, 1.3)
+    mean = outd.get_array()
+    want_g = np.empty((H, W), np.float32)
+    oracle_cpu.lib().orc_mean2d(med.ctypes.data, H, W, k.ctypes.data, k.shape[0], np.float32(1.3),
+                                want_g.ctypes.data)
+    np.testing.assert_allclose(mean, want_g, rtol=1e-6, atol=1e-6)
+
+
+def test_lr_check_equals_reference(gpu, oracle_cpu, case):
+    """outlier_detection (post.cu:717-754), interpolate_mismatch (:757-827),
+    interpolate_occlusion (:829-869) on the left disparity and the right
+    view's disparity (argmin of get_right_cost of the volume, test.py:296)."""
+    ref = _require_ref()
+    H, W, D = case["H"], case["W"], case["D"]
+    d0 = np.argmin(case["hwd"], axis=2).astype(np.float32)
+    right = oracle_cpu.fte.get_right_cost(case["hwd"])
+    d1 = np.argmin(right, axis=2).astype(np.float32)
+    P = ref.post
+    a, b, o = P.CUDA_float_array(d0), P.CUDA_float_array(d1), P.CUDA_float_array(np.zeros((H, W), np.float32))
+    P.outlier_detection(a, b, o, D)
+    outl = o.get_array()
+    want = np.empty((H, W), np.float32)
+    oracle_cpu.lib().orc_outlier_detection(d0.ctypes.data, d1.ctypes.data, H, W, D, want.ctypes.data)
+    assert np.array_equal(outl, want)
+    counts = [int(np.sum(outl == v)) for v in (0, 1, 2)]
+    print("outliers %dx%d: match %d occlusion %d mismatch %d" % (W, H, *counts))
+    assert all(n > 0 for n in counts)
+    assert mismatch_rays_ok(outl)
+    for name, fn in (("interpolate_mismatch", "orc_interpolate_mismatch"),
+                     ("interpolate_occlusion", "orc_interpolate_occlusion")):
+        od = P.CUDA_float_array(d0)
+        getattr(P, name)(P.CUDA_float_array(d0), P.CUDA_float_array(outl), od)
+        got = od.get_array()
+        w = np.empty((H, W), np.float32)
+        getattr(oracle_cpu.lib(), fn)(d0.ctypes.data, outl.ctypes.data, H, W, w.ctypes.data)
+        assert np.array_equal(got, w), name
+
+
+@pytest.fixture(scope="module")
+def forest_cost(case):
+    """P(class 0) of the committed forest on the case's pair, from the fused
+    path (its leaves and probabilities are sklearn's, see test_gpu_forest)."""
+    import os
+    from cbmv_b200.forest import FlatForest
+    from cbmv_b200.forest_gpu import GpuForest
+    from cbmv_b200.pipeline import StereoPipeline
+    path = os.path.join(os.path.dirname(__file__), "golden", "forest_694x554.npz")
+    pipe = StereoPipeline(GpuForest(FlatForest.load(path)))
+    H, W, D = case["H"], case["W"], case["D"]
+    prob = torch.empty((H, W, D), device="cuda")
+    pipe.run_rf(case["L"], case["R"], D, prob_out=prob)
+    p0 = prob.cpu().numpy().astype(np.float64).reshape(-1)
+    return np.stack([p0, 1.0 - p0], 1)
+
+
+def _check_rays(outlier):
+    assert mismatch_rays_ok(outlier), "a mismatch pixel with no valid neighbour on any ray"
+
+
+@pytest.mark.parametrize("interpolate", [False, True])
+def test_post_chains_equal_reference(gpu, oracle_cpu, case, forest_cost, interpolate):
+    """Testing.eval_prob (test.py:143-149) with the _mem chain (test.py:341-449)
+    or the _interp chain (test.py:153-338): the reference's post.cu vs the
+    oracle, then the package's fused device post vs the reference."""
+    from oracle import glue
+    from cbmv_b200 import _lib
+    from cbmv_b200.pipeline import StereoPipeline
+    ref = _require_ref()
+    L, R, D = case["L"], case["R"], case["D"]
+    d_ref = glue.eval_prob(ref.post, ref.fte, forest_cost, L, R, D, interpolate=interpolate,
+                           check_outlier=_check_rays)
+    d_orc = glue.eval_prob(oracle_cpu.post, oracle_cpu.fte, forest_cost, L, R, D, interpolate=interpolate)
+    np.testing.assert_allclose(d_orc, d_ref, rtol=1e-6, atol=1e-6)
+    if interpolate:
+        return  # the fused device chain with the LR check: test_gpu_pipeline
+    cost = forest_cost[:, 0].astype(np.float32).reshape(case["H"], case["W"], D)
+    for exact in (0, 1):
+        prm = _lib.default_params()
+        prm.exact_cbca = exact
+        disp = StereoPipeline(params=prm).run_post(L, R, cost)
+        close = float(np.mean(np.abs(disp - d_ref) <= 0.5))
+        print("fused post (exact_cbca=%d) vs reference post.cu %dx%d D=%d: within 0.5 px %.5f"
+              % (exact, case["W"], case["H"], D, close))
+        assert close >= 0.999, close

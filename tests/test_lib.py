@@ -45,6 +45,30 @@ def test_host_side_argument_checks():
     assert abs(p.pi1 - 1.3) < 1e-6 and abs(p.blur_t - 1.3) < 1e-6
 
 
+def test_census_entry_points_reject_alike():
+    """cbmv_census_static validates its arguments with cbmv_census's own
+    checks, so both return the same code for the same bad input; only its
+    pixel limit is its own (checked without forming an overflowing H*W)."""
+    from cbmv_b200 import _lib
+    L = _lib.lib()
+    buf = ctypes.c_void_p(16)  # never dereferenced
+    bad = [(None, buf, 10, 10, 4, 11, 0, 0),       # null image
+           (buf, buf, 10, 10, 4, 4, 0, 0),         # even window
+           (buf, buf, 10, 10, 4, 13, 0, 0),        # window beyond 11
+           (buf, buf, 10, 10, 0, 11, 0, 0),        # D = 0
+           (buf, buf, 70000, 10, 4, 11, 0, 0),     # H beyond 65535
+           (buf, buf, 10, 10, 70000, 11, 0, 0),    # D beyond 65535
+           (buf, buf, 10, 10, 4, 11, 5, 0),        # dtype
+           (buf, buf, 10, 10, 4, 11, 0, 9)]        # layout
+    for a, b, H, W, D, w, dt, lay in bad:
+        r1 = L.cbmv_census(a, b, H, W, D, w, buf, dt, lay, None)
+        r2 = L.cbmv_census_static(a, b, H, W, D, w, buf, dt, lay, None)
+        assert r1 == r2 != 0, (H, W, D, w, dt, lay, r1, r2)
+    mx = L.cbmv_census_static_max_pixels()
+    assert L.cbmv_census_static(buf, buf, 1024, mx // 1024 + 1, 4, 11, buf, 0, 0, None) == -4
+    assert L.cbmv_census_static(buf, buf, 65535, 1 << 50, 4, 11, buf, 0, 0, None) == -4  # H*W > 2^63
+
+
 def test_argument_checks_of_the_fused_entry_points():
     """The batch, post-only, separable CBCA and parameter checks reject bad
     arguments on the host, before any device work."""
