@@ -36,11 +36,15 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FOREST = os.path.join(ROOT, "tests", "golden", "forest_694x554.npz")
-MLP = os.path.join(ROOT, "tests", "golden", "mlp_694x554.npz")
+MLP = os.path.join(ROOT, "tests", "golden", "mlp_gelu_694x554.npz")       # the GELU network of record
+MLP_RELU = os.path.join(ROOT, "tests", "golden", "mlp_694x554.npz")      # the ReLU variant
 W0, H0, D0 = 694, 554, 128
 UNITS = W0 * H0 * D0
 METRIC = "pixel·disparities/s end-to-end at 694×554, D=128; MLP vs RF at matched bad-2.0"
 BYTES_PER_UNIT_FUSED = 4.0  # algorithmic HBM bytes of matchers+features+classifier per (p,d)
+BYTES_PER_UNIT_PATH = 80.0  # algorithmic HBM bytes per (p,d) of the whole path with the _mem post
+BYTES_PER_UNIT_INTERP = 156.0  # the same with the _interp post (the right view's chain added)
+REF_BUDGET_S = 100  # the reference arm's timed whole-pair steps stop after this many seconds
 # dense flops of the 20-128-128-64-1 network per (p,d): 2*(20*128 + 128*128 + 128*64 + 64)
 FLOPS_PER_UNIT_MLP = 2.0 * (20 * 128 + 128 * 128 + 128 * 64 + 64)
 # MMA work the fused kernel issues per (pixel, d): layer 1 K = 32 (20 inputs + 2 bias ones + padding),
@@ -189,9 +193,43 @@ def _time_e2e(run_host, a, ws, flush, st):
     return reduce_max(tot / a.steps, ws)
 
 
+def clk_max_mhz():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p)).get("sm_max_mhz", 1965.0))
+    return 1965.0
+
+
+def forest_visits_per_unit(pipe, gf, flat, l, r, n=65536):
+    """Mean comparisons per (pixel, d) over all trees: the depth of the leaf
+    each tree's walk reaches, for n sampled (p,d) of the pair (the forest
+    path's own features and leaves)."""
+    import torch
+    H, W = l.shape
+    rng = np.random.default_rng(0)
+    idx = torch.from_numpy(rng.integers(0, H * W * D0, n, dtype=np.int64)).cuda()
+    X = pipe.features_at(l, r, D0, idx)
+    leaves = gf.apply(X).cpu().numpy()  # sklearn node ids [n, T]
+    depth = flat.node_depths()
+    return float(depth[flat.roots[None, :].astype(np.int64) + leaves].sum(axis=1).mean())
+
+
+def launches_per_pair(prm):
+    """Kernel launches of one cbmv_run_mlp / cbmv_run_rf call (pipeline.cu)
+    for parameters prm: 8 per-pixel terms (census descriptors, NCC sums,
+    ZSAD means, Sobel; both images), 4 cost volumes, 2 row statistics,
+    1 features+classifier; post: 4 image normalisation, 2 cross, 1 SGM
+    neighbour differences, 2 per SGM iteration, 1 CBCA support build and 1
+    per CBCA pass, WTA+subpixel, median per iteration, mean2d."""
+    post = 4 + 2 + (1 + 2 * prm.sgm_i if prm.sgm_i else 0) + (1 + prm.cbca_i2 if prm.cbca_i2 else 0) \
+        + (1 + prm.cbca_i1 if prm.cbca_i1 else 0) + 1 + prm.median_i + 1
+    return 8 + 4 + 2 + 1 + post
+
+
 def run_cbmv(a, ws, rank, local):
     import torch
     from cbmv_b200 import evaluate, synth
+    from cbmv_b200._lib import default_params as _default_params
     from cbmv_b200.forest import FlatForest
     from cbmv_b200.forest_gpu import GpuForest
     from cbmv_b200.mlp import GpuMlp
@@ -227,13 +265,36 @@ def run_cbmv(a, ws, rank, local):
         paths["mlp"] = (lambda: pipe.run_mlp(net, l, r, D0, disp_out=disp),
                         lambda: pipe.run_mlp(net, Lh, Rh, D0))
     res = {}
+    relu = None
     with Clocks(local) as clk:
         for name, (run_dev, run_host) in paths.items():
             ms, stage = _time_path(run_dev, a, ws, flush, st, pipe)
             d = disp.cpu().numpy()
             res[name] = {"ms": ms, "stage_ms": stage, "bad2_nonocc": evaluate.bad_x(d, gt, nonocc)}
+        # the same architecture with ReLU hidden layers, a labelled variant
+        if a.classifier in ("both", "mlp") and os.path.exists(a.mlp_relu):
+            net_r = GpuMlp.load(a.mlp_relu)
+            ms_r, stage_r = _time_path(lambda: pipe.run_mlp(net_r, l, r, D0, disp_out=disp), a, ws, flush, st, pipe)
+            relu = {"activation": net_r.activation, "ms_per_step": ms_r, "value": units * ws / (ms_r / 1e3),
+                    "stage_ms": stage_r, "bad2_nonocc": evaluate.bad_x(disp.cpu().numpy(), gt, nonocc),
+                    "classify_tflops": FLOPS_PER_UNIT_MLP * units / (stage_r["classify"] / 1e3) / 1e12}
+            net_r.close()
     for name, (_, run_host) in paths.items():
         res[name]["e2e_ms"] = _time_e2e(run_host, a, ws, flush, st)
+    # the _interp post (test.py:153-338: the right view's chain, the left-right
+    # check and its fills) as a separate variant of the learned path
+    interp = None
+    if net is not None and a.classifier in ("both", "mlp"):
+        pipe_i = StereoPipeline(gf, params=_default_params(interpolate=1))
+        ms_i, stage_i = _time_path(lambda: pipe_i.run_mlp(net, l, r, D0, disp_out=disp), a, ws, flush, st, pipe_i)
+        hbm_i, _ = peaks()
+        interp = {"ms_per_step": ms_i, "value": units * ws / (ms_i / 1e3), "stage_ms": stage_i,
+                  "bad2_nonocc": evaluate.bad_x(disp.cpu().numpy(), gt, nonocc),
+                  "whole_path": {"bytes_per_unit": BYTES_PER_UNIT_INTERP,
+                                 "achieved": BYTES_PER_UNIT_INTERP * units / (ms_i / 1e3) / 1e9,
+                                 "frac": BYTES_PER_UNIT_INTERP * units / (ms_i / 1e3) / 1e9 / hbm_i,
+                                 "unit": "GB/s"}}
+        pipe_i.close()
     if net is not None and net.status() != 0:
         raise RuntimeError("a tensor-core wait of the MLP kernel timed out")
 
@@ -251,10 +312,7 @@ def run_cbmv(a, ws, rank, local):
         head = a.classifier
     h = res[head]
 
-    # kernel launches per step (pipeline.cu): 8 per-pixel terms, 4 cost volumes,
-    # 4 feature statistics, 1 features+classifier, post: 4 normalisation, 2 cross,
-    # 4 x sgm_i SGM directions, cbca_i2 CBCA, WTA+subpixel, median, mean2d
-    launches = 8 + 4 + 4 + 1 + 4 + 2 + 4 * 2 + 4 + 3
+    launches = launches_per_pair(pipe.params)
 
     hbm, hbm_kind = peaks()
     tc, tc_kind = tensor_peak()
@@ -263,12 +321,23 @@ def run_cbmv(a, ws, rank, local):
     if os.path.exists(tp):
         traffic = json.load(open(tp))
     if "rf" in res:
-        rf_achieved = BYTES_PER_UNIT_FUSED * units / (res["rf"]["stage_ms"]["classify"] / 1e3) / 1e9
+        visits = forest_visits_per_unit(pipe, gf, flat, l, r)
+        t_rf = res["rf"]["stage_ms"]["classify"] / 1e3
+        rf_achieved = visits * units / t_rf
+        sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = clk_max_mhz()
+        # L1 sector bound of the walk: each lane's next 32-byte node block (two tree
+        # levels) is a different sector; an SM's L1 returns 4 sectors (128 B) per clock
+        rf_peak = sm_count * 4 * 2 * mhz * 1e6
         res["rf"]["roofline"] = {
-            "bound": "hbm", "kernel": "features_rf_kernel", "achieved": rf_achieved, "peak": hbm,
-            "unit": "GB/s", "frac": rf_achieved / hbm, "traffic": traffic.get("features_rf_kernel"),
-            "peak_kind": hbm_kind, "bytes_per_unit": BYTES_PER_UNIT_FUSED,
-            "note": "the forest walk is bound by dependent node-visit gathers, not HBM"}
+            "bound": "l1", "kernel": "features_rf_tiled", "achieved": rf_achieved, "peak": rf_peak,
+            "unit": "node-visits/s", "frac": rf_achieved / rf_peak,
+            "traffic": traffic.get("features_rf_kernel"), "peak_kind": "derived (L1 sectors/clock)",
+            "visits_per_unit": visits,
+            "note": "node visits = comparisons per (pixel,d) summed over the 50 trees (mean over 65,536 "
+                    "sampled (p,d) of this pair); peak = SMs x 4 sectors/clock x 2 levels per 32-byte "
+                    "block x max SM clock; HBM: %.0f GB/s of %.0f for 4 B/(p,d)"
+                    % (BYTES_PER_UNIT_FUSED * units / t_rf / 1e9, hbm)}
     if "mlp" in res:
         mlp_tflops = FLOPS_PER_UNIT_MLP * units / (res["mlp"]["stage_ms"]["classify"] / 1e3) / 1e12
         t_cls = res["mlp"]["stage_ms"]["classify"]
@@ -287,7 +356,8 @@ def run_cbmv(a, ws, rank, local):
     roof = res[head]["roofline"]
 
     classifier = {"rf": "random_forest (50 trees, depth<=20)",
-                  "mlp": "bf16 MLP 20-128-128-64-1 on tcgen05 (RF as judge)"}[head]
+                  "mlp": "bf16 MLP 20-128-128-64-1 (%s) on tcgen05 (RF as judge)"
+                         % (net.activation.upper() if net is not None else "")}[head]
     line = {
         "metric": METRIC, "value": units * ws / (h["ms"] / 1e3), "unit": "pixel·disparities/s",
         "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": h["ms"],
@@ -307,11 +377,20 @@ def run_cbmv(a, ws, rank, local):
                 "ms_per_step": h["e2e_ms"], "h2d_bytes_per_step": 2 * L.size,
                 "d2h_bytes_per_step": 4 * L.size},
         "roofline": roof,
+        "whole_path": {"bound": "hbm", "bytes_per_unit": BYTES_PER_UNIT_PATH,
+                       "achieved": BYTES_PER_UNIT_PATH * units / (h["ms"] / 1e3) / 1e9, "peak": hbm,
+                       "unit": "GB/s", "frac": BYTES_PER_UNIT_PATH * units / (h["ms"] / 1e3) / 1e9 / hbm,
+                       "peak_kind": hbm_kind,
+                       "note": "compulsory HBM bytes of an ideal fused path with the _mem post (4 B cost + "
+                               "SGM 2 x 20 B + CBCA 4 x 8 B + WTA 4 B per (p,d)) over the device step time; "
+                               "the learned classifier's own bound is the tensor roofline above"},
         "classifiers": {k: {"value": units * ws / (v["ms"] / 1e3), "ms_per_step": v["ms"],
                             "e2e_ms": v["e2e_ms"], "stage_ms": v["stage_ms"],
                             "bad2_nonocc": v["bad2_nonocc"], "roofline": v["roofline"]}
                         for k, v in res.items()},
         "matched_bad2": matched,
+        "interp_variant": interp,
+        "relu_variant": relu,
         "clocks": clk.summary(),
     }
     if rank == 0 and ws == 1 and not a.no_cpu_baseline and have_forest:
@@ -352,7 +431,17 @@ def cpu_baseline(flat, L, R, a):
 
 
 def run_reference(a, ws, rank, local):
-    """--impl reference: the reference's implementation of the path."""
+    """--impl reference: the reference's implementation of the path on one
+    whole 694x554 D=128 pair per step: its compiled matchers and feature
+    assembly (oracle/_ref, all host cores) batched as test.py:597-626 does
+    (floor(100000/694) = 144 rows per batch, np.append of every batch's
+    probabilities), scikit-learn's predict_proba on the same forest, then
+    Testing.eval_prob with the _mem chain on that classifier's own P(class 0)
+    through the reference's post.cu on the GPU (as shipped: its host copies
+    and host argmin included).  Each step is ~30 s of host work, so the timed
+    steps stop once REF_BUDGET_S has passed (at least one; the line states
+    how many ran); the warm-up is one 16-row band, which pages in the
+    libraries and starts the thread pools."""
     if rank != 0:
         return None
     import torch
@@ -368,42 +457,47 @@ def run_reference(a, ws, rank, local):
         return {"impl": "reference", "unavailable": "forest fixture missing (tests/golden/make_forest.py)"}
     flat = FlatForest.load(a.forest)
     skl = skforest.to_sklearn(flat, n_jobs=cores)
+    ref.set_threads(cores)
     L, R, gt, nonocc = synth.pair_694x554(seed=0)
-    post_kind = "reference post.cu on the GPU (as shipped)" if ref.post_available() and \
-        torch.cuda.is_available() else "oracle CPU restatement of post.cu"
-    post_mod = ref.post if "post.cu" in post_kind else cpu.post
-    rows = a.cpu_rows
-    rng = np.random.default_rng(0)
-    prob_full = rng.random((H0, W0, D0, 2))  # the post stage's input: a [H,W,D] cost volume
-    prob_full = prob_full.reshape(-1, 2)
-    times = []
-    for k in range(a.warmup + a.steps):
-        t_cpu = _cpu_stage_band(ref, skl, L, R, rows, cores)
+    on_gpu = ref.post_available() and torch.cuda.is_available()
+    post_kind = "reference post.cu on the GPU (as shipped)" if on_gpu else "oracle CPU restatement of post.cu"
+    post_mod = ref.post if on_gpu else cpu.post
+    glue.test_model(ref.mtc, ref.fte, skl.predict_proba, L[:26], R[:26], D0, rows=16)  # warm-up
+    times, disp = [], None
+    t_start = time.perf_counter()
+    for k in range(max(1, a.steps)):
         t0 = time.perf_counter()
-        glue.eval_prob(post_mod, ref.fte, prob_full, L, R, D0)
-        if post_mod is ref.post:
+        proba = glue.test_model(ref.mtc, ref.fte, skl.predict_proba, L, R, D0)
+        t1 = time.perf_counter()
+        disp = glue.eval_prob(post_mod, ref.fte, proba, L, R, D0)
+        if on_gpu:
             ref.post.sync()
-        t_post = time.perf_counter() - t0
-        if k >= a.warmup:
-            times.append((t_cpu, t_post))
+        t2 = time.perf_counter()
+        times.append((t1 - t0, t2 - t1))
+        if time.perf_counter() - t_start > REF_BUDGET_S:
+            break
+    from cbmv_b200 import evaluate
     t_cpu = float(np.mean([t for t, _ in times]))
     t_post = float(np.mean([t for _, t in times]))
-    t_pair = t_cpu * (H0 / rows) + t_post  # a whole pair: CPU stages scaled from the band
+    t_pair = t_cpu + t_post
     value = UNITS / t_pair
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "pixel·disparities/s",
-        "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_pair * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded 694x554 pair)",
+        "n_gpus": ws, "steps": len(times), "steps_requested": a.steps, "warmup": 1,
+        "ms_per_step": t_pair * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded 694x554 pair, seed 0)",
         "config": {"workload": "694x554 D=128 test path: 4 matchers, 20 features, RF 50 trees "
                                "depth<=20, MC-CNN _mem post", "width": W0, "height": H0, "ndisp": D0},
+        "step_cap": "timed whole-pair steps stop after %d s (at least one): %d of %d ran"
+                    % (REF_BUDGET_S, len(times), a.steps),
+        "bad2_nonocc": evaluate.bad_x(disp, gt, nonocc),
+        "stage_s": {"matchers_features_rf": t_cpu, "post": t_post},
         "cpu_baseline": {"value": value, "unit": "pixel·disparities/s", "cores": cores,
                          "kind": "reference",
-                         "sample": "per step: reference CPU stages (matchers, feature assembly, sklearn "
-                                   "predict_proba) on the first %d rows, scaled to the %d rows of the "
-                                   "pair (%.2f s -> %.2f s), plus the full-pair post (%s, %.2f s incl. "
-                                   "its host copies and host argmin)"
-                                   % (rows, H0, t_cpu, t_cpu * H0 / rows, post_kind, t_post)},
+                         "sample": "per step one whole 694x554 D=128 pair: reference matchers + feature "
+                                   "assembly in 4 row batches of 144 (test.py:597-626) + sklearn "
+                                   "predict_proba (n_jobs=%d) %.2f s, then %s on that P(class 0) %.2f s"
+                                   % (cores, t_cpu, post_kind, t_post)},
         "e2e": {"value": value, "unit": "pixel·disparities/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -419,20 +513,29 @@ def run_batch(a, ws, rank, local):
     D in {64,128,192,256}, seeds 4000..4063) through the learned path as one
     CUDA graph launch per step, launch shape from the autotuner; per-pair
     latency p50/p99 beside the aggregate throughput, and the same pairs run
-    one after another (one pipeline call each) for comparison."""
+    one after another (one pipeline call each) for comparison.  With N
+    ranks the 64 pairs are split longest-first over the GPUs
+    (cbmv_b200.shard.lpt_assign; strong scaling: the total work is fixed),
+    each GPU runs its share as its own graph, and rank 0 gathers every
+    pair's disparity map, latency and bad-2.0 (the only data-path
+    collectives)."""
     import multiprocessing as mp
     import torch
     from cbmv_b200 import _lib, evaluate, synth
     from cbmv_b200.batch import StereoBatch, tune_batch
     from cbmv_b200.mlp import GpuMlp
     from cbmv_b200.pipeline import StereoPipeline
-    specs = synth.batch_specs(a.batch_pairs, 4000 + 1000 * rank)
+    from cbmv_b200 import shard
+    all_specs = synth.batch_specs(a.batch_pairs, 4000)
+    all_shapes = [(sp["height"], sp["width"], sp["ndisp"]) for sp in all_specs]
+    assign = shard.lpt_assign(shard.pair_work(all_shapes), ws)  # this rank runs assign[rank]
+    specs = [all_specs[i] for i in assign[rank]]
     with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
         pairs = pool.map(_make_pair_spec, specs)
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     shapes = [(sp["height"], sp["width"], sp["ndisp"]) for sp in specs]
-    units = int(sum(h * w * d for h, w, d in shapes))
+    units = int(sum(h * w * d for h, w, d in all_shapes))
     lefts = [torch.from_numpy(p[0]).to(dev) for p in pairs]
     rights = [torch.from_numpy(p[1]).to(dev) for p in pairs]
     net = GpuMlp.load(a.mlp)
@@ -459,10 +562,10 @@ def run_batch(a, ws, rank, local):
             pair_ms.append(t["pair_ms"])
             done_ms.append(t["done_ms"])
         barrier(ws)
-    ms = reduce_max(float(np.mean(spans)), ws)
+    ms = shard.max_over_ranks(float(np.mean(spans)), device=dev)
     disp = [t.cpu().numpy() for t in b.disp]
-    bad = float(np.mean([evaluate.bad_x(d, p[2], p[3]) for d, p in zip(disp, pairs)]))
-    pair_ms, done_ms = np.concatenate(pair_ms), np.concatenate(done_ms)
+    bad_local = [evaluate.bad_x(d, p[2], p[3]) for d, p in zip(disp, pairs)]
+    pair_ms, done_ms = np.stack(pair_ms), np.stack(done_ms)  # [steps, this rank's pairs]
     # the same pairs one pipeline call each, back to back on one stream
     pipe = StereoPipeline()
     outs = [torch.empty(l.shape, dtype=torch.float32, device=dev) for l in lefts]
@@ -475,24 +578,39 @@ def run_batch(a, ws, rank, local):
         pipe.run_mlp(net, lefts[i], rights[i], shapes[i][2], disp_out=outs[i])
     e1.record(st)
     e1.synchronize()
-    seq_ms = e0.elapsed_time(e1)
+    seq_ms = shard.max_over_ranks(e0.elapsed_time(e1), device=dev)
     same = all(np.array_equal(o.cpu().numpy(), d) for o, d in zip(outs, disp))
+    same = shard.max_over_ranks(0.0 if same else 1.0, device=dev) == 0.0
+    # every pair's map, latency and error on rank 0 (the only collectives of the data path)
+    maps = shard.gather_maps(list(b.disp), assign, all_shapes, device=dev)
+    n = len(all_shapes)
+    lat = {k: shard.gather_values(v.mean(axis=0), assign, n, device=dev)
+           for k, v in (("pair", pair_ms), ("done", done_ms))}
+    bad = shard.gather_values(bad_local, assign, n, device=dev)
+    if rank != 0:
+        return None
+    assert all(m is not None and tuple(m.shape) == (h, w) for m, (h, w, _) in zip(maps, all_shapes))
     return {
-        "metric": "pixel·disparities/s, %d uneven pairs in one CUDA graph launch (learned classifier)" % len(shapes),
-        "value": units * ws / (ms / 1e3), "unit": "pixel·disparities/s", "n_gpus": ws, "steps": a.steps,
-        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "metric": "pixel·disparities/s, %d uneven pairs in one CUDA graph launch per GPU (learned classifier)" % n,
+        "value": units / (ms / 1e3), "unit": "pixel·disparities/s", "n_gpus": ws, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong" if ws > 1 else "weak", "vs_baseline": None,
         "dtype": "bf16/f32", "data": "synthetic (seeded uneven pairs, seeds 4000+)",
-        "config": {"workload": "%d pairs W~U[320,1500] H~U[240,1000] D in {64,128,192,256}" % len(shapes),
+        "config": {"workload": "%d pairs W~U[320,1500] H~U[240,1000] D in {64,128,192,256}" % n,
                    "units": units,
                    "autotune": {k: tune.get(k) for k in ("streams", "mlp_ctas", "cbca_rows", "sgm_prefetch", "ms",
                                                          "tried")},
-                   "autotune_seconds": t_tune, "parallelism": "pairs over concurrent contexts in one graph"},
-        "latency_ms": {"pair_p50": float(np.percentile(pair_ms, 50)), "pair_p99": float(np.percentile(pair_ms, 99)),
-                       "done_p50": float(np.percentile(done_ms, 50)), "done_p99": float(np.percentile(done_ms, 99)),
-                       "note": "pair: a pair's first to last kernel; done: graph start to the pair's end"},
+                   "autotune_seconds": t_tune,
+                   "parallelism": "pairs split longest-first over %d GPU(s), concurrent contexts in one graph "
+                                  "per GPU, disparity maps gathered on rank 0" % ws,
+                   "shards": shard.assignment_summary(assign, shard.pair_work(all_shapes))},
+        "latency_ms": {"pair_p50": float(np.percentile(lat["pair"], 50)), "pair_p99": float(np.percentile(lat["pair"], 99)),
+                       "done_p50": float(np.percentile(lat["done"], 50)), "done_p99": float(np.percentile(lat["done"], 99)),
+                       "note": "pair: a pair's first to last kernel; done: its GPU's graph start to the pair's end "
+                               "(means over the timed steps)"},
         "sequential_ms": seq_ms, "sequential_value": units / (seq_ms / 1e3),
-        "identical_to_sequential": bool(same), "bad2_nonocc_mean": bad,
-        "gpu_launches": "1 graph launch per step", "clocks": clk.summary(),
+        "identical_to_sequential": bool(same), "bad2_nonocc_mean": float(np.mean(bad)),
+        "gpu_launches": "1 graph launch per step per GPU", "clocks": clk.summary(),
     }
 
 
@@ -504,6 +622,7 @@ def main():
     ap.add_argument("--impl", choices=["cbmv", "reference"], default="cbmv")
     ap.add_argument("--forest", default=FOREST)
     ap.add_argument("--mlp", default=MLP, help="trained MLP parameters (cbmv_b200.train_mlp)")
+    ap.add_argument("--mlp-relu", default=MLP_RELU, help="the ReLU network, timed as a variant")
     ap.add_argument("--classifier", choices=["both", "rf", "mlp"], default="both",
                     help="classifier paths to time (both: the MLP is the headline when it matches "
                          "the RF's held-out bad-2.0)")
@@ -512,16 +631,14 @@ def main():
     ap.add_argument("--batch-pairs", type=int, default=64)
     ap.add_argument("--no-eval", action="store_true",
                     help="skip the held-out bad-2.0 comparison (the RF stays the headline)")
-    ap.add_argument("--cpu-rows", type=int, default=48)
+    ap.add_argument("--cpu-rows", type=int, default=288,
+                    help="rows of the cpu_baseline sample (288 = two of the reference's 144-row batches)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--height", type=int, default=H0,
                     help="rows of the pair (smaller cases for profiler captures; default 554)")
     a = ap.parse_args()
     ws, rank, local = dist_init()
     if a.impl == "reference":
-        if a.steps > 3:  # each reference step is seconds of CPU work; keep the run within minutes
-            a.steps = 3
-        a.warmup = min(a.warmup, 1)
         line = run_reference(a, ws, rank, local)
     elif a.batch:
         line = run_batch(a, ws, rank, local)

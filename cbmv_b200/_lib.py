@@ -10,6 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SO = os.path.join(HERE, "libcbmv.so")
 
 F32, F64 = 0, 1
+ACT_RELU, ACT_GELU = 0, 1
 HWD, DHW = 0, 1
 
 _i64 = ctypes.c_int64
@@ -32,7 +33,8 @@ class cbmv_params(ctypes.Structure):
                 ("alpha1", _flt), ("tau_so", _flt), ("sgm_i", _int), ("L1", _int),
                 ("tau1", _flt), ("cbca_i1", _int), ("cbca_i2", _int), ("median_i", _int),
                 ("median_w", _int), ("blur_sigma", _flt), ("blur_t", _flt), ("direction", _int),
-                ("exact_cbca", _int), ("mlp_ctas", _int), ("cbca_rows", _int), ("sgm_prefetch", _int)]
+                ("exact_cbca", _int), ("mlp_ctas", _int), ("cbca_rows", _int), ("sgm_prefetch", _int),
+                ("interpolate", _int)]
 
 
 # name -> argtypes (all return int status unless listed in _RESTYPE)
@@ -73,6 +75,8 @@ SIGNATURES = {
     "cbmv_mlp_train_step": [_vp, _vp, _vp, _flt, _flt, _vp, _vp],
     "cbmv_mlp_gradients": [_vp, _vp, _vp, _vp, _vp, _vp],
     "cbmv_mlp_status": [_vp, ctypes.POINTER(_int)],
+    "cbmv_mlp_set_activation": [_vp, _int],
+    "cbmv_mlp_get_activation": [_vp, _vp],
     "cbmv_cross": [_vp, _i64, _i64, _int, _flt, _vp, _vp],
     "cbmv_sgm": [_vp, _vp, _vp, _i64, _i64, _int, _flt, _flt, _flt, _flt, _flt, _flt, _int, _vp, _vp],
     "cbmv_cbca": [_vp, _vp, _vp, _i64, _i64, _int, _int, _int, _vp, _vp],

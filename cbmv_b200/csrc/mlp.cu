@@ -11,12 +11,11 @@
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "mlp_net.cuh"
 #include "umma.cuh"
 
 namespace cbmv {
 namespace {
-
-constexpr uint32_t kWaitLimit = 1u << 22;
 
 template <int NT>
 __global__ void __launch_bounds__(128) gemm_bf16_kernel(const uint16_t* __restrict__ A,
@@ -140,21 +139,6 @@ extern "C" int cbmv_gemm_bf16(const uint16_t* A, const uint16_t* B, float* C, in
 namespace cbmv {
 namespace {
 
-constexpr int kF = 20, kK1 = 64, kH1 = 128, kH2 = 128, kH3 = 64;
-constexpr int kNormN = 3 * kF;
-constexpr int kOffW1 = kNormN, kOffB1 = kOffW1 + kH1 * kF, kOffW2 = kOffB1 + kH1,
-              kOffB2 = kOffW2 + kH2 * kH1, kOffW3 = kOffB2 + kH2, kOffB3 = kOffW3 + kH3 * kH2,
-              kOffW4 = kOffB3 + kH3, kOffB4 = kOffW4 + kH3, kNParams = kOffB4 + 1;
-
-// ReLU and its derivative (0 at x = 0)
-__device__ __forceinline__ float relu_t(float x, float* drelu) {
-  if (drelu) *drelu = x > 0.0f ? 1.0f : 0.0f;
-  return x > 0.0f ? x : 0.0f;
-}
-
-__device__ __forceinline__ uint16_t to_bf16(float x) {
-  return __bfloat16_as_ushort(__float2bfloat16_rn(x));
-}
 
 #define GS(i, n) for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
@@ -171,15 +155,15 @@ __global__ void mlp_prep_kernel(const float* __restrict__ X, int B, const float*
   }
 }
 
-// S = Z + b; A = relu(S) as bf16 [B,N] and [N,B]; Af = relu(S) float (optional)
-__global__ void mlp_bias_relu_kernel(const float* __restrict__ Z, const float* __restrict__ bias, int B,
-                                     int N, float* __restrict__ S, uint16_t* __restrict__ A,
-                                     uint16_t* __restrict__ AT, float* __restrict__ Af) {
+// S = Z + b; A = act(S) as bf16 [B,N] and [N,B]; Af = act(S) float (optional)
+__global__ void mlp_bias_act_kernel(const float* __restrict__ Z, const float* __restrict__ bias, int B,
+                                    int N, int act, float* __restrict__ S, uint16_t* __restrict__ A,
+                                    uint16_t* __restrict__ AT, float* __restrict__ Af) {
   GS(t, (int64_t)B * N) {
     const int b = (int)(t / N), n = (int)(t % N);
     const float s = Z[t] + bias[n];
     S[t] = s;
-    const float a = relu_t(s, nullptr);
+    const float a = act_t(act, s, nullptr);
     if (A) A[t] = to_bf16(a);
     if (AT) AT[(int64_t)n * B + b] = to_bf16(a);
     if (Af) Af[t] = a;
@@ -188,10 +172,10 @@ __global__ void mlp_bias_relu_kernel(const float* __restrict__ Z, const float* _
 
 // output layer, loss and the first backward step, one warp per sample:
 // z = A3 . w4 + b4, p = sigmoid(z), loss_i = BCE; dz = (p - y) / B;
-// dS3 = dz * w4 * relu'(S3) -> bf16 [B,64] and [64,B]; per-sample dz and
+// dS3 = dz * w4 * act'(S3) -> bf16 [B,64] and [64,B]; per-sample dz and
 // dz*A3 kept for the (ordered) reductions of dw4 / db4.
 __global__ void mlp_head_kernel(const float* __restrict__ A3f, const float* __restrict__ S3,
-                                const float* __restrict__ y, const float* __restrict__ P, int B,
+                                const float* __restrict__ y, const float* __restrict__ P, int B, int act,
                                 float* __restrict__ loss_i, float* __restrict__ dz,
                                 float* __restrict__ dw4_i, uint16_t* __restrict__ dS3,
                                 uint16_t* __restrict__ dS3T, float* __restrict__ dS3f) {
@@ -213,7 +197,7 @@ __global__ void mlp_head_kernel(const float* __restrict__ A3f, const float* __re
     }
     for (int k = lane; k < kH3; k += 32) {
       float dg;
-      relu_t(S3[(int64_t)b * kH3 + k], &dg);
+      act_t(act, S3[(int64_t)b * kH3 + k], &dg);
       const float d = g * P[kOffW4 + k] * dg;
       dS3[(int64_t)b * kH3 + k] = to_bf16(d);
       dS3T[(int64_t)k * B + b] = to_bf16(d);
@@ -223,14 +207,14 @@ __global__ void mlp_head_kernel(const float* __restrict__ A3f, const float* __re
   }
 }
 
-// dS = dA * relu'(S) -> bf16 [B,N], [N,B] and float [B,N]
-__global__ void mlp_drelu_kernel(const float* __restrict__ dA, const float* __restrict__ S, int B, int N,
+// dS = dA * act'(S) -> bf16 [B,N], [N,B] and float [B,N]
+__global__ void mlp_dact_kernel(const float* __restrict__ dA, const float* __restrict__ S, int B, int N, int act,
                                  uint16_t* __restrict__ dS, uint16_t* __restrict__ dST,
                                  float* __restrict__ dSf) {
   GS(t, (int64_t)B * N) {
     const int b = (int)(t / N), n = (int)(t % N);
     float dg;
-    relu_t(S[t], &dg);
+    act_t(act, S[t], &dg);
     const float d = dA[t] * dg;
     dS[t] = to_bf16(d);
     dST[(int64_t)n * B + b] = to_bf16(d);
@@ -329,17 +313,6 @@ __global__ void sum_kernel(const float* __restrict__ a, int n, float* __restrict
 }  // namespace
 }  // namespace cbmv
 
-struct cbmv_mlp {
-  int B = 0;
-  void* mem = nullptr;
-  float *P, *m, *v, *g;                  // params, Adam moments, gathered grads
-  uint16_t *W1b, *W1T, *W2b, *W2T, *W3b, *W3T;
-  uint16_t *X0, *X0T, *A1, *A1T, *A2, *A2T, *dS3, *dS3T, *dS2, *dS2T, *dS1, *dS1T;
-  float *Z, *S1, *S2, *S3, *A3f, *dA, *dSf, *loss_i, *dz, *dw4_i;
-  float *dW1, *dW2, *dW3T, *db1, *db2, *db3, *dw4, *db4, *loss;
-  int* status;
-  int step = 0;
-};
 
 namespace {
 size_t carve_mlp(cbmv_mlp* n, char* base) {
@@ -459,12 +432,12 @@ int mlp_fwd_bwd(cbmv_mlp* n, const float* X, const float* y, cudaStream_t st) {
   int rc;
   mlp_prep_kernel<<<g, 256, 0, st>>>(X, B, n->P, n->X0, n->X0T);
   if ((rc = launch_gemm_bf16(n->X0, n->W1b, n->Z, B, kH1, kK1, n->status, st))) return rc;
-  mlp_bias_relu_kernel<<<g, 256, 0, st>>>(n->Z, n->P + kOffB1, B, kH1, n->S1, n->A1, n->A1T, nullptr);
+  mlp_bias_act_kernel<<<g, 256, 0, st>>>(n->Z, n->P + kOffB1, B, kH1, n->act, n->S1, n->A1, n->A1T, nullptr);
   if ((rc = launch_gemm_bf16(n->A1, n->W2b, n->Z, B, kH2, kH1, n->status, st))) return rc;
-  mlp_bias_relu_kernel<<<g, 256, 0, st>>>(n->Z, n->P + kOffB2, B, kH2, n->S2, n->A2, n->A2T, nullptr);
+  mlp_bias_act_kernel<<<g, 256, 0, st>>>(n->Z, n->P + kOffB2, B, kH2, n->act, n->S2, n->A2, n->A2T, nullptr);
   if ((rc = launch_gemm_bf16(n->A2, n->W3b, n->Z, B, kH3, kH2, n->status, st))) return rc;
-  mlp_bias_relu_kernel<<<g, 256, 0, st>>>(n->Z, n->P + kOffB3, B, kH3, n->S3, nullptr, nullptr, n->A3f);
-  mlp_head_kernel<<<grid_for((int64_t)B * 32, 256), 256, 0, st>>>(n->A3f, n->S3, y, n->P, B, n->loss_i,
+  mlp_bias_act_kernel<<<g, 256, 0, st>>>(n->Z, n->P + kOffB3, B, kH3, n->act, n->S3, nullptr, nullptr, n->A3f);
+  mlp_head_kernel<<<grid_for((int64_t)B * 32, 256), 256, 0, st>>>(n->A3f, n->S3, y, n->P, B, n->act, n->loss_i,
                                                                   n->dz, n->dw4_i, n->dS3, n->dS3T, n->dSf);
   mlp_colsum_kernel<<<1, 64, 0, st>>>(n->dw4_i, B, kH3, n->dw4);
   mlp_colsum_kernel<<<1, 64, 0, st>>>(n->dz, B, 1, n->db4);
@@ -473,12 +446,12 @@ int mlp_fwd_bwd(cbmv_mlp* n, const float* X, const float* y, cudaStream_t st) {
   // layer 3: dW3^T = A2^T dS3, dA2 = dS3 W3
   if ((rc = launch_gemm_bf16(n->A2T, n->dS3T, n->dW3T, kH2, kH3, B, n->status, st))) return rc;
   if ((rc = launch_gemm_bf16(n->dS3, n->W3T, n->dA, B, kH2, kH3, n->status, st))) return rc;
-  mlp_drelu_kernel<<<g, 256, 0, st>>>(n->dA, n->S2, B, kH2, n->dS2, n->dS2T, n->dSf);
+  mlp_dact_kernel<<<g, 256, 0, st>>>(n->dA, n->S2, B, kH2, n->act, n->dS2, n->dS2T, n->dSf);
   mlp_colsum_kernel<<<1, 128, 0, st>>>(n->dSf, B, kH2, n->db2);
   // layer 2: dW2 = dS2^T A1, dA1 = dS2 W2
   if ((rc = launch_gemm_bf16(n->dS2T, n->A1T, n->dW2, kH2, kH1, B, n->status, st))) return rc;
   if ((rc = launch_gemm_bf16(n->dS2, n->W2T, n->dA, B, kH1, kH2, n->status, st))) return rc;
-  mlp_drelu_kernel<<<g, 256, 0, st>>>(n->dA, n->S1, B, kH1, n->dS1, n->dS1T, n->dSf);
+  mlp_dact_kernel<<<g, 256, 0, st>>>(n->dA, n->S1, B, kH1, n->act, n->dS1, n->dS1T, n->dSf);
   mlp_colsum_kernel<<<1, 128, 0, st>>>(n->dSf, B, kH1, n->db1);
   // layer 1: dW1 = dS1^T X0
   if ((rc = launch_gemm_bf16(n->dS1T, n->X0T, n->dW1, kH1, kK1, B, n->status, st))) return rc;
@@ -520,453 +493,22 @@ extern "C" int cbmv_mlp_gradients(cbmv_mlp* n, const float* X, const float* y, f
   return CBMV_OK;
 }
 
+extern "C" int cbmv_mlp_set_activation(cbmv_mlp* n, int act) {
+  CBMV_REQUIRE(n, CBMV_EINVAL, "null pointer argument");
+  CBMV_REQUIRE(act == CBMV_ACT_RELU || act == CBMV_ACT_GELU, CBMV_EINVAL, "unknown activation %d", act);
+  n->act = act;
+  return CBMV_OK;
+}
+
+extern "C" int cbmv_mlp_get_activation(const cbmv_mlp* n, int* act) {
+  CBMV_REQUIRE(n && act, CBMV_EINVAL, "null pointer argument");
+  *act = n->act;
+  return CBMV_OK;
+}
+
 // Status of the tensor-core waits since creation (0 = fine).
 extern "C" int cbmv_mlp_status(const cbmv_mlp* n, int* status) {
   CBMV_REQUIRE(n && status, CBMV_EINVAL, "null pointer argument");
   CBMV_CUDA(cudaMemcpy(status, n->status, sizeof(int), cudaMemcpyDeviceToHost));
   return CBMV_OK;
 }
-
-// ====================================================================
-// Fused inference: features of 128 consecutive (pixel, d) samples -> the
-// network on the tensor cores -> matching cost 1 - P(correct), float32.
-//
-// One persistent CTA per SM, four independent groups of 128 threads; each
-// group owns a 128-row tile in flight (its activation buffer in shared
-// memory and 128 tensor-memory columns), so while one group's MMAs run the
-// others compute features or epilogues.  Thread r of a group owns row r of
-// its tile: it forms the 20 features of sample r (their inputs for the
-// next tile are loaded while this one runs through the network), then
-// that row's columns in each epilogue.  The group's first thread issues
-// its MMAs, commits them to the group's mbarrier and alone polls it; the
-// others wait on the group's named barrier (no issue slots spent
-// spinning), which also hands them the poll's result.
-//
-// Arithmetic, per layer (the float32 accumulator in tensor memory); every
-// bias enters as bf16 high + low parts multiplied by constant ones:
-//   layer 1  K = 32: 20 normalised features, two constant-one columns whose
-//            weights are b1's parts, zeros;
-//   layers 2, 3: a first K = 16 MMA of a constant tile (ones in columns 0
-//            and 1) against b2's / b3's parts (stored in the unused K
-//            columns 32..63 of layer 1's weight tile) initialises the
-//            accumulator, the layer's MMAs accumulate onto it;
-//   hidden activations: ReLU and the bf16 rounding in one instruction
-//            (cvt.rn.relu.bf16x2.f32) per pair of columns;
-//   output   layer 4 is an MMA too: N = 16, rows 0 and 1 of its weight tile
-//            are the high and low bf16 parts of w4, z = D[0] + D[1] + b4,
-//            cost = 1 - sigmoid(z) = 1 / (1 + exp(z)).
-// The features themselves are formed in float32 (they enter the network as
-// bf16), from float32 cost volumes and float32 row statistics (min, 1/den),
-// with one reciprocal 1/(c + e) shared by the left and right ratio.
-// ====================================================================
-#include "features.cuh"
-
-namespace cbmv {
-namespace {
-
-struct FeatVolsF {
-  const float* v[4];
-};
-
-constexpr int kGroups = 4;                        // tiles in flight per CTA
-constexpr int kGroupThreads = 128;               // one thread per tile row
-constexpr int kInfThreads = kGroupThreads * kGroups;
-constexpr size_t kSmW1i = 128 * 128;      // [128 x 64] SW128, K = 32 used
-constexpr size_t kSmW2i = 2 * 128 * 128;  // [128 x 128]
-constexpr size_t kSmW3i = 2 * 64 * 128;   // [64 x 128]
-constexpr size_t kSmW4i = 16 * 128;       // [16 x 64]
-constexpr size_t kSmOne = 128 * 128;      // [128 x 64], ones in columns 0 and 1
-constexpr size_t kSmTile = 2 * 128 * 128; // a group's activation tile [128 x 128]
-constexpr size_t kSmInf = 1024 + kSmW1i + kSmW2i + kSmW3i + kSmW4i + kSmOne + kGroups * kSmTile;
-constexpr int kColB2 = 32, kColB3 = 48;  // K columns of layer 1's weight tile holding b2, b3
-constexpr uint32_t kBf16OneOne = 0x3F803F80u;  // two bf16 ones
-
-static __constant__ float kEpsF[4] = {0.01f, 1.01f, 0.01f, 0.01f};
-static __constant__ float kInvSigmaF[4] = {(float)(1.0 / (2.0 * 8 * 8)), (float)(1.0 / 0.02),
-                                           (float)(1.0 / (2.0 * 100 * 100)), (float)(1.0 / (2.0 * 100 * 100))};
-
-__device__ __forceinline__ void group_sync(int g) {
-  asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "n"(kGroupThreads) : "memory");
-}
-// barrier of the group that also ANDs a flag over its threads
-__device__ __forceinline__ bool group_all(int g, bool v) {
-  uint32_t r;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.u32 p, %1, 0;\n\t"
-      "bar.red.and.pred q, %2, %3, p;\n\t"
-      "selp.u32 %0, 1, 0, q;\n\t}"
-      : "=r"(r)
-      : "r"((uint32_t)v), "r"(g + 1), "n"(kGroupThreads)
-      : "memory");
-  return r != 0;
-}
-
-// Two float32 values as a packed bf16 pair (low = a), round to nearest even
-__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
-  const __nv_bfloat162 x = __floats2bfloat162_rn(a, b);
-  return *reinterpret_cast<const uint32_t*>(&x);
-}
-
-// ReLU of two float32 pre-activations, as a packed bf16 pair (low = a),
-// round to nearest even
-__device__ __forceinline__ uint32_t relu_bf16x2(float a, float b) {
-  uint32_t r;
-  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
-  return r;
-}
-
-// ratio and likelihood of cost c (featextract.cpp:333 and :440) in float32
-// against its row statistics st = (min, 1/den); inv_ce = 1 / (c + e).
-// expf (about 1 ulp over the whole range) rather than the approximate
-// exponential, whose error grows with the argument (large for the census
-// and NCC likelihoods far from the row minimum).
-__device__ __forceinline__ void conf_f32(float c, float inv_ce, float2 st, float e, float inv_sigma,
-                                         float* ratio, float* lik) {
-  const float t = c - st.x;
-  *ratio = st.x == kRandMaxF ? 0.0f : (st.x + e) * inv_ce;
-  *lik = expf(-(t * t) * inv_sigma) * st.y;  // 1/den = 0 on sentinel rows
-}
-
-// bf16 high part of x and the bf16 rounding of the rest: x ~ hi + lo
-__device__ __forceinline__ void split_bf16(float x, float* hi, float* lo) {
-  *hi = __bfloat162float(__float2bfloat16_rn(x));
-  *lo = x - *hi;
-}
-
-// Stage the inference weights from the float32 parameter vector, and the
-// constant tile of the bias MMAs.
-__device__ void stage_inference_weights(const float* __restrict__ P, unsigned char* sW1, unsigned char* sW2,
-                                        unsigned char* sW3, unsigned char* sW4, unsigned char* sOne) {
-  for (int q = threadIdx.x; q < 128 * 64; q += blockDim.x) {
-    const int r = q >> 6, k = q & 63;
-    float v = 0.0f, hi, lo;
-    if (k < kF) {
-      v = P[kOffW1 + r * kF + k];
-    } else if (k == kF || k == kF + 1) {
-      split_bf16(P[kOffB1 + r], &hi, &lo);
-      v = k == kF ? hi : lo;
-    } else if (k == kColB2 || k == kColB2 + 1) {
-      split_bf16(P[kOffB2 + r], &hi, &lo);
-      v = k == kColB2 ? hi : lo;
-    } else if (r < kH3 && (k == kColB3 || k == kColB3 + 1)) {
-      split_bf16(P[kOffB3 + r], &hi, &lo);
-      v = k == kColB3 ? hi : lo;
-    }
-    *reinterpret_cast<uint16_t*>(sW1 + umma::sw128_offset(128, r, k)) = to_bf16(v);
-    *reinterpret_cast<uint16_t*>(sOne + umma::sw128_offset(128, r, k)) = to_bf16(k < 2 ? 1.0f : 0.0f);
-  }
-  for (int q = threadIdx.x; q < 128 * 128; q += blockDim.x) {
-    const int r = q >> 7, k = q & 127;
-    *reinterpret_cast<uint16_t*>(sW2 + umma::sw128_offset(128, r, k)) = to_bf16(P[kOffW2 + q]);
-  }
-  for (int q = threadIdx.x; q < 64 * 128; q += blockDim.x) {
-    const int r = q >> 7, k = q & 127;
-    *reinterpret_cast<uint16_t*>(sW3 + umma::sw128_offset(64, r, k)) = to_bf16(P[kOffW3 + q]);
-  }
-  for (int q = threadIdx.x; q < 16 * 64; q += blockDim.x) {
-    const int r = q >> 6, k = q & 63;
-    float hi, lo;
-    split_bf16(P[kOffW4 + k], &hi, &lo);
-    *reinterpret_cast<uint16_t*>(sW4 + umma::sw128_offset(16, r, k)) = to_bf16(r == 0 ? hi : r == 1 ? lo : 0.0f);
-  }
-}
-
-// Row `row` of a K-major SW128 activation tile: 16-byte chunk j (columns
-// 8j .. 8j+7 of a 64-column atom) of atom a sits at
-// rowp + a * 128 * 128 + ((j << 4) ^ r7s), r7s = (row % 8) << 4.
-__device__ __forceinline__ uint4* tile_chunk(unsigned char* rowp, int r7s, int a, int j) {
-  return reinterpret_cast<uint4*>(rowp + a * 128 * 128 + ((j << 4) ^ r7s));
-}
-
-// ReLU of 32 loaded accumulator columns c .. c+31 -> the activation tile
-__device__ __forceinline__ void epilogue_chunk(unsigned char* rowp, int r7s, int c, const uint32_t* v) {
-  uint32_t h[16];
-#pragma unroll
-  for (int i = 0; i < 16; i++) h[i] = relu_bf16x2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
-#pragma unroll
-  for (int q = 0; q < 4; q++)
-    *tile_chunk(rowp, r7s, c >> 6, ((c & 63) >> 3) + q) = make_uint4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);
-}
-
-// One hidden-layer epilogue of this thread's row: accumulator columns
-// 0 .. NC-1 -> ReLU as bf16 into the activation tile.  The load of the
-// next 32 columns is in flight while the current ones are computed.
-template <int NC>
-__device__ __forceinline__ void epilogue_hidden(uint32_t tlane, unsigned char* rowp, int r7s) {
-  uint32_t va[32], vb[32];
-  umma::tmem_ld32_issue(tlane, va);
-  umma::tmem_ld32_wait(va);
-#pragma unroll
-  for (int c = 0; c < NC; c += 64) {
-    umma::tmem_ld32_issue(tlane + c + 32, vb);
-    epilogue_chunk(rowp, r7s, c, va);
-    umma::tmem_ld32_wait(vb);
-    if (c + 64 < NC) umma::tmem_ld32_issue(tlane + c + 64, va);
-    epilogue_chunk(rowp, r7s, c + 32, vb);
-    if (c + 64 < NC) umma::tmem_ld32_wait(va);
-  }
-}
-
-// Inputs of the four matchers' features of one sample: its costs and the
-// row statistics (min, 1/den) of its left and right views.
-struct FeatIn {
-  float c[4];
-  float2 sl[4], sr[4];
-};
-
-__device__ __forceinline__ void load_feat_in(const FeatVolsF& fv, const float2* __restrict__ statsf, int64_t HW,
-                                             int64_t N, int64_t t, int64_t p, int d, int64_t x, FeatIn& in) {
-  const bool valid = t < N;
-  const int64_t tv = valid ? t : 0, pv = valid ? p : 0;
-  const int dv = valid ? d : 0;
-  const bool has_right = valid && x >= d;
-#pragma unroll
-  for (int m = 0; m < 4; m++) {
-    in.c[m] = __ldg(fv.v[m] + tv);
-    in.sl[m] = __ldg(statsf + (int64_t)(2 * m) * HW + pv);
-    in.sr[m] = has_right ? __ldg(statsf + (int64_t)(2 * m + 1) * HW + pv - dv) : make_float2(kRandMaxF, 0.0f);
-  }
-}
-
-// The 20 features of one sample in the reference's column order
-// (test.py:521-595): 0-3 the costs, 4-7 ratio, 8-11 likelihood, 12-19 the
-// same two of the right view warped to the left, all in float32.
-__device__ __forceinline__ void features_f32(const FeatIn& in, float* f) {
-#pragma unroll
-  for (int m = 0; m < 4; m++) {
-    const float c = in.c[m];
-    const float inv_ce = __fdividef(1.0f, c + kEpsF[m]);
-    f[m] = c;
-    conf_f32(c, inv_ce, in.sl[m], kEpsF[m], kInvSigmaF[m], &f[4 + m], &f[8 + m]);
-    conf_f32(c, inv_ce, in.sr[m], kEpsF[m], kInvSigmaF[m], &f[12 + m], &f[16 + m]);
-  }
-}
-
-// The learned path's float32 features of the samples idx[i] = (y*W + x)*D + d,
-// through the same code as the fused kernel below; out [n, 20].
-__global__ void features_f32_gather_kernel(FeatVolsF fv, const float2* __restrict__ statsf, int64_t H, int64_t W,
-                                           int D, const int64_t* __restrict__ idx, int64_t n, float* __restrict__ out) {
-  const int64_t HW = H * W, N = HW * D;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t t = idx[i];
-    const int64_t p = t / D;
-    FeatIn in;
-    load_feat_in(fv, statsf, HW, N, t, p, (int)(t - p * D), p % W, in);
-    float f[20];
-    features_f32(in, f);
-#pragma unroll
-    for (int k = 0; k < 20; k++) out[i * 20 + k] = f[k];
-  }
-}
-
-__global__ void __launch_bounds__(kInfThreads, 1)
-    features_mlp_kernel(FeatVolsF fv, const float2* __restrict__ statsf, int64_t H, int64_t W, int D,
-                        const float* __restrict__ P, float* __restrict__ prob0, int* __restrict__ status) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char* sW1 = base;
-  unsigned char* sW2 = sW1 + kSmW1i;
-  unsigned char* sW3 = sW2 + kSmW2i;
-  unsigned char* sW4 = sW3 + kSmW3i;
-  unsigned char* sOne = sW4 + kSmW4i;
-  unsigned char* sTiles = sOne + kSmOne;
-  __shared__ float4 s_nrm[kF];  // per feature column: cap, mu, inv_sd
-  __shared__ float s_b4;
-  __shared__ uint64_t bars[kGroups];
-  __shared__ uint32_t tmem_base;
-  const int tid = threadIdx.x, g = tid / kGroupThreads, row = tid % kGroupThreads, wq = row >> 5;
-
-  if (tid < 32) umma::tmem_alloc(&tmem_base, 128 * kGroups);
-  if (tid < kGroups) umma::mbar_init(&bars[tid], 1);
-  stage_inference_weights(P, sW1, sW2, sW3, sW4, sOne);
-  for (int i = tid; i < kF; i += kInfThreads) s_nrm[i] = make_float4(P[i], P[kF + i], P[2 * kF + i], 0.0f);
-  if (tid == 0) s_b4 = P[kOffB4];
-  umma::fence_async_smem();
-  umma::tc_fence_before();
-  __syncthreads();
-  umma::tc_fence_after();
-
-  unsigned char* sA = sTiles + g * kSmTile;
-  unsigned char* rowp = sA + (row >> 3) * 1024 + (row & 7) * 128;
-  const int r7s = (row & 7) << 4;
-  uint64_t* bar = &bars[g];
-  const uint32_t tacc = tmem_base + (uint32_t)(g * 128);
-  const uint32_t tlane = tacc + ((uint32_t)(wq * 32) << 16);
-  const bool leader = row == 0;
-  constexpr uint32_t id128 = umma::idesc_bf16(128, 128), id64 = umma::idesc_bf16(128, 64),
-                     id16 = umma::idesc_bf16(128, 16);
-  // operand descriptors, formed where the leader issues (keeps them out of the other threads' registers)
-#define DESC(ptr) umma::sw128_desc(umma::smem_u32(ptr))
-
-  const int64_t HW = H * W, N = HW * D;
-  const int64_t tiles = (N + 127) / 128;
-  const int64_t tstride = (int64_t)gridDim.x * kGroups;
-  // this thread's sample t = tile * 128 + row as (pixel p, disparity d, column x), advanced incrementally
-  int64_t tile = (int64_t)blockIdx.x * kGroups + g;
-  int64_t t = tile * 128 + row;
-  int64_t p = t / D;
-  int d = (int)(t - p * D);
-  int64_t x = p % W;
-  const int64_t step = tstride * 128;
-  const int64_t sp = step / D;
-  const int sd = (int)(step - sp * D);
-  const int64_t sx = sp % W;
-  uint32_t phase = 0;
-  bool ok = true;
-
-  FeatIn in;
-  load_feat_in(fv, statsf, HW, N, t, p, d, x, in);
-  for (; tile < tiles; tile += tstride) {
-    // 1. the 20 features of sample t -> row of X0 (the first atom of the tile):
-    //    columns 0..19 in the reference's order, 20 and 21 the bias inputs, 22..31 zero
-    {
-      float f[20];
-      features_f32(in, f);
-      uint32_t u[10];
-#pragma unroll
-      for (int k = 0; k < 20; k += 2) {
-        const float4 na = s_nrm[k], nb = s_nrm[k + 1];
-        u[k >> 1] = pack_bf16x2((fminf(f[k], na.x) - na.y) * na.z, (fminf(f[k + 1], nb.x) - nb.y) * nb.z);
-      }
-      *tile_chunk(rowp, r7s, 0, 0) = make_uint4(u[0], u[1], u[2], u[3]);
-      *tile_chunk(rowp, r7s, 0, 1) = make_uint4(u[4], u[5], u[6], u[7]);
-      *tile_chunk(rowp, r7s, 0, 2) = make_uint4(u[8], u[9], kBf16OneOne, 0u);
-      *tile_chunk(rowp, r7s, 0, 3) = make_uint4(0u, 0u, 0u, 0u);
-    }
-    // advance to this thread's next sample (tile + tstride) and load its
-    // inputs, in flight while this tile runs through the network
-    const int64_t t_cur = t;
-    t += step;
-    p += sp;
-    d += sd;
-    x += sx;
-    if (d >= D) {
-      d -= D;
-      p += 1;
-      x += 1;
-    }
-    if (x >= W) x -= W;
-    if (tile + tstride < tiles) load_feat_in(fv, statsf, HW, N, t, p, d, x, in);
-    umma::fence_async_smem();
-    umma::tc_fence_before();
-    group_sync(g);
-    umma::tc_fence_after();
-    // 2. layer 1 (K = 32) -> accumulator columns 0..127
-    if (leader) {
-      const uint64_t dA0 = DESC(sA), dW1 = DESC(sW1);
-      umma::mma_bf16(tacc, dA0, dW1, id128, false);
-      umma::mma_bf16(tacc, dA0 + 2, dW1 + 2, id128, true);
-      umma::mma_commit(bar);
-    }
-    ok = group_all(g, leader ? umma::mbar_wait(bar, phase, kWaitLimit) : true);
-    phase ^= 1u;
-    umma::tc_fence_after();
-    if (!ok) break;
-    epilogue_hidden<128>(tlane, rowp, r7s);
-    umma::fence_async_smem();
-    umma::tc_fence_before();
-    group_sync(g);
-    umma::tc_fence_after();
-    // 3. layer 2 (K = 128) onto the bias b2
-    if (leader) {
-      const uint64_t dA0 = DESC(sA), dA1 = DESC(sA + 128 * 128), dW20 = DESC(sW2), dW21 = DESC(sW2 + 128 * 128);
-      umma::mma_bf16(tacc, DESC(sOne), DESC(sW1) + 2 * (kColB2 / 16), id128, false);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA0 + 2 * kk, dW20 + 2 * kk, id128, true);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA1 + 2 * kk, dW21 + 2 * kk, id128, true);
-      umma::mma_commit(bar);
-    }
-    ok = group_all(g, leader ? umma::mbar_wait(bar, phase, kWaitLimit) : true);
-    phase ^= 1u;
-    umma::tc_fence_after();
-    if (!ok) break;
-    epilogue_hidden<128>(tlane, rowp, r7s);
-    umma::fence_async_smem();
-    umma::tc_fence_before();
-    group_sync(g);
-    umma::tc_fence_after();
-    // 4. layer 3 (N = 64) onto the bias b3
-    if (leader) {
-      const uint64_t dA0 = DESC(sA), dA1 = DESC(sA + 128 * 128), dW30 = DESC(sW3), dW31 = DESC(sW3 + 64 * 128);
-      umma::mma_bf16(tacc, DESC(sOne), DESC(sW1) + 2 * (kColB3 / 16), id64, false);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA0 + 2 * kk, dW30 + 2 * kk, id64, true);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA1 + 2 * kk, dW31 + 2 * kk, id64, true);
-      umma::mma_commit(bar);
-    }
-    ok = group_all(g, leader ? umma::mbar_wait(bar, phase, kWaitLimit) : true);
-    phase ^= 1u;
-    umma::tc_fence_after();
-    if (!ok) break;
-    epilogue_hidden<64>(tlane, rowp, r7s);
-    umma::fence_async_smem();
-    umma::tc_fence_before();
-    group_sync(g);
-    umma::tc_fence_after();
-    // 5. output layer (N = 16, rows 0/1 = high/low parts of w4) -> columns 64..79
-    if (leader) {
-      const uint64_t dA0 = DESC(sA), dW4 = DESC(sW4);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc + 64, dA0 + 2 * kk, dW4 + 2 * kk, id16, kk > 0);
-      umma::mma_commit(bar);
-    }
-    ok = group_all(g, leader ? umma::mbar_wait(bar, phase, kWaitLimit) : true);
-    phase ^= 1u;
-    umma::tc_fence_after();
-    if (!ok) break;
-    {
-      uint32_t z2[2];
-      asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];"
-                   : "=r"(z2[0]), "=r"(z2[1])
-                   : "r"(tlane + 64));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(z2[0]), "+r"(z2[1]) : : "memory");
-      const float z = (__uint_as_float(z2[0]) + __uint_as_float(z2[1])) + s_b4;
-      if (t_cur < N) prob0[t_cur] = 1.0f / (1.0f + __expf(z));
-    }
-    umma::tc_fence_before();
-  }
-  if (!ok) {
-    // let this group's MMAs still in flight finish (bounded) before the memory is freed
-    if (leader) {
-      atomicExch(status, 1);
-      umma::mbar_wait(bar, phase ^ 1u, kWaitLimit);
-    }
-  }
-  umma::tc_fence_before();
-  __syncthreads();
-  if (tid < 32) umma::tmem_dealloc(tmem_base, 128 * kGroups);
-#undef DESC
-}
-
-}  // namespace
-
-int launch_features_f32_gather(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
-                               const int64_t* idx, int64_t n, float* out, cudaStream_t st) {
-  FeatVolsF fv = {{vols[0], vols[1], vols[2], vols[3]}};
-  const int64_t blocks = (n + 255) / 256;
-  features_f32_gather_kernel<<<(unsigned)(blocks < 65535 * 16 ? blocks : 65535 * 16), 256, 0, st>>>(
-      fv, statsf, H, W, D, idx, n, out);
-  return check_launch("features_f32_gather");
-}
-
-int launch_features_mlp(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
-                        const cbmv_mlp* m, float* prob0, cudaStream_t st, int max_ctas) {
-  int dev = 0, sms = 0;
-  CBMV_CUDA(cudaGetDevice(&dev));
-  CBMV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  CBMV_CUDA(cudaFuncSetAttribute(features_mlp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kSmInf));
-  CBMV_REQUIRE(((uintptr_t)statsf & 7) == 0, CBMV_EINVAL, "feature statistics must be 8-byte aligned");
-  const int64_t tiles = (H * W * D + 127) / 128;
-  const int64_t need = (tiles + kGroups - 1) / kGroups;
-  const int cap = max_ctas > 0 && max_ctas < sms ? max_ctas : sms;
-  const int grid = (int)(need < cap ? need : cap);
-  FeatVolsF fv = {{vols[0], vols[1], vols[2], vols[3]}};
-  features_mlp_kernel<<<grid, kInfThreads, kSmInf, st>>>(fv, statsf, H, W, D, m->P, prob0, m->status);
-  return check_launch("features_mlp");
-}
-
-}  // namespace cbmv

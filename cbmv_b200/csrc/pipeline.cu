@@ -54,6 +54,7 @@ extern "C" void cbmv_params_default(cbmv_params* p) {
   p->mlp_ctas = 0;
   p->cbca_rows = 0;
   p->sgm_prefetch = 0;
+  p->interpolate = 0;  // main.py:70 runs the _mem post
 }
 
 struct cbmv_ctx {
@@ -105,14 +106,16 @@ struct Work {
   double* stats;
   float2* statsf;  // (min, 1/den) in float32 for the classifier network
   float *volA, *volB;
-  float *imL, *imR, *crossL, *crossR, *dtmp, *dtmp2;
+  float* volC;  // the right view's cost of the _interp post (else null)
+  float *imL, *imR, *crossL, *crossR, *dtmp, *dtmp2, *dright, *outlier;
   float* grad;  // SGM neighbour differences: left h/v, right h/v
   double* mom;
 };
 
 // f32: the four matcher volumes hold float32 (4 B per (p,d) each) instead of
 // float64; the four SGM direction volumes then alias them one to one.
-Work carve(void* base, int64_t H, int64_t W, int D, size_t* bytes, bool f32 = false) {
+// interp: one more float32 volume for the right view of the _interp post.
+Work carve(void* base, int64_t H, int64_t W, int D, size_t* bytes, bool f32, bool interp) {
   Carve c{(char*)base};
   Work w;
   const size_t HW = (size_t)H * W, V = HW * (size_t)D;
@@ -132,12 +135,15 @@ Work carve(void* base, int64_t H, int64_t W, int D, size_t* bytes, bool f32 = fa
   w.statsf = c.take<float2>(8 * HW);
   w.volA = c.take<float>(V);
   w.volB = c.take<float>(V);
+  w.volC = interp ? c.take<float>(V) : nullptr;
   w.imL = c.take<float>(HW);
   w.imR = c.take<float>(HW);
   w.crossL = c.take<float>(4 * HW);
   w.crossR = c.take<float>(4 * HW);
   w.dtmp = c.take<float>(HW);
   w.dtmp2 = c.take<float>(HW);
+  w.dright = c.take<float>(HW);
+  w.outlier = c.take<float>(HW);
   w.grad = c.take<float>(4 * HW);
   w.mom = c.take<double>(4);
   *bytes = c.off + 256;
@@ -159,6 +165,7 @@ int check_params(const cbmv_params* p) {
   CBMV_REQUIRE(p->sgm_prefetch == 0 || p->sgm_prefetch == 1 || p->sgm_prefetch == 2 || p->sgm_prefetch == 4,
                CBMV_EINVAL, "sgm_prefetch must be 0, 1, 2 or 4");
   CBMV_REQUIRE(p->mlp_ctas >= 0, CBMV_EINVAL, "mlp_ctas must be >= 0");
+  CBMV_REQUIRE(p->interpolate == 0 || p->interpolate == 1, CBMV_EINVAL, "interpolate must be 0 or 1");
   return CBMV_OK;
 }
 
@@ -231,8 +238,63 @@ static int ensure_gaussian(cbmv_ctx* c, float sigma) {
     if (rc_) return rc_;      \
   } while (0)
 
-// Steps 5 of the header comment on the float32 volume in w.volA; the
-// disparity lands in `disp`.
+// The cost-optimisation chain of Testing.__postprocessing_mem
+// (test.py:355-405) on one float32 [H,W,D] cost volume held in `cur`:
+// cbca_i1 CBCA passes, sgm_i SGM iterations (each the mean of the four
+// scan directions, test.py:378-383), cbca_i2 CBCA passes.  crossA / crossB
+// are the arms of the volume's own view and of the matching view: the left
+// view's chain passes (left, right, direction); the right view's chain of
+// the _interp post (test.py:176-251) passes (right, left, -direction), and
+// its SGM keeps the images in their order (test.py:203-207).  `oth` is a
+// second volume; *result receives the buffer holding the result.
+static int cost_chain(const cbmv_params* p, Work& w, int64_t H, int64_t W, int D, const float* crossA,
+                      const float* crossB, int direction, float* cur, float* oth, float** result,
+                      cudaStream_t st) {
+  const int64_t HW = H * W;
+  // the separable form's supports, shared by a run of passes, in the first
+  // matcher volume (dead during the post; the SGM reuses it in between)
+  const bool masked = !p->exact_cbca && p->L1 - 1 <= kCbcaMaskMaxHalo;
+  uint32_t* masks = reinterpret_cast<uint32_t*>(w.vol[0]);
+  auto cbca = [&](const float* in, float* out) {
+    const int rows = p->cbca_rows == 16 ? 16 : 32;
+    if (p->exact_cbca)
+      return launch_cbca(crossA, crossB, in, H, W, D, CBMV_HWD, direction, out, st, p->L1 - 1);
+    if (masked) return launch_cbca_masked(masks, in, H, W, D, out, st, rows);
+    return launch_cbca_sep(crossA, crossB, in, H, W, D, direction, out, st, p->L1 - 1, rows);
+  };
+  if (masked && p->cbca_i1 > 0) RC(launch_cbca_mask_build(crossA, crossB, H, W, D, direction, masks, st));
+  for (int i = 0; i < p->cbca_i1; i++) {
+    RC(cbca(cur, oth));
+    float* t = cur; cur = oth; oth = t;
+  }
+  SgmParams sp{p->pi1, p->pi2, p->tau_so, p->alpha1, p->sgm_q1, p->sgm_q2, direction};
+  SgmGrad g{w.grad, w.grad + HW, w.grad + 2 * HW, w.grad + 3 * HW};
+  // the four direction volumes reuse the cost volumes, dead by now
+  const int64_t V = HW * D;
+  SgmOut so = w.f32 ? SgmOut{{(float*)w.vol[0], (float*)w.vol[1], (float*)w.vol[2], (float*)w.vol[3]}}
+                    : SgmOut{{(float*)w.vol[0], (float*)w.vol[0] + V, (float*)w.vol[1], (float*)w.vol[1] + V}};
+  for (int i = 0; i < p->sgm_i; i++) {
+    // out = ((L0 + L1 + L2) + L3) / 4   (test.py:379-383)
+    RC(launch_sgm4(g, cur, H, W, D, sp, so, st, p->sgm_prefetch));
+    RC(launch_sgm_combine(so, V, nullptr, 0.25f, oth, st));
+    float* t = cur; cur = oth; oth = t;
+  }
+  if (masked && p->cbca_i2 > 0) RC(launch_cbca_mask_build(crossA, crossB, H, W, D, direction, masks, st));
+  for (int i = 0; i < p->cbca_i2; i++) {
+    RC(cbca(cur, oth));
+    float* t = cur; cur = oth; oth = t;
+  }
+  *result = cur;
+  return CBMV_OK;
+}
+
+// Step 5 of the header comment on the float32 volume in w.volA; the
+// disparity lands in `disp`.  p->interpolate = 0: the _mem post
+// (test.py:341-449); 1: the _interp post (test.py:153-338), which first runs
+// the right view's chain on get_right_cost of the cost (its winner-take-all
+// is the right disparity) and after the left view's subpixel step marks
+// occlusions and mismatches (left-right check) and fills them
+// (interpolate_mismatch, then interpolate_occlusion) before the median.
 static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
                     int64_t H, int64_t W, int D, Work& w, float* disp) {
   cudaStream_t st = c->stream;
@@ -242,45 +304,25 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
   RC(launch_normalise(R, HW, w.mom + 2, w.imR, st));
   RC(launch_cross(w.imL, H, W, p->L1, p->tau1, w.crossL, st));
   RC(launch_cross(w.imR, H, W, p->L1, p->tau1, w.crossR, st));
-  float* cur = w.volA;
-  float* oth = w.volB;
-  // the separable form's supports, shared by a run of passes, in the first
-  // matcher volume (dead during the post; the SGM reuses it in between)
-  const bool masked = !p->exact_cbca && p->L1 - 1 <= kCbcaMaskMaxHalo;
-  uint32_t* masks = reinterpret_cast<uint32_t*>(w.vol[0]);
-  auto cbca = [&](const float* in, float* out) {
-    const int rows = p->cbca_rows == 16 ? 16 : 32;
-    if (p->exact_cbca)
-      return launch_cbca(w.crossL, w.crossR, in, H, W, D, CBMV_HWD, p->direction, out, st, p->L1 - 1);
-    if (masked) return launch_cbca_masked(masks, in, H, W, D, out, st, rows);
-    return launch_cbca_sep(w.crossL, w.crossR, in, H, W, D, p->direction, out, st, p->L1 - 1, rows);
-  };
-  if (masked && p->cbca_i1 > 0) RC(launch_cbca_mask_build(w.crossL, w.crossR, H, W, D, p->direction, masks, st));
-  for (int i = 0; i < p->cbca_i1; i++) {
-    RC(cbca(cur, oth));
-    float* t = cur; cur = oth; oth = t;
-  }
-  SgmParams sp{p->pi1, p->pi2, p->tau_so, p->alpha1, p->sgm_q1, p->sgm_q2, p->direction};
   SgmGrad g{w.grad, w.grad + HW, w.grad + 2 * HW, w.grad + 3 * HW};
-  // the four direction volumes reuse the cost volumes, dead by now
-  const int64_t V = HW * D;
-  SgmOut so = w.f32 ? SgmOut{{(float*)w.vol[0], (float*)w.vol[1], (float*)w.vol[2], (float*)w.vol[3]}}
-                    : SgmOut{{(float*)w.vol[0], (float*)w.vol[0] + V, (float*)w.vol[1], (float*)w.vol[1] + V}};
   if (p->sgm_i > 0) RC(launch_sgm_grad(w.imL, w.imR, H, W, &g, st));
-  for (int i = 0; i < p->sgm_i; i++) {
-    // out = ((L0 + L1 + L2) + L3) / 4   (test.py:379-383)
-    RC(launch_sgm4(g, cur, H, W, D, sp, so, st, p->sgm_prefetch));
-    RC(launch_sgm_combine(so, V, nullptr, 0.25f, oth, st));
-    float* t = cur; cur = oth; oth = t;
+  float* res = nullptr;
+  if (p->interpolate) {
+    // right view (test.py:154, 176-255): its cost, its chain, its argmin
+    RC(launch_right_cost_f32(w.volA, H, W, D, w.volC, st));
+    RC(cost_chain(p, w, H, W, D, w.crossR, w.crossL, -p->direction, w.volC, w.volB, &res, st));
+    RC(launch_wta_subpixel(res, H, W, D, w.dright, nullptr, st));
   }
-  if (masked && p->cbca_i2 > 0) RC(launch_cbca_mask_build(w.crossL, w.crossR, H, W, D, p->direction, masks, st));
-  for (int i = 0; i < p->cbca_i2; i++) {
-    RC(cbca(cur, oth));
-    float* t = cur; cur = oth; oth = t;
-  }
+  RC(cost_chain(p, w, H, W, D, w.crossL, w.crossR, p->direction, w.volA, w.volB, &res, st));
   float* d0 = w.dtmp;
   float* d1 = w.dtmp2;
-  RC(launch_wta_subpixel(cur, H, W, D, nullptr, d0, st));
+  RC(launch_wta_subpixel(res, H, W, D, nullptr, d0, st));
+  if (p->interpolate) {
+    // left-right check and fills (test.py:295-303, post.cu:717-869)
+    RC(launch_outlier(d0, w.dright, H, W, D, w.outlier, st));
+    RC(launch_mismatch(d0, w.outlier, H, W, d1, st));
+    RC(launch_occlusion(d1, w.outlier, H, W, d0, st));
+  }
   for (int i = 0; i < p->median_i; i++) {
     RC(launch_median(d0, H, W, p->median_w, d1, st));
     float* t = d0; d0 = d1; d1 = t;
@@ -301,9 +343,9 @@ static int run_front(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const 
                (long long)W, (long long)H);
   CBMV_REQUIRE(H <= 65535 && D >= 1 && D <= 1024, CBMV_ERANGE, "H must be <= 65535 and D in 1..1024");
   size_t bytes = 0;
-  carve(nullptr, H, W, D, &bytes, f32);
+  carve(nullptr, H, W, D, &bytes, f32, p->interpolate != 0);
   RC(ensure_workspace(c, bytes));
-  Work w = carve(c->ws, H, W, D, &bytes, f32);
+  Work w = carve(c->ws, H, W, D, &bytes, f32, p->interpolate != 0);
   cudaStream_t st = c->stream;
   CBMV_CUDA(cudaEventRecord(c->ev[0], st));
   RC(launch_census_desc(L, H, W, p->censw, w.descL, st));
@@ -393,9 +435,9 @@ extern "C" int cbmv_run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L
                (long long)W, (long long)H);
   CBMV_REQUIRE(H <= 65535 && D >= 1 && D <= 1024, CBMV_ERANGE, "H must be <= 65535 and D in 1..1024");
   size_t bytes = 0;
-  carve(nullptr, H, W, D, &bytes, true);
+  carve(nullptr, H, W, D, &bytes, true, p->interpolate != 0);
   RC(ensure_workspace(c, bytes));
-  Work w = carve(c->ws, H, W, D, &bytes, true);
+  Work w = carve(c->ws, H, W, D, &bytes, true, p->interpolate != 0);
   cudaStream_t st = c->stream;
   for (int i = 0; i < 4; i++) CBMV_CUDA(cudaEventRecord(c->ev[i], st));
   CBMV_CUDA(cudaMemcpyAsync(w.volA, cost, sizeof(float) * H * W * D, cudaMemcpyDeviceToDevice, st));
@@ -528,7 +570,7 @@ extern "C" int cbmv_batch_create(int n, const int64_t* H, const int64_t* W, cons
     size_t need = 0;
     for (int i : b->order[k]) {
       size_t bytes = 0;
-      carve(nullptr, H[i], W[i], D[i], &bytes, true);
+      carve(nullptr, H[i], W[i], D[i], &bytes, true, false);
       need = std::max(need, bytes);
     }
     if ((rc = ensure_workspace(c, need))) return fail(rc);
@@ -610,6 +652,7 @@ extern "C" int cbmv_batch_run_mlp(cbmv_batch* b, const cbmv_mlp* m, const cbmv_p
   cbmv_params def;
   p = params_or_default(p, &def);
   RC(check_params(p));
+  CBMV_REQUIRE(p->interpolate == 0, CBMV_EINVAL, "batches run the _mem post (interpolate = 0)");
   for (int i = 0; i < b->n; i++) CBMV_REQUIRE(L[i] && R[i] && disp[i], CBMV_EINVAL, "pair %d: null pointer", i);
   cudaStream_t user = as_stream(stream);
   bool same = b->exec && b->net == m && memcmp(&b->params, p, sizeof(cbmv_params)) == 0;

@@ -1035,6 +1035,24 @@ int launch_normalise(const uint8_t* img, int64_t n, double* mom, float* out, cud
   return check_launch("normalise");
 }
 
+// get_right_cost (featextract.cpp:115-152) of a float32 [H,W,D] volume:
+// R[y,x,d] = C[y,x+d,d] where x + d < W, else C[0,0,0] (test.py:154)
+__global__ void right_cost_f32_kernel(const float* __restrict__ in, int64_t H, int64_t W, int64_t D,
+                                      float* __restrict__ out) {
+  const float fill = in[0];
+  GRID_STRIDE(t, H * W * D) {
+    const int64_t d = t % D;
+    const int64_t p = t / D;
+    const int64_t x = p % W;
+    out[t] = x + d < W ? in[(p + d) * D + d] : fill;
+  }
+}
+
+int launch_right_cost_f32(const float* in, int64_t H, int64_t W, int D, float* out, cudaStream_t st) {
+  right_cost_f32_kernel<<<grid_for(H * W * D, kBlock), kBlock, 0, st>>>(in, H, W, D, out);
+  return check_launch("right_cost_f32");
+}
+
 int launch_outlier(const float* d0, const float* d1, int64_t H, int64_t W, int disp_max, float* out,
                    cudaStream_t st) {
   outlier_kernel<<<grid_for(H * W, kBlock), kBlock, 0, st>>>(d0, d1, H, W, disp_max, out);

@@ -50,6 +50,8 @@ int launch_median(const float* in, int64_t H, int64_t W, int k, float* out, cuda
 int launch_mean2d(const float* in, int64_t H, int64_t W, const float* kernel, int ks, float alpha2,
                   float* out, cudaStream_t st);
 int launch_normalise(const uint8_t* img, int64_t n, double* mom, float* out, cudaStream_t st);
+// get_right_cost of a float32 [H,W,D] volume (the _interp post's right view)
+int launch_right_cost_f32(const float* in, int64_t H, int64_t W, int D, float* out, cudaStream_t st);
 int launch_outlier(const float* d0, const float* d1, int64_t H, int64_t W, int disp_max, float* out,
                    cudaStream_t st);
 int launch_mismatch(const float* d0, const float* o, int64_t H, int64_t W, float* out,

@@ -64,6 +64,21 @@ class FlatForest:
         ends = np.append(self.roots[1:], self.n_nodes)
         return ends - self.roots
 
+    def node_depths(self):
+        """Depth of every node (root 0), indexed like `feature`: the number of
+        comparisons a walk makes before it stands on that node."""
+        depth = np.zeros(self.n_nodes, np.int32)
+        for t in range(self.n_trees):
+            base = int(self.roots[t])
+            stack = [0]
+            while stack:
+                n = stack.pop()
+                if self.left[base + n] >= 0:
+                    for c in (int(self.left[base + n]), int(self.right[base + n])):
+                        depth[base + c] = depth[base + n] + 1
+                        stack.append(c)
+        return depth
+
     @classmethod
     def from_sklearn(cls, rf):
         """Flatten a fitted binary RandomForestClassifier (classes [0, 1])."""

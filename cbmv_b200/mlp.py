@@ -6,10 +6,11 @@ forest (test.py:603-620) as the per-(pixel, d) matching-probability model.
     loss = tr.step(X, y, lr)                 # X [B,20] float32, y [B] (1 = correct)
     net = tr.params()
 
-Architecture 20 -> 128 -> 128 -> 64 -> 1 with ReLU and a sigmoid output
-P(correct); the matching cost handed to the post-processing is
-1 - P, as the reference hands it P(class 0) of the forest.  The parameter
-vector layout is documented in include/cbmv.h (cbmv_mlp_*).
+Architecture 20 -> 128 -> 128 -> 64 -> 1 with GELU (or ReLU) hidden
+layers and a sigmoid output P(correct); the matching cost handed to the
+post-processing is 1 - P, as the reference hands it P(class 0) of the
+forest.  The parameter vector layout is documented in include/cbmv.h
+(cbmv_mlp_*); the activation is stored beside it ("gelu" or "relu").
 """
 import ctypes
 
@@ -19,6 +20,7 @@ from . import _dev, _lib
 
 F = 20
 LAYERS = [(128, F), (128, 128), (64, 128)]
+ACTIVATIONS = {"relu": 0, "gelu": 1}  # CBMV_ACT_RELU, CBMV_ACT_GELU
 
 
 def num_params():
@@ -28,9 +30,12 @@ def num_params():
 class MlpParams:
     """Host-side parameter vector with named views."""
 
-    def __init__(self, vec):
+    def __init__(self, vec, activation="relu"):
         self.vec = np.ascontiguousarray(vec, np.float32)
         assert self.vec.size == num_params()
+        if activation not in ACTIVATIONS:
+            raise ValueError("activation must be one of %s" % sorted(ACTIVATIONS))
+        self.activation = activation
 
     def views(self):
         v, o, out = self.vec, 0, {}
@@ -45,26 +50,27 @@ class MlpParams:
         return out
 
     @classmethod
-    def init(cls, seed, cap, mu, sd):
+    def init(cls, seed, cap, mu, sd, activation="relu"):
         rng = np.random.default_rng(seed)
         vec = np.zeros(num_params(), np.float32)
-        p = cls(vec)
+        p = cls(vec, activation)
         v = p.views()
         v["cap"][:] = cap
         v["mu"][:] = mu
         v["inv_sd"][:] = 1.0 / np.maximum(sd, 1e-12)
         for (n, k), name in zip(LAYERS + [(1, 64)], ["W1", "W2", "W3", "w4"]):
-            # He-uniform into the ReLU layers, Glorot-uniform into the output
+            # He-uniform into the hidden layers, Glorot-uniform into the output
             lim = np.sqrt(6.0 / k) if n > 1 else np.sqrt(6.0 / (k + n))
             v[name][...] = rng.uniform(-lim, lim, v[name].shape).astype(np.float32)
         return p
 
     def save(self, path):
-        np.savez(path, params=self.vec)
+        np.savez(path, params=self.vec, activation=np.array(self.activation))
 
     @classmethod
     def load(cls, path):
-        return cls(np.load(path)["params"])
+        z = np.load(path)
+        return cls(z["params"], str(z["activation"]) if "activation" in z.files else "relu")
 
 
 def input_stats(X):
@@ -91,11 +97,13 @@ class MlpTrainer:
 
     def set_params(self, params):
         _lib.call("cbmv_mlp_set_params", self.h, params.vec.ctypes.data)
+        _lib.call("cbmv_mlp_set_activation", self.h, ACTIVATIONS[params.activation])
+        self.activation = params.activation
 
     def params(self):
         out = np.empty(num_params(), np.float32)
         _lib.call("cbmv_mlp_get_params", self.h, out.ctypes.data)
-        return MlpParams(out)
+        return MlpParams(out, self.activation)
 
     def step(self, X, y, lr, weight_decay=0.0):
         """X, y: torch CUDA float32 tensors [batch,20], [batch]; returns the
@@ -138,6 +146,8 @@ class GpuMlp:
         _lib.call("cbmv_mlp_create", 128, ctypes.byref(h))
         self.h = h
         _lib.call("cbmv_mlp_set_params", self.h, params.vec.ctypes.data)
+        _lib.call("cbmv_mlp_set_activation", self.h, ACTIVATIONS[params.activation])
+        self.activation = params.activation
 
     @classmethod
     def load(cls, path):

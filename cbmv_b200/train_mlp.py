@@ -1,6 +1,6 @@
 """Trains the learned classifier on samples the GPU pipeline emits.
 
-    python -m cbmv_b200.train_mlp --out mlp.npz [--pairs 200] [--per-pair 50000]
+    python -m cbmv_b200.train_mlp --out mlp.npz [--pairs 200] [--per-pair 50000] [--activation gelu]
 
 Training data (the GPU counterpart of the reference's train.py:100-273, with
 the MLP's labelling): seeded synthetic 694x554, D=128 pairs (seeds 2000..),
@@ -78,12 +78,12 @@ def emit(pairs, per_pair, seed0=TRAIN_SEED0, log=print, hard_frac=0.5):
     return torch.cat(Xs), torch.cat(ys)
 
 
-def train(X, y, epochs=4, batch=8192, lr=2e-3, wd=1e-4, seed=0, log=print):
+def train(X, y, epochs=4, batch=8192, lr=2e-3, wd=1e-4, seed=0, log=print, activation="gelu"):
     import torch
     n = X.shape[0]
     sub = X[torch.randperm(n, generator=torch.Generator().manual_seed(seed))[:1_000_000].cuda()]
     cap, mu, sd = input_stats(sub.cpu().numpy())
-    tr = MlpTrainer(MlpParams.init(seed, cap, mu, sd), batch=batch)
+    tr = MlpTrainer(MlpParams.init(seed, cap, mu, sd, activation), batch=batch)
     steps_per_epoch = n // batch
     total = epochs * steps_per_epoch
     g = torch.Generator(device="cuda").manual_seed(seed)
@@ -115,10 +115,11 @@ def main():
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--hard-frac", type=float, default=0.5)
+    ap.add_argument("--activation", choices=["gelu", "relu"], default="gelu")
     a = ap.parse_args()
     X, y = emit(a.pairs, a.per_pair, hard_frac=a.hard_frac)
     print("samples", tuple(X.shape), "positives", float(y.mean()), flush=True)
-    net = train(X, y, a.epochs, a.batch, a.lr)
+    net = train(X, y, a.epochs, a.batch, a.lr, activation=a.activation)
     net.save(a.out)
     print("saved", a.out, flush=True)
 

@@ -47,6 +47,8 @@ enum cbmv_status {
 };
 
 enum cbmv_dtype { CBMV_F32 = 0, CBMV_F64 = 1 };
+/* Hidden-layer activation of the learned classifier (cbmv_mlp_set_activation). */
+enum cbmv_activation { CBMV_ACT_RELU = 0, CBMV_ACT_GELU = 1 };
 enum cbmv_layout { CBMV_HWD = 0, CBMV_DHW = 1 };
 
 /* Message of the last failed call on this thread ("" if none). */
@@ -200,8 +202,9 @@ int cbmv_forest_predict(const cbmv_forest* f, const float* X, int64_t N, double*
 int cbmv_gemm_bf16(const uint16_t* A, const uint16_t* B, float* C, int64_t M, int64_t N, int64_t K,
                    int* status, void* stream);
 
-/* The classifier network: 20 -> 128 -> 128 -> 64 -> 1, ReLU, sigmoid
- * output = P(correct match); its matching cost is 1 - P.  Its
+/* The classifier network: 20 -> 128 -> 128 -> 64 -> 1, GELU or ReLU hidden
+ * layers (cbmv_mlp_set_activation; ReLU when created), sigmoid output =
+ * P(correct match); its matching cost is 1 - P.  Its
  * parameter vector (float32, cbmv_mlp_num_params() values) is, in order:
  * cap[20], mu[20], inv_sd[20] (input transform x' = (min(x,cap)-mu)*inv_sd),
  * W1[128x20], b1[128], W2[128x128], b2[128], W3[64x128], b3[64], w4[64],
@@ -226,6 +229,14 @@ int cbmv_mlp_gradients(cbmv_mlp* m, const float* X, const float* y, float* grads
                        void* stream);
 /* 0 while every tensor-core completion wait has succeeded. */
 int cbmv_mlp_status(const cbmv_mlp* m, int* status);
+/* Hidden-layer activation, CBMV_ACT_RELU or CBMV_ACT_GELU, used by training
+ * and by the fused inference of cbmv_run_mlp alike.  The GELU is x * Phi(x)
+ * evaluated as x * clamp(0.5 + x p(x^2), 0, 1) with a fixed degree-4
+ * polynomial p (float32, within 1.15e-3 of the exact erf form everywhere);
+ * it runs on the FMA pipe, not the special-function unit.  No counterpart in
+ * the reference (its classifier is the random forest). */
+int cbmv_mlp_set_activation(cbmv_mlp* m, int act);
+int cbmv_mlp_get_activation(const cbmv_mlp* m, int* act);
 
 /* ------------------------------------------------------------------ */
 /* cost optimisation -- post (post.cu), float32 on the device          */
@@ -309,6 +320,15 @@ typedef struct cbmv_params {
    * autotuner): rows per CBCA tile, 16 or 32 (0 = 32); SGM steps loaded
    * ahead, 1, 2 or 4 (0 = the default for the disparity count). */
   int cbca_rows, sgm_prefetch;
+  /* Post-processing chain, Testing.eval_prob's `interpolate` (main.py:70,
+   * test.py:143-149): 0 (default) the _mem post (test.py:341-449); 1 the
+   * _interp post (test.py:153-338): the right view's cost
+   * (get_right_cost) through the same chain with the arms swapped and the
+   * direction negated, then after the left view's subpixel step the
+   * left-right check (outlier_detection) and its fills
+   * (interpolate_mismatch, interpolate_occlusion).  Needs one more float32
+   * [H,W,D] volume of workspace.  cbmv_batch_run_mlp accepts 0 only. */
+  int interpolate;
 } cbmv_params;
 void cbmv_params_default(cbmv_params* p);
 

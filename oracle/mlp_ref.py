@@ -25,6 +25,46 @@ def relu(x):
     return np.maximum(x, 0.0), (x > 0).astype(np.float64)
 
 
+# the network's GELU polynomial (cbmv_b200/csrc/mlp_net.cuh, gelu_t):
+# x * clamp(0.5 + x p(x^2), 0, 1), p(u) = G[0] + G[1] u + ... + G[4] u^4
+G = np.array([3.9385697e-01, -5.9378225e-02, 6.5808324e-03, -3.9975342e-04, 9.9452836e-06], np.float32)
+
+
+def gelu(x):
+    """The network's GELU and its derivative, in float64."""
+    x = np.asarray(x, np.float64)
+    g = G.astype(np.float64)
+    u = x * x
+    p = (((g[4] * u + g[3]) * u + g[2]) * u + g[1]) * u + g[0]
+    dp = ((4 * g[4] * u + 3 * g[3]) * u + 2 * g[2]) * u + g[1]
+    qr = 0.5 + x * p
+    q = np.clip(qr, 0.0, 1.0)
+    inside = (qr > 0) & (qr < 1)
+    return x * q, q + np.where(inside, x * (p + 2 * u * dp), 0.0)
+
+
+def _fma32(a, b, c):
+    """float32 fused multiply-add: the exact product and sum (in float64,
+    exact for float32 operands up to one rounding of the sum) rounded once."""
+    return (np.float64(a) * np.float64(b) + np.float64(c)).astype(np.float32)
+
+
+def gelu_f32(x):
+    """The fused kernel's GELU of float32 accumulators, in its float32
+    operations and order (mlp_infer.cuh gelu_bf16x2)."""
+    x = np.asarray(x, np.float32)
+    u = (x * x).astype(np.float32)
+    p = _fma32(G[4], u, G[3])
+    p = _fma32(p, u, G[2])
+    p = _fma32(p, u, G[1])
+    p = _fma32(p, u, G[0])
+    q = np.clip(_fma32(x, p, np.float32(0.5)), 0, 1).astype(np.float32)
+    return (x * q).astype(np.float32)
+
+
+ACT = {"relu": relu, "gelu": gelu}
+
+
 def unpack(vec):
     v, o, out = np.asarray(vec, np.float64), 0, {}
     for name, size in [("cap", F), ("mu", F), ("inv_sd", F), ("W1", 128 * F), ("b1", 128),
@@ -38,24 +78,25 @@ def unpack(vec):
     return out
 
 
-def forward(vec, X):
+def forward(vec, X, act="relu"):
+    f_act = ACT[act]
     p = unpack(vec)
     # the input transform in float32, as the device computes it
     c32, m32, s32 = (np.float32(p[k]) for k in ("cap", "mu", "inv_sd"))
     X0 = bf16((np.minimum(np.asarray(X, np.float32), c32) - m32) * s32)
     S1 = X0 @ bf16(p["W1"]).T + p["b1"]
-    A1, d1 = relu(S1)
+    A1, d1 = f_act(S1)
     S2 = bf16(A1) @ bf16(p["W2"]).T + p["b2"]
-    A2, d2 = relu(S2)
+    A2, d2 = f_act(S2)
     S3 = bf16(A2) @ bf16(p["W3"]).T + p["b3"]
-    A3, d3 = relu(S3)
+    A3, d3 = f_act(S3)
     z = A3 @ p["w4"] + p["b4"][0]
     return dict(X0=X0, S1=S1, A1=A1, d1=d1, S2=S2, A2=A2, d2=d2, S3=S3, A3=A3, d3=d3, z=z, p=p)
 
 
-def loss_and_grads(vec, X, y):
+def loss_and_grads(vec, X, y, act="relu"):
     """Mean BCE and its gradients in parameter order (input transform excluded)."""
-    f = forward(vec, X)
+    f = forward(vec, X, act)
     p, z = f["p"], f["z"]
     y = np.asarray(y, np.float64)
     B = z.shape[0]
@@ -86,11 +127,18 @@ def split_bf16(x):
     return hi, bf16(x - np.float32(hi))
 
 
-def forward_fused(vec, X):
+def forward_fused(vec, X, act="relu"):
     """The network as the fused inference kernel evaluates it (test
     infrastructure): every bias (and w4) enters as its bf16 high + low
-    parts; hidden activations are ReLU rounded to bf16 (cvt.rn.relu); the
-    output layer runs on those bf16 activations.  Returns z."""
+    parts; hidden activations are ReLU or the float32 GELU of the float32
+    accumulator, rounded to bf16; the output layer runs on those bf16
+    activations.  Returns z."""
+    if act == "gelu":
+        def h(s):
+            return bf16(gelu_f32(np.asarray(s, np.float32)))
+    else:
+        def h(s):
+            return bf16(np.maximum(s, 0))
     p = unpack(vec)
     c32, m32, s32 = (np.float32(p[k]) for k in ("cap", "mu", "inv_sd"))
     X0 = bf16((np.minimum(np.asarray(X, np.float32), c32) - m32) * s32)
@@ -98,7 +146,7 @@ def forward_fused(vec, X):
     b2h, b2l = split_bf16(p["b2"])
     b3h, b3l = split_bf16(p["b3"])
     wh, wl = split_bf16(p["w4"])
-    A1 = bf16(np.maximum(X0 @ bf16(p["W1"]).T + (b1h + b1l), 0))
-    A2 = bf16(np.maximum(A1 @ bf16(p["W2"]).T + (b2h + b2l), 0))
-    A3 = bf16(np.maximum(A2 @ bf16(p["W3"]).T + (b3h + b3l), 0))
+    A1 = h(X0 @ bf16(p["W1"]).T + (b1h + b1l))
+    A2 = h(A1 @ bf16(p["W2"]).T + (b2h + b2l))
+    A3 = h(A2 @ bf16(p["W3"]).T + (b3h + b3l))
     return A3 @ (wh + wl) + p["b4"][0]

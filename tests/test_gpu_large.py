@@ -1,10 +1,12 @@
 """The larger workloads on the device.
 
 1482x994, D=256 (the plain path at a larger size, seed 1): census and
-SAD-on-Sobel volumes of the whole image bit-exact against the oracle run on a
-band of rows (every matcher is row-local within its window, so a band with a
-10-row margin reproduces the whole-image rows), and the forest's leaves and
-P(class 0) bit-exact on sampled (pixel, d) of that band.
+SAD-on-Sobel volumes bit-exact against the oracle on four bands of rows (the
+first rows, two interior bands and the last rows; every matcher is row-local
+within its window, so a band with a 10-row margin reproduces the
+whole-image rows), the forest's leaves and P(class 0) bit-exact on sampled
+(pixel, d) of one band, and the disparity of the fused path against the
+reference's own post.cu run on the same P(class 0) (>= 99.9 % within 0.5 px).
 
 2880x1988, D=400 (the full-resolution pair, seed 5; 2.29 G (pixel, d), past
 2^31): the learned path's four float32 volumes checked on rows near the
@@ -43,15 +45,18 @@ def test_1482x994_census_sad_and_forest_bitexact(gpu, oracle_cpu):
     L, R, _, _ = synth.pair_1482x994()
     H, W = L.shape
     D = 256
-    y0, rows = 700, 4
-    ref = _band_costs(oracle_cpu, L, R, y0, rows, D)
     l, r = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
     census = mtc.census(l, r, D, 11)                                   # [H,W,D] float64, device
-    assert torch.equal(census[y0:y0 + rows].cpu(), torch.from_numpy(ref[0]))
-    del census
     sad = mtc.sadsob(mtc.sobel(l), mtc.sobel(r), D, 5)                 # [D,H,W] float64, device
-    assert torch.equal(sad[:, y0:y0 + rows].permute(1, 2, 0).cpu(), torch.from_numpy(ref[2]))
-    del sad
+    bands = [(0, 4), (350, 4), (700, 4), (H - 4, 4)]
+    for b0, n in bands:
+        rb = _band_costs(oracle_cpu, L, R, b0, n, D)
+        assert torch.equal(census[b0:b0 + n].cpu(), torch.from_numpy(rb[0])), b0
+        assert torch.equal(sad[:, b0:b0 + n].permute(1, 2, 0).cpu(), torch.from_numpy(rb[2])), b0
+    del census, sad
+    torch.cuda.empty_cache()
+    y0, rows = 700, 4
+    ref = _band_costs(oracle_cpu, L, R, y0, rows, D)
     # forest: the fused path's P(class 0) and the leaves of sampled (pixel, d)
     flat = FlatForest.load(FOREST)
     gf = GpuForest(flat)
@@ -67,6 +72,39 @@ def test_1482x994_census_sad_and_forest_bitexact(gpu, oracle_cpu):
     assert np.array_equal(gf.apply(feats), leaves_ref)
     p0 = prob.reshape(-1)[band_idx].cpu().numpy()
     assert np.mean(p0 == p_ref.astype(np.float32)) > 0.9999
+
+
+def test_1482x994_disparity_against_reference_post(gpu):
+    """The fused forest path's disparity at 1482x994, D=256 against the
+    reference's post.cu (oracle/_ref, run on the GPU as shipped) driven by
+    Testing.__postprocessing_mem (test.py:341-449) on the same P(class 0)
+    volume (whose leaves and probabilities the test above holds to the
+    reference).  The reference's kernels need W >= H (its SGM state) and
+    read up to 48 pixels x D past the end of a volume in swap_axis_back when
+    H*W is not a multiple of 64: here 96 KB, inside the 2 MiB rounding of
+    its 3 GB allocation."""
+    from cbmv_b200 import synth
+    from cbmv_b200.forest_gpu import GpuForest
+    from cbmv_b200.pipeline import StereoPipeline
+    from oracle import glue, ref
+    assert ref.post_available(), "oracle/_ref/libcbmv_ref_post.so is not built"
+    L, R, _, _ = synth.pair_1482x994()
+    H, W = L.shape
+    D = 256
+    assert W >= H
+    pipe = StereoPipeline(GpuForest.load(FOREST))
+    prob = torch.empty((H, W, D), device="cuda")
+    disp = pipe.run_rf(L, R, D, prob_out=prob)
+    cost = prob.cpu().numpy().astype(np.float64)
+    del prob
+    pipe.close()
+    torch.cuda.empty_cache()
+    ref.post.InitCUDA()
+    imgl, imgr = glue.normalise_images(L, R)
+    d_ref = glue.postprocessing_mem(ref.post, imgl, imgr, cost, -1)
+    close = float(np.mean(np.abs(disp - d_ref) <= 0.5))
+    print("1482x994 D=256: fused forest path vs reference post.cu, within 0.5 px %.5f" % close)
+    assert close >= 0.999, close
 
 
 def test_2880x1988_learned_path_judged_by_forest(gpu, oracle_cpu):

@@ -32,7 +32,8 @@ def _toy(seed, n):
     return X, y
 
 
-def test_mlp_gradients_match_fp64_oracle(gpu):
+@pytest.mark.parametrize("act", ["relu", "gelu"])
+def test_mlp_gradients_match_fp64_oracle(gpu, act):
     """Device forward+backward (tcgen05 GEMMs, float32 accumulation) vs the
     float64 restatement rounding to bf16 at the same points: rel. error of
     every gradient block below 1e-3."""
@@ -40,7 +41,7 @@ def test_mlp_gradients_match_fp64_oracle(gpu):
     from oracle import mlp_ref
     X, y = _toy(0, 256)
     cap, mu, sd = input_stats(X)
-    net = MlpParams.init(1, cap, mu, sd)
+    net = MlpParams.init(1, cap, mu, sd, act)
     v = net.views()
     v["b1"][:] = 0.1
     v["b2"][:] = -0.05
@@ -50,7 +51,7 @@ def test_mlp_gradients_match_fp64_oracle(gpu):
     g, loss = tr.gradients(torch.from_numpy(X).cuda(), torch.from_numpy(y).cuda())
     torch.cuda.synchronize()
     assert tr.status() == 0
-    lref, gref, _ = mlp_ref.loss_and_grads(net.vec, X, y)
+    lref, gref, _ = mlp_ref.loss_and_grads(net.vec, X, y, act)
     assert abs(loss.item() - lref) < 1e-5 * max(1.0, abs(lref))
     g = g.cpu().numpy().astype(np.float64)
     sizes = [128 * 20, 128, 128 * 128, 128, 64 * 128, 64, 64, 1]
@@ -62,11 +63,12 @@ def test_mlp_gradients_match_fp64_oracle(gpu):
         o += s
 
 
-def test_mlp_training_reduces_loss(gpu):
+@pytest.mark.parametrize("act", ["relu", "gelu"])
+def test_mlp_training_reduces_loss(gpu, act):
     from cbmv_b200.mlp import MlpParams, MlpTrainer, input_stats
     X, y = _toy(1, 8192)
     cap, mu, sd = input_stats(X)
-    tr = MlpTrainer(MlpParams.init(2, cap, mu, sd), batch=1024)
+    tr = MlpTrainer(MlpParams.init(2, cap, mu, sd, act), batch=1024)
     Xt, yt = torch.from_numpy(X).cuda(), torch.from_numpy(y).cuda()
     losses = []
     for it in range(60):
@@ -76,9 +78,10 @@ def test_mlp_training_reduces_loss(gpu):
     assert np.mean(losses[-8:]) < 0.5 * np.mean(losses[:4]), losses
 
 
-def test_fused_inference_matches_oracle_forward(gpu, small_pair):
+@pytest.mark.parametrize("act", ["relu", "gelu"])
+def test_fused_inference_matches_oracle_forward(gpu, small_pair, act):
     """cbmv_run_mlp's matching cost (float32 features + four tcgen05 layers
-    fused, bf16 ReLU activations, biases as bf16 high + low parts) against
+    fused, bf16 ReLU or GELU activations, biases as bf16 high + low parts) against
     (a) the oracle's model of the same arithmetic: max 5e-3, mean 3e-4 on P
     -- the kernel's float32 features and accumulation order move a bf16
     rounding of an input or activation here and there; (b) the float64
@@ -94,7 +97,7 @@ def test_fused_inference_matches_oracle_forward(gpu, small_pair):
     idx = torch.arange(H * W * D, device="cuda")
     X = pipe.features_at(L, R, D, idx).cpu().numpy()
     cap, mu, sd = input_stats(X)
-    net = MlpParams.init(5, cap, mu, sd)
+    net = MlpParams.init(5, cap, mu, sd, act)
     v = net.views()
     v["b1"][:] = 0.05
     v["b2"][:] = np.linspace(-0.2, 0.2, 128)
@@ -106,11 +109,11 @@ def test_fused_inference_matches_oracle_forward(gpu, small_pair):
     torch.cuda.synchronize()
     assert g.status() == 0
     got = prob.cpu().numpy().reshape(-1)
-    model = 1.0 / (1.0 + np.exp(mlp_ref.forward_fused(net.vec, X)))
-    exact = 1.0 / (1.0 + np.exp(mlp_ref.forward(net.vec, X)["z"]))
+    model = 1.0 / (1.0 + np.exp(mlp_ref.forward_fused(net.vec, X, act)))
+    exact = 1.0 / (1.0 + np.exp(mlp_ref.forward(net.vec, X, act)["z"]))
     e_model, e_exact = np.abs(got - model), np.abs(got - exact)
-    print("fused vs model: max %.2e mean %.2e; vs float64 network: max %.2e mean %.2e"
-          % (e_model.max(), e_model.mean(), e_exact.max(), e_exact.mean()))
+    print("%s fused vs model: max %.2e mean %.2e; vs float64 network: max %.2e mean %.2e"
+          % (act, e_model.max(), e_model.mean(), e_exact.max(), e_exact.mean()))
     assert e_model.max() < 5e-3 and e_model.mean() < 3e-4, (e_model.max(), e_model.mean())
     assert e_exact.max() < 3e-2 and e_exact.mean() < 2e-3, (e_exact.max(), e_exact.mean())
 

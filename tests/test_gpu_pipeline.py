@@ -124,34 +124,41 @@ def test_saved_cost_volume_gives_the_same_disparity(gpu, small_pair, tmp_path):
         assert np.array_equal(pipe.run_post(L, R, cost), disp), fmt
 
 
-@pytest.mark.parametrize("W,H,D", [(97, 53, 37), (150, 64, 70)])
-def test_learned_path_matches_reference_path(gpu, oracle_cpu, W, H, D):
+NETS = {"gelu": "mlp_gelu_694x554.npz", "relu": "mlp_694x554.npz"}
+
+
+@pytest.mark.parametrize("net_kind", ["gelu", "relu"])
+@pytest.mark.parametrize("W,H,D", [(97, 53, 37), (150, 64, 70), (694, 64, 128)])
+def test_learned_path_matches_reference_path(gpu, oracle_cpu, W, H, D, net_kind):
     """The learned classifier's whole path at sizes off the tile grids (D not
-    a multiple of 32, widths not multiples of 8 or 16) against the
-    reference's test path restated over the oracle (test_model with the
-    network as its classifier, then eval_prob with the _mem post in the
-    reference's summation order): disparities within 0.5 px on >= 99.9 % of
-    pixels, the bar for final disparity maps (the device forms the features
-    in float32 and rounds activations to bf16; the network's cost differs
-    from the oracle's float64 model by ~1e-4 on average)."""
+    a multiple of 32, widths not multiples of 8 or 16) and at the headline
+    width and disparity count, for the GELU network of record and the ReLU
+    variant, against the reference's test path restated over the oracle
+    (test_model with the network as its classifier, in batches of 8 rows,
+    then eval_prob with the _mem post in the reference's summation order):
+    disparities within 0.5 px on >= 99.9 % of pixels, the bar for final
+    disparity maps (the device forms the features in float32 and rounds
+    activations to bf16; the oracle models that arithmetic from the
+    float64 features)."""
     import os
     from oracle import glue, mlp_ref
     from cbmv_b200 import synth
     from cbmv_b200.mlp import GpuMlp, MlpParams
     from cbmv_b200.pipeline import StereoPipeline
-    mlp = os.path.join(os.path.dirname(__file__), "golden", "mlp_694x554.npz")
+    mlp = os.path.join(os.path.dirname(__file__), "golden", NETS[net_kind])
     L, R, _, _ = synth.make_pair(seed=W + H + D, width=W, height=H, ndisp=D, planes=4, dmin=2, dmax=D - 4)
-    vec = MlpParams.load(mlp).vec
+    params = MlpParams.load(mlp)
+    assert params.activation == net_kind
 
     def predict(X):
-        p0 = 1.0 / (1.0 + np.exp(mlp_ref.forward_fused(vec, X)))
+        p0 = 1.0 / (1.0 + np.exp(mlp_ref.forward_fused(params.vec, X, params.activation)))
         return np.stack([p0, 1 - p0], 1)
 
-    proba = glue.test_model(oracle_cpu.mtc, oracle_cpu.fte, predict, L, R, D)
+    proba = glue.test_model(oracle_cpu.mtc, oracle_cpu.fte, predict, L, R, D, batch=8 * W)
     disp_ref = glue.eval_prob(oracle_cpu.post, oracle_cpu.fte, proba, L, R, D)
-    disp = StereoPipeline().run_mlp(GpuMlp.load(mlp), L, R, D)
+    disp = StereoPipeline().run_mlp(GpuMlp(params), L, R, D)
     close = np.mean(np.abs(disp - disp_ref) <= 0.5)
-    print("learned path %dx%d D=%d: within 0.5 px %.5f" % (W, H, D, close))
+    print("learned path (%s) %dx%d D=%d: within 0.5 px %.5f" % (net_kind, W, H, D, close))
     assert close >= 0.999, close
 
 

@@ -13,8 +13,9 @@ interpolate_occlusion) must equal the oracle bit for bit; mean2d within
 fused multiply-adds, the oracle multiplies and adds).  The whole `_mem`
 and `_interp` chains of test.py:153-449 (Testing.eval_prob) over the
 reference's post and over the oracle's agree to the same 1e-6; the
-package's fused post (cbmv_run_post, separable and reference-order CBCA)
-agrees with the reference's chain on >= 99.9 % of pixels within 0.5 px.
+package's fused post (cbmv_run_post, separable and reference-order CBCA,
+with interpolate = 0 and 1) agrees with the reference's chain on >= 99.9 %
+of pixels within 0.5 px.
 
 Inputs the reference's kernels need, checked here before they are called:
   * W >= H: sgm2 keeps its scan-line state in tmp[d * W + blockIdx.x]
@@ -262,14 +263,11 @@ def test_post_chains_equal_reference(gpu, oracle_cpu, case, forest_cost, interpo
                            check_outlier=_check_rays)
     d_orc = glue.eval_prob(oracle_cpu.post, oracle_cpu.fte, forest_cost, L, R, D, interpolate=interpolate)
     np.testing.assert_allclose(d_orc, d_ref, rtol=1e-6, atol=1e-6)
-    if interpolate:
-        return  # the fused device chain with the LR check: test_gpu_pipeline
     cost = forest_cost[:, 0].astype(np.float32).reshape(case["H"], case["W"], D)
     for exact in (0, 1):
-        prm = _lib.default_params()
-        prm.exact_cbca = exact
+        prm = _lib.default_params(exact_cbca=exact, interpolate=int(interpolate))
         disp = StereoPipeline(params=prm).run_post(L, R, cost)
         close = float(np.mean(np.abs(disp - d_ref) <= 0.5))
-        print("fused post (exact_cbca=%d) vs reference post.cu %dx%d D=%d: within 0.5 px %.5f"
-              % (exact, case["W"], case["H"], D, close))
+        print("fused %s post (exact_cbca=%d) vs reference post.cu %dx%d D=%d: within 0.5 px %.5f"
+              % ("_interp" if interpolate else "_mem", exact, case["W"], case["H"], D, close))
         assert close >= 0.999, close

@@ -2,9 +2,32 @@
 against central finite differences of its own loss (no bf16 rounding in
 this check), so the GPU gradient test rests on a verified backward pass."""
 import numpy as np
+import pytest
 
 
-def test_oracle_backward_matches_finite_differences(monkeypatch):
+def test_gelu_polynomial_against_erf():
+    """The network's GELU (x * clamp(0.5 + x p(x^2), 0, 1)) is within
+    1.15e-3 of x * Phi(x) everywhere, in its float32 evaluation and in the
+    float64 one, is exactly x / 0 in the tails, and its float64 derivative
+    matches central differences wherever the clamp is not active."""
+    from scipy.special import erf
+    from oracle import mlp_ref
+    x = np.linspace(-40, 40, 800001)
+    exact = 0.5 * x * (1 + erf(x / np.sqrt(2)))
+    g64, d64 = mlp_ref.gelu(x)
+    g32 = mlp_ref.gelu_f32(x.astype(np.float32)).astype(np.float64)
+    assert np.max(np.abs(g64 - exact)) <= 1.15e-3
+    assert np.max(np.abs(g32 - 0.5 * x.astype(np.float32) * (1 + erf(x.astype(np.float32) / np.sqrt(2))))) <= 1.15e-3
+    assert np.all(g64[x >= 3.5] == x[x >= 3.5]) and np.all(g64[x <= -3.5] == 0)
+    assert np.all(np.diff(g64[x >= 0]) > 0)  # increasing for x >= 0, as x Phi(x)
+    h = 1e-6
+    xm = np.linspace(-3.3, 3.3, 2001)
+    fd = (mlp_ref.gelu(xm + h)[0] - mlp_ref.gelu(xm - h)[0]) / (2 * h)
+    assert np.max(np.abs(fd - mlp_ref.gelu(xm)[1])) < 1e-6
+
+
+@pytest.mark.parametrize("act", ["relu", "gelu"])
+def test_oracle_backward_matches_finite_differences(monkeypatch, act):
     from oracle import mlp_ref
     monkeypatch.setattr(mlp_ref, "bf16", lambda x: np.asarray(x, np.float64))
     rng = np.random.default_rng(0)
@@ -18,17 +41,18 @@ def test_oracle_backward_matches_finite_differences(monkeypatch):
     vec[40:60] = 1.0    # inv_sd
     # the input transform runs in float32 even here; use exactly representable inputs
     X = X.astype(np.float32).astype(np.float64)
-    _, g, _ = mlp_ref.loss_and_grads(vec, X, y)
+    _, g, _ = mlp_ref.loss_and_grads(vec, X, y, act)
     for j in rng.choice(np.arange(60, vec.size), 40, replace=False):
         e = np.zeros_like(vec)
         e[j] = 1e-6
-        lp, _, _ = mlp_ref.loss_and_grads(vec + e, X, y)
-        lm, _, _ = mlp_ref.loss_and_grads(vec - e, X, y)
+        lp, _, _ = mlp_ref.loss_and_grads(vec + e, X, y, act)
+        lm, _, _ = mlp_ref.loss_and_grads(vec - e, X, y, act)
         fd = (lp - lm) / 2e-6
         assert abs(fd - g[j - 60]) < 1e-6 + 1e-4 * abs(fd), (j, fd, g[j - 60])
 
 
-def test_fused_model_close_to_float64_network():
+@pytest.mark.parametrize("act", ["relu", "gelu"])
+def test_fused_model_close_to_float64_network(act):
     """The oracle's model of the fused inference kernel (bf16 inputs,
     weights and ReLU activations, biases as bf16 high + low parts) stays
     within bf16 rounding of the float64 network, and the high + low split
@@ -39,8 +63,8 @@ def test_fused_model_close_to_float64_network():
     vec = np.concatenate([np.full(20, 1e9), np.zeros(20), np.ones(20),
                           rng.normal(scale=0.2, size=sum(sizes) - 60)])
     X = rng.normal(size=(500, 20)).astype(np.float32)
-    z_model = mlp_ref.forward_fused(vec, X)
-    z_exact = mlp_ref.forward(vec, X)["z"]
+    z_model = mlp_ref.forward_fused(vec, X, act)
+    z_exact = mlp_ref.forward(vec, X, act)["z"]
     scale = np.abs(z_exact).max()
     assert np.abs(z_model - z_exact).max() < 0.05 * scale
     assert np.abs(z_model - z_exact).mean() < 0.01 * scale

@@ -1,10 +1,14 @@
-"""The multi-GPU form of the benchmark, on CPU: world-size-2 gloo ranks each
-take their own pair (weak scaling by independent pairs, no data-path
-collective) and agree on the step time by a max-reduction, as bench.py does
-over NCCL."""
+"""The multi-GPU form of the batched path, on CPU: cbmv_b200.shard splits a
+batch of uneven pairs longest-processing-time first over the ranks, every
+rank runs its own pairs, and rank 0 gathers every pair's disparity map and
+per-pair numbers (world-size-2 gloo ranks here; bench.py --batch runs the
+same functions over NCCL).  The per-pair work of each rank is a small
+stand-in computed on the host (the census winner-take-all of the oracle),
+so that the gathered maps can be checked against a single-process run."""
 import os
 import socket
 
+import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
@@ -17,41 +21,70 @@ def _free_port():
     return p
 
 
+def _specs():
+    rng = np.random.default_rng(3)
+    return [dict(seed=100 + i, width=int(rng.integers(40, 90)), height=int(rng.integers(24, 40)),
+                 ndisp=int(rng.choice([8, 12, 16])), planes=3, dmin=1, dmax=6) for i in range(9)]
+
+
+def _disparity(spec):
+    """A stand-in for one pair's device path: census cost, first minimum."""
+    from cbmv_b200 import synth
+    from oracle import cpu
+    L, R, _, _ = synth.make_pair(**spec)
+    return np.argmin(cpu.mtc.census(L, R, spec["ndisp"], 11), axis=2).astype(np.float32)
+
+
 def _rank(rank, world, port, q):
-    import numpy as np
     import torch
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
-    dist.init_process_group("gloo", rank=rank, world_size=world)
-    from cbmv_b200 import synth
-    from oracle import cpu
-    # each rank its own pair (seed = rank), as bench.py shards pairs
-    L, R, _, _ = synth.make_pair(seed=rank, width=64, height=40, ndisp=12, planes=3, dmin=1, dmax=9)
-    c = cpu.mtc.census(L, R, 12, 11)
-    local_ms = float(10 + rank)  # stand-in for the rank's device time
-    t = torch.tensor([local_ms], dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    digest = torch.tensor([float(np.sum(c[c < 1e9]))], dtype=torch.float64)
-    got = [torch.zeros(1, dtype=torch.float64) for _ in range(world)]
-    dist.all_gather(got, digest)
-    q.put((rank, float(t.item()), [float(g.item()) for g in got]))
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    from cbmv_b200 import shard
+    specs = _specs()
+    shapes = [(s["height"], s["width"], s["ndisp"]) for s in specs]
+    assign = shard.lpt_assign(shard.pair_work(shapes), world)
+    mine = [torch.from_numpy(_disparity(specs[i])) for i in assign[rank]]
+    maps = shard.gather_maps(mine, assign, shapes)
+    lat = shard.gather_values([10.0 * i + rank for i in assign[rank]], assign, len(shapes))
+    t = shard.max_over_ranks(5.0 + rank)
+    q.put((rank, assign, None if maps is None else [m.numpy() for m in maps], lat.tolist(), t))
     dist.destroy_process_group()
 
 
-def test_two_ranks_shard_pairs_and_reduce_time():
+def test_lpt_assignment_properties():
+    from cbmv_b200 import shard
+    work = [5, 9, 1, 9, 3, 7, 2, 8]
+    a = shard.lpt_assign(work, 3)
+    assert sorted(i for r in a for i in r) == list(range(len(work)))  # each pair exactly once
+    assert a == shard.lpt_assign(work, 3)                             # deterministic
+    loads = [sum(work[i] for i in r) for r in a]
+    # LPT's bound: the largest load is within 4/3 of the best possible split
+    assert max(loads) <= 4 / 3 * max(max(work), sum(work) / 3)
+    assert a[0][0] == 1 and a[1][0] == 3   # the two longest pairs go first, to different ranks
+    assert shard.lpt_assign(work, 1) == [sorted(range(len(work)), key=lambda i: (-work[i], i))]
+    with pytest.raises(ValueError):
+        shard.lpt_assign(work, 0)
+
+
+def test_two_ranks_shard_gather_and_reduce():
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
     procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
     for p in procs:
         p.start()
-    res = [q.get(timeout=120) for _ in procs]
+    res = sorted([q.get(timeout=180) for _ in procs], key=lambda r: r[0])
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    res.sort()
-    # both ranks see the slower rank's time
-    assert res[0][1] == res[1][1] == 11.0
-    # and they processed different pairs
-    digests = res[0][2]
-    assert digests == res[1][2] and digests[0] != digests[1]
+    (r0, a0, maps, lat0, t0), (r1, a1, none, lat1, t1) = res
+    assert a0 == a1 and len(a0[0]) and len(a1[0])      # both ranks computed the same split
+    assert none is None and maps is not None
+    specs = _specs()
+    for i, s in enumerate(specs):                      # every map in its pair's slot
+        assert np.array_equal(maps[i], _disparity(s)), i
+    owner = {i: r for r in range(2) for i in a0[r]}
+    assert lat0 == lat1 == [10.0 * i + owner[i] for i in range(len(specs))]
+    assert t0 == t1 == 6.0                             # both see the slower rank's time
