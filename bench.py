@@ -272,7 +272,7 @@ def run_cbmv(a, ws, rank, local):
             d = disp.cpu().numpy()
             res[name] = {"ms": ms, "stage_ms": stage, "bad2_nonocc": evaluate.bad_x(d, gt, nonocc)}
         # the same architecture with ReLU hidden layers, a labelled variant
-        if a.classifier in ("both", "mlp") and os.path.exists(a.mlp_relu):
+        if a.classifier in ("both", "mlp") and os.path.exists(a.mlp_relu) and not a.device_only:
             net_r = GpuMlp.load(a.mlp_relu)
             ms_r, stage_r = _time_path(lambda: pipe.run_mlp(net_r, l, r, D0, disp_out=disp), a, ws, flush, st, pipe)
             relu = {"activation": net_r.activation, "ms_per_step": ms_r, "value": units * ws / (ms_r / 1e3),
@@ -280,11 +280,11 @@ def run_cbmv(a, ws, rank, local):
                     "classify_tflops": FLOPS_PER_UNIT_MLP * units / (stage_r["classify"] / 1e3) / 1e12}
             net_r.close()
     for name, (_, run_host) in paths.items():
-        res[name]["e2e_ms"] = _time_e2e(run_host, a, ws, flush, st)
+        res[name]["e2e_ms"] = _time_e2e(run_host, a, ws, flush, st) if not a.device_only else None
     # the _interp post (test.py:153-338: the right view's chain, the left-right
     # check and its fills) as a separate variant of the learned path
     interp = None
-    if net is not None and a.classifier in ("both", "mlp"):
+    if net is not None and a.classifier in ("both", "mlp") and not a.device_only:
         pipe_i = StereoPipeline(gf, params=_default_params(interpolate=1))
         ms_i, stage_i = _time_path(lambda: pipe_i.run_mlp(net, l, r, D0, disp_out=disp), a, ws, flush, st, pipe_i)
         hbm_i, _ = peaks()
@@ -300,7 +300,7 @@ def run_cbmv(a, ws, rank, local):
 
     # held-out accuracy: the RF judges the MLP (bad-2.0 on 20 seeded pairs)
     matched = None
-    if net is not None and a.classifier == "both" and not a.no_eval and rank == 0:
+    if net is not None and a.classifier == "both" and not a.no_eval and not a.device_only and rank == 0:
         ev = evaluate.compare_loaded(pipe, net, evaluate.HELD_OUT, D0)
         matched = {"seeds": "%d-%d" % (ev["seeds"][0], ev["seeds"][-1]), "bad2_rf": ev["bad2_rf"],
                    "bad2_mlp": ev["bad2_mlp"], "delta_pp": 100 * (ev["bad2_mlp"] - ev["bad2_rf"]),
@@ -321,7 +321,7 @@ def run_cbmv(a, ws, rank, local):
     if os.path.exists(tp):
         traffic = json.load(open(tp))
     if "rf" in res:
-        visits = forest_visits_per_unit(pipe, gf, flat, l, r)
+        visits = forest_visits_per_unit(pipe, gf, flat, l, r) if not a.device_only else 0.0
         t_rf = res["rf"]["stage_ms"]["classify"] / 1e3
         rf_achieved = visits * units / t_rf
         sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
@@ -373,9 +373,9 @@ def run_cbmv(a, ws, rank, local):
         "stage_ms": h["stage_ms"],
         "bad2_nonocc": h["bad2_nonocc"],
         "gpu_launches": launches * a.steps,
-        "e2e": {"value": units * ws / (h["e2e_ms"] / 1e3), "unit": "pixel·disparities/s",
-                "ms_per_step": h["e2e_ms"], "h2d_bytes_per_step": 2 * L.size,
-                "d2h_bytes_per_step": 4 * L.size},
+        "e2e": None if h["e2e_ms"] is None else {
+            "value": units * ws / (h["e2e_ms"] / 1e3), "unit": "pixel·disparities/s",
+            "ms_per_step": h["e2e_ms"], "h2d_bytes_per_step": 2 * L.size, "d2h_bytes_per_step": 4 * L.size},
         "roofline": roof,
         "whole_path": {"bound": "hbm", "bytes_per_unit": BYTES_PER_UNIT_PATH,
                        "achieved": BYTES_PER_UNIT_PATH * units / (h["ms"] / 1e3) / 1e9, "peak": hbm,
@@ -393,7 +393,7 @@ def run_cbmv(a, ws, rank, local):
         "relu_variant": relu,
         "clocks": clk.summary(),
     }
-    if rank == 0 and ws == 1 and not a.no_cpu_baseline and have_forest:
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline and not a.device_only and have_forest:
         line["cpu_baseline"] = cpu_baseline(flat, L, R, a)
     return line
 
@@ -634,6 +634,9 @@ def main():
     ap.add_argument("--cpu-rows", type=int, default=288,
                     help="rows of the cpu_baseline sample (288 = two of the reference's 144-row batches)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--device-only", action="store_true",
+                    help="time the device path(s) only: no e2e, variants, held-out evaluation or CPU "
+                         "baseline (short runs for profiler captures)")
     ap.add_argument("--height", type=int, default=H0,
                     help="rows of the pair (smaller cases for profiler captures; default 554)")
     a = ap.parse_args()

@@ -291,8 +291,8 @@ __global__ void stats_f32_left_kernel(VolsF vols, int64_t HW, int D, float2* __r
       for (int k = 0; k < 4; k++) {
         if (lane + 32 * k < nq) {
           const float tx = v[k].x - mn, ty = v[k].y - mn, tz = v[k].z - mn, tw = v[k].w - mn;
-          den += (expf(-(tx * tx) * inv_sigma) + expf(-(ty * ty) * inv_sigma)) +
-                 (expf(-(tz * tz) * inv_sigma) + expf(-(tw * tw) * inv_sigma));
+          den += (__expf(-(tx * tx) * inv_sigma) + __expf(-(ty * ty) * inv_sigma)) +
+                 (__expf(-(tz * tz) * inv_sigma) + __expf(-(tw * tw) * inv_sigma));
         }
       }
     } else {
@@ -300,7 +300,7 @@ __global__ void stats_f32_left_kernel(VolsF vols, int64_t HW, int D, float2* __r
       for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
       for (int d = lane; d < D; d += 32) {
         const float t = __ldg(r + d) - mn;
-        den += expf(-(t * t) * inv_sigma);
+        den += __expf(-(t * t) * inv_sigma);
       }
     }
     for (int o = 16; o; o >>= 1) den += __shfl_xor_sync(0xffffffffu, den, o);
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(RS_PIX) stats_f32_right_kernel(VolsF vols, int
         } else {
           for (int j = 0; j < nj; j++) {
             const float t = tile[(tid + j) * 33 + j] - mn;
-            den += expf(-(t * t) * inv_sigma);
+            den += __expf(-(t * t) * inv_sigma);
           }
         }
       }

@@ -25,7 +25,7 @@ pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FOREST = os.path.join(HERE, "golden", "forest_694x554.npz")
-MLP = os.path.join(HERE, "golden", "mlp_694x554.npz")
+MLP = os.path.join(HERE, "golden", "mlp_gelu_694x554.npz")
 
 
 def _band_costs(oracle_cpu, L, R, y0, rows, D, margin=10):

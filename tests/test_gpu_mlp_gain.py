@@ -3,8 +3,9 @@
 On held-out seeded 694x554, D=128 pairs, the same test path (matchers, 20
 features, classifier, MC-CNN `_mem` post) is run three ways:
 
-- with the trained bf16 MLP (tests/golden/mlp_694x554.npz, trained by
-  cbmv_b200/train_mlp.py on GPU-emitted samples of pairs 2000..2199);
+- with the trained bf16 GELU network (tests/golden/mlp_gelu_694x554.npz,
+  trained by cbmv_b200/train_mlp.py on GPU-emitted samples of pairs
+  2000..2199);
 - with the same network before training (its random initialisation, same
   input transform): the learned weights alone are what differs;
 - without a classifier: the post-processing applied to the normalised census
@@ -21,7 +22,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-MLP = os.path.join(HERE, "golden", "mlp_694x554.npz")
+MLP = os.path.join(HERE, "golden", "mlp_gelu_694x554.npz")
 SEEDS = [3000, 3001, 3002]
 
 
@@ -44,7 +45,7 @@ def test_trained_mlp_beats_untrained_and_no_classifier(gpu):
     from cbmv_b200.pipeline import StereoPipeline
     trained = MlpParams.load(MLP)
     v = trained.views()
-    untrained = MlpParams.init(0, v["cap"].copy(), v["mu"].copy(), 1.0 / v["inv_sd"])
+    untrained = MlpParams.init(0, v["cap"].copy(), v["mu"].copy(), 1.0 / v["inv_sd"], trained.activation)
     net_t, net_u = GpuMlp(trained), GpuMlp(untrained)
     pipe = StereoPipeline()
     rows = []
