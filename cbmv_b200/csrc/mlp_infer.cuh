@@ -34,7 +34,8 @@
 //            columns 32..63 of layer 1's weight tile) initialises the
 //            accumulator, the layer's MMAs accumulate onto it;
 //   hidden activations: ReLU and the bf16 rounding in one instruction
-//            (cvt.rn.relu.bf16x2.f32) per pair of columns;
+//            (cvt.rn.relu.bf16x2.f32) per pair of columns, or the GELU in
+//            packed bf16 arithmetic (seven instructions per pair);
 //   output   layer 4 is an MMA too: N = 16, rows 0 and 1 of its weight tile
 //            are the high and low bf16 parts of w4, z = D[0] + D[1] + b4,
 //            cost = 1 - sigmoid(z) = 1 / (1 + exp(z)).
@@ -98,20 +99,22 @@ __device__ __forceinline__ uint32_t relu_bf16x2(float a, float b) {
   return r;
 }
 
-// GELU (gelu_t above) of two float32 pre-activations as a packed bf16 pair
-// (low = a): the polynomial on both lanes at once with the packed float32
-// multiply / FMA, the saturating FMA per lane; the same float32 operations
-// in the same order as gelu_t, so training and inference agree bit for bit.
+// GELU (gelu_t) of two float32 pre-activations as a packed bf16 pair (low =
+// a): the same bf16 operations as gelu_t, both lanes per instruction --
+// seven instructions per pair, the conversion included.
 __device__ __forceinline__ uint32_t gelu_bf16x2(float a, float b) {
-  const float2 x = make_float2(a, b);
-  const float2 u = __fmul2_rn(x, x);
-  float2 p = __ffma2_rn(make_float2(kG4, kG4), u, make_float2(kG3, kG3));
-  p = __ffma2_rn(p, u, make_float2(kG2, kG2));
-  p = __ffma2_rn(p, u, make_float2(kG1, kG1));
-  p = __ffma2_rn(p, u, make_float2(kG0, kG0));
-  const float2 q = make_float2(fma_sat(x.x, p.x, 0.5f), fma_sat(x.y, p.y, 0.5f));
-  const float2 g = __fmul2_rn(x, q);
-  return pack_bf16x2(g.x, g.y);
+  const __nv_bfloat162 g0 = __bfloat162bfloat162(bf16_bits(kG0Bits)),
+                       g1 = __bfloat162bfloat162(bf16_bits(kG1Bits)),
+                       g2 = __bfloat162bfloat162(bf16_bits(kG2Bits));
+  const __nv_bfloat162 half = __float2bfloat162_rn(0.5f), one = __float2bfloat162_rn(1.0f);
+  const __nv_bfloat162 x = __floats2bfloat162_rn(a, b);
+  const __nv_bfloat162 u = __hmul2(x, x);
+  __nv_bfloat162 p = __hfma2(g2, u, g1);
+  p = __hfma2(p, u, g0);
+  __nv_bfloat162 q = __hfma2_relu(x, p, half);
+  q = __hmin2(q, one);
+  const __nv_bfloat162 g = __hmul2(x, q);
+  return *reinterpret_cast<const uint32_t*>(&g);
 }
 
 // ratio and likelihood of cost c (featextract.cpp:333 and :440) in float32
@@ -281,12 +284,12 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   unsigned char* sTiles = sOne + kSmOne;
   __shared__ float4 s_nrm[kF];  // per feature column: cap, mu, inv_sd
   __shared__ float s_b4;
-  __shared__ uint64_t bars[2 * kGroups];
+  __shared__ uint64_t bars[kGroups];
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, g = tid / kGroupThreads, row = tid % kGroupThreads, wq = row >> 5;
 
   if (tid < 32) umma::tmem_alloc(&tmem_base, 128 * kGroups);
-  if (tid < 2 * kGroups) umma::mbar_init(&bars[tid], 1);
+  if (tid < kGroups) umma::mbar_init(&bars[tid], 1);
   stage_inference_weights(P, sW1, sW2, sW3, sW4, sOne);
   for (int i = tid; i < kF; i += kInfThreads) s_nrm[i] = make_float4(P[i], P[kF + i], P[2 * kF + i], 0.0f);
   if (tid == 0) s_b4 = P[kOffB4];
@@ -298,12 +301,11 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   unsigned char* sA = sTiles + g * kSmTile;
   unsigned char* rowp = sA + (row >> 3) * 1024 + (row & 7) * 128;
   const int r7s = (row & 7) << 4;
-  uint64_t* bar0 = &bars[2 * g];
-  uint64_t* bar1 = &bars[2 * g + 1];
+  uint64_t* bar0 = &bars[g];
   const uint32_t tacc = tmem_base + (uint32_t)(g * 128);
   const uint32_t tlane = tacc + ((uint32_t)(wq * 32) << 16);
   const bool leader = row == 0;
-  constexpr uint32_t id64 = umma::idesc_bf16(128, 64),
+  constexpr uint32_t id128 = umma::idesc_bf16(128, 128), id64 = umma::idesc_bf16(128, 64),
                      id16 = umma::idesc_bf16(128, 16);
   // operand descriptors, formed where the leader issues (keeps them out of the other threads' registers)
 #define DESC(ptr) umma::sw128_desc(umma::smem_u32(ptr))
@@ -321,16 +323,9 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   const int64_t sp = step / D;
   const int sd = (int)(step - sp * D);
   const int64_t sx = sp % W;
-  // bar0 takes every layer's (first half's) commit, bar1 the second halves
-  // of layers 1 and 2; `last_*` is the latest commit (the one whose
-  // completion implies all of the group's earlier MMAs have completed)
-  uint32_t ph0 = 0, ph1 = 0;
-  uint32_t last = 0;  // latest commit: barrier (bit 1) and its phase (bit 0)
+  // the group's MMAs are committed to bar0, one phase per layer
+  uint32_t ph0 = 0;
   bool ok = true;
-  auto commit = [&](int which, uint32_t ph) {
-    umma::mma_commit(which ? bar1 : bar0);
-    last = ((uint32_t)which << 1) | ph;
-  };
   // the leader polls, the group learns the result at its named barrier
   auto wait = [&](uint64_t* b, uint32_t& ph) {
     const bool r = group_all(g, leader ? umma::mbar_wait(b, ph, kWaitLimit) : true);
@@ -344,16 +339,13 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     group_sync(g);
     umma::tc_fence_after();
   };
-  // operand tiles: W rows 64..127 start 8 row-groups (8 KB) into each atom
-  constexpr int kHalf = 64 * 128;
 
   FeatIn in;
   load_feat_in(fv, statsf, HW, N, t, p, d, x, in);
   for (; tile < tiles; tile += tstride) {
-    // 1. the 20 features of sample t -> row of X0, in the tile's second atom
-    //    (the first receives layer 1's first half while the second half's
-    //    MMAs still read X0): columns 0..19 in the reference's order, 20 and
-    //    21 the bias inputs, 22..31 zero
+    // 1. the 20 features of sample t -> row of X0, in the tile's second
+    //    atom: columns 0..19 in the reference's order, 20 and 21 the bias
+    //    inputs, 22..31 zero
     {
       float f[20];
       features_f32(in, f);
@@ -383,47 +375,28 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     if (x >= W) x -= W;
     if (tile + tstride < tiles) load_feat_in(fv, statsf, HW, N, t, p, d, x, in);
     handoff();
-    // 2. layer 1 (K = 32) as two N = 64 halves -> accumulator columns 0..63, 64..127
+    // 2. layer 1 (K = 32) -> accumulator columns 0..127
     if (leader) {
-      const uint64_t dX = DESC(sA + 128 * 128), dW1 = DESC(sW1), dW1h = DESC(sW1 + kHalf);
-      umma::mma_bf16(tacc, dX, dW1, id64, false);
-      umma::mma_bf16(tacc, dX + 2, dW1 + 2, id64, true);
-      commit(0, ph0);
-      umma::mma_bf16(tacc + 64, dX, dW1h, id64, false);
-      umma::mma_bf16(tacc + 64, dX + 2, dW1h + 2, id64, true);
-      commit(1, ph1);
+      const uint64_t dX = DESC(sA + 128 * 128), dW1 = DESC(sW1);
+      umma::mma_bf16(tacc, dX, dW1, id128, false);
+      umma::mma_bf16(tacc, dX + 2, dW1 + 2, id128, true);
+      umma::mma_commit(bar0);
     }
     if (!(ok = wait(bar0, ph0))) break;
-    epilogue_hidden<0, 64, ACT>(tlane, rowp, r7s);  // -> atom 0 (X0 in atom 1 untouched)
-    if (!(ok = wait(bar1, ph1))) break;
-    epilogue_hidden<64, 64, ACT>(tlane, rowp, r7s);  // -> atom 1, X0 read by now
+    epilogue_hidden<0, 128, ACT>(tlane, rowp, r7s);
     handoff();
-    // 3. layer 2 (K = 128) onto the bias b2, as two N = 64 halves ordered so
-    //    that the first completion also frees the tile's first atom:
-    //    [bias, K 0..63 of both halves, K 64..127 of the first] -> bar0,
-    //    [K 64..127 of the second] -> bar1
+    // 3. layer 2 (K = 128) onto the bias b2
     if (leader) {
-      const uint64_t dA0 = DESC(sA), dA1 = DESC(sA + 128 * 128);
-      const uint64_t dW20 = DESC(sW2), dW21 = DESC(sW2 + 128 * 128);
-      const uint64_t dW20h = DESC(sW2 + kHalf), dW21h = DESC(sW2 + 128 * 128 + kHalf);
-      const uint64_t dOne = DESC(sOne);
-      umma::mma_bf16(tacc, dOne, DESC(sW1) + 2 * (kColB2 / 16), id64, false);
-      umma::mma_bf16(tacc + 64, dOne, DESC(sW1 + kHalf) + 2 * (kColB2 / 16), id64, false);
+      const uint64_t dA0 = DESC(sA), dA1 = DESC(sA + 128 * 128), dW20 = DESC(sW2), dW21 = DESC(sW2 + 128 * 128);
+      umma::mma_bf16(tacc, DESC(sOne), DESC(sW1) + 2 * (kColB2 / 16), id128, false);
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA0 + 2 * kk, dW20 + 2 * kk, id64, true);
+      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA0 + 2 * kk, dW20 + 2 * kk, id128, true);
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc + 64, dA0 + 2 * kk, dW20h + 2 * kk, id64, true);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA1 + 2 * kk, dW21 + 2 * kk, id64, true);
-      commit(0, ph0);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc + 64, dA1 + 2 * kk, dW21h + 2 * kk, id64, true);
-      commit(1, ph1);
+      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA1 + 2 * kk, dW21 + 2 * kk, id128, true);
+      umma::mma_commit(bar0);
     }
     if (!(ok = wait(bar0, ph0))) break;
-    epilogue_hidden<0, 64, ACT>(tlane, rowp, r7s);   // -> atom 0, no longer read
-    if (!(ok = wait(bar1, ph1))) break;
-    epilogue_hidden<64, 64, ACT>(tlane, rowp, r7s);  // -> atom 1
+    epilogue_hidden<0, 128, ACT>(tlane, rowp, r7s);
     handoff();
     // 4. layer 3 (N = 64) onto the bias b3
     if (leader) {
@@ -433,7 +406,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA0 + 2 * kk, dW30 + 2 * kk, id64, true);
 #pragma unroll
       for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA1 + 2 * kk, dW31 + 2 * kk, id64, true);
-      commit(0, ph0);
+      umma::mma_commit(bar0);
     }
     if (!(ok = wait(bar0, ph0))) break;
     epilogue_hidden<0, 64, ACT>(tlane, rowp, r7s);
@@ -443,7 +416,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       const uint64_t dA0 = DESC(sA), dW4 = DESC(sW4);
 #pragma unroll
       for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc + 64, dA0 + 2 * kk, dW4 + 2 * kk, id16, kk > 0);
-      commit(0, ph0);
+      umma::mma_commit(bar0);
     }
     if (!(ok = wait(bar0, ph0))) break;
     {
@@ -459,9 +432,10 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   }
   if (!ok && leader) {
     // a wait gave up: record it, then let the group's MMAs still in flight
-    // finish (bounded: the latest commit's phase) before the memory is freed
+    // finish (bounded: the phase that was waited for) before the memory is
+    // freed
     atomicExch(status, 1);
-    umma::mbar_wait((last >> 1) ? bar1 : bar0, last & 1u, kWaitLimit);
+    umma::mbar_wait(bar0, ph0 ^ 1u, kWaitLimit);
   }
   umma::tc_fence_before();
   __syncthreads();

@@ -26,37 +26,42 @@ __device__ __forceinline__ float relu_t(float x, float* drelu) {
 }
 
 // The network's GELU, x * Phi(x) with Phi the standard normal CDF, computed
-// without the special-function unit: Phi(x) ~ sat(0.5 + x * p(x^2)), sat =
-// clamp to [0, 1], p(u) = G0 + G1 u + G2 u^2 + G3 u^3 + G4 u^4.  The
-// coefficients are a minimax fit of x * (0.5 + x p(x^2)) to x * Phi(x) on
-// [0, 3.45] by linear programming, constrained so that 0.5 + x p(x^2) >= 1
-// for x >= 3.45 (where Phi > 0.9997) and, by symmetry, <= 0 for x <= -3.45:
-// the saturation then makes the function exact to x (or 0) in the tails.
-// In float32, in exactly the order below, |gelu(x) - x Phi(x)| <= 1.15e-3
-// for every x (the activation is rounded to bf16 next, a relative 2^-9).
-// Training and the fused inference kernel evaluate it identically (the
-// inference kernel two lanes at a time with the packed float32 FMA).
-constexpr float kG0 = 3.9385697e-01f, kG1 = -5.9378225e-02f, kG2 = 6.5808324e-03f,
-                kG3 = -3.9975342e-04f, kG4 = 9.9452836e-06f;
+// in bfloat16 arithmetic (the activation is stored as bf16 anyway), on the
+// packed half-precision FMA pipe, without the special-function unit:
+//   x <- bf16(x);  u = x * x;  p = G2 u + G1;  p = p u + G0;
+//   q = min(max(x p + 0.5, 0), 1);  gelu = x * q
+// every operation one bf16 rounding (round to nearest even), q ~ Phi(x).
+// G0..G2 (bf16) are a minimax fit of x * clamp(0.5 + x (G0 + G1 x^2 + G2 x^4),
+// 0, 1) to x * Phi(x), then the bf16 coefficients searched for the smallest
+// error of this bf16 evaluation: over every bf16 x, |gelu(x) - x Phi(x)|
+// <= 1.21e-2 (rounding x Phi(x) itself to bf16 costs up to 7.8e-3); the
+// clamp makes it x for x >= 3.5 and 0 (-0) for x <= -3.5.  Training and
+// the fused inference kernel (two lanes at a time) evaluate it identically.
+constexpr uint16_t kG0Bits = 0x3ebf, kG1Bits = 0xbd30, kG2Bits = 0x3b1c;  // 0.373046875, -0.04296875, 0.00238037109375
 
-__device__ __forceinline__ float fma_sat(float a, float b, float c) {
-  float r;
-  asm("fma.rn.sat.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-  return r;
-}
+__device__ __forceinline__ __nv_bfloat16 bf16_bits(uint16_t b) { return __ushort_as_bfloat16(b); }
 
-// GELU and its derivative: Phi~ + x Phi~' where 0 < 0.5 + x p < 1, else Phi~
+// GELU of x (float32 in, its bf16 rounding used) and, for the backward pass,
+// the derivative of the smooth function it approximates at that point:
+// q + x (p + 2 u p'(u)) where 0 < x p + 0.5 < 1, else q (0 or 1), in float32.
 __device__ __forceinline__ float gelu_t(float x, float* dgelu) {
-  const float u = x * x;
-  const float p = fmaf(fmaf(fmaf(fmaf(kG4, u, kG3), u, kG2), u, kG1), u, kG0);
-  const float q = fma_sat(x, p, 0.5f);
+  const __nv_bfloat16 xb = __float2bfloat16_rn(x);
+  const __nv_bfloat16 u = __hmul(xb, xb);
+  __nv_bfloat16 p = __hfma(bf16_bits(kG2Bits), u, bf16_bits(kG1Bits));
+  p = __hfma(p, u, bf16_bits(kG0Bits));
+  __nv_bfloat16 q = __hfma_relu(xb, p, __float2bfloat16_rn(0.5f));
+  q = __hmin(q, __float2bfloat16_rn(1.0f));
+  const float g = __bfloat162float(__hmul(xb, q));
   if (dgelu) {
-    const float qr = fmaf(x, p, 0.5f);
-    const float dp = fmaf(fmaf(fmaf(4.0f * kG4, u, 3.0f * kG3), u, 2.0f * kG2), u, kG1);  // p'(u)
-    const float dq = fmaf(2.0f * u, dp, p);                                                 // d(x p(x^2))/dx
-    *dgelu = (qr > 0.0f && qr < 1.0f) ? fmaf(x, dq, q) : q;
+    const float xf = __bfloat162float(xb), uf = xf * xf;
+    const float g0 = __bfloat162float(bf16_bits(kG0Bits)), g1 = __bfloat162float(bf16_bits(kG1Bits)),
+                g2 = __bfloat162float(bf16_bits(kG2Bits));
+    const float pf = fmaf(fmaf(g2, uf, g1), uf, g0);
+    const float qr = fmaf(xf, pf, 0.5f);
+    const float dq = fmaf(2.0f * uf, fmaf(2.0f * g2, uf, g1), pf);  // d(x p(x^2))/dx
+    *dgelu = qr <= 0.0f ? 0.0f : qr >= 1.0f ? 1.0f : fmaf(xf, dq, qr);
   }
-  return x * q;
+  return g;
 }
 
 // the network's activation (cbmv_mlp_set_activation) and its derivative

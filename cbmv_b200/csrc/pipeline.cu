@@ -275,7 +275,8 @@ static int cost_chain(const cbmv_params* p, Work& w, int64_t H, int64_t W, int D
                     : SgmOut{{(float*)w.vol[0], (float*)w.vol[0] + V, (float*)w.vol[1], (float*)w.vol[1] + V}};
   for (int i = 0; i < p->sgm_i; i++) {
     // out = ((L0 + L1 + L2) + L3) / 4   (test.py:379-383)
-    RC(launch_sgm_mean(g, cur, H, W, D, sp, so, oth, st, p->sgm_prefetch));
+    RC(launch_sgm4(g, cur, H, W, D, sp, so, st, p->sgm_prefetch));
+    RC(launch_sgm_combine(so, V, nullptr, 0.25f, oth, st));
     float* t = cur; cur = oth; oth = t;
   }
   if (masked && p->cbca_i2 > 0) RC(launch_cbca_mask_build(crossA, crossB, H, W, D, direction, masks, st));

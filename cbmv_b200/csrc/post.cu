@@ -81,16 +81,9 @@ __global__ void grad_kernel(const float* __restrict__ img, int64_t H, int64_t W,
 // lane = d (mod 32), KPL disparities per lane.  The scan runs inside the
 // kernel; the step's costs, D1 and the per-d D2 do not depend on the
 // recursion and are loaded PF steps ahead from a register ring.
-//
-// COMB: the scan of the last direction (3) also forms the mean of the four
-// directions, ((L0 + L1) + L2 + L3) / 4 in that order (test.py:379-383, the
-// order sgm_combine_kernel adds them in), from the three direction volumes
-// written by an earlier launch (`prior`), loaded ahead with the step's
-// costs, and writes it to `out` instead of its own path costs.
-template <int KPL, int PF, bool FULL, bool COMB>
+template <int KPL, int PF, bool FULL>
 __device__ __noinline__ void sgm_scan(const SgmGrad& g, const float* __restrict__ in, int H, int W, int D,
-                                      const SgmParams& sp, int line, float* __restrict__ out, const int DIR,
-                                      const SgmOut& prior) {
+                                      const SgmParams& sp, int line, float* __restrict__ out, const int DIR) {
   const int lane = threadIdx.x & 31;
   const int nsteps = DIR <= 1 ? W : H;
   const int dx = DIR == 0 ? 1 : DIR == 1 ? -1 : 0;
@@ -126,7 +119,6 @@ __device__ __noinline__ void sgm_scan(const SgmGrad& g, const float* __restrict_
 
   struct Step {
     float cost[KPL], d2[KPL];
-    float part[COMB ? KPL : 1];  // COMB: (L0 + L1) + L2 of the step's pixel
     float d1;
   };
   auto load = [&](int step, Step& st) {
@@ -141,10 +133,6 @@ __device__ __noinline__ void sgm_scan(const SgmGrad& g, const float* __restrict_
       st.cost[k] = dk ? src[32 * k] : inf;
       const bool inside = (unsigned)(xl + 32 * k * s) < xspan;
       st.d2[k] = (step > 0 && dk && inside) ? grp[32 * k * s] : 10.0f;
-      if constexpr (COMB) {
-        const int64_t i = ind2 * D + lane + 32 * k;
-        st.part[k] = dk ? (prior.dir[0][i] + prior.dir[1][i]) + prior.dir[2][i] : 0.0f;
-      }
     }
   };
   float prev[KPL];
@@ -195,34 +183,32 @@ __device__ __noinline__ void sgm_scan(const SgmGrad& g, const float* __restrict_
       float* dst = out + (p0 + step * pstep) * D + lane;
 #pragma unroll
       for (int k = 0; k < KPL; k++) {
-        if constexpr (COMB) {
-          if (FULL || lane + 32 * k < D) dst[32 * k] = (cur.part[k] + L[k]) * 0.25f;
-        } else {
-          if (FULL || lane + 32 * k < D) dst[32 * k] = L[k];
-        }
+        if (FULL || lane + 32 * k < D) dst[32 * k] = L[k];
         prev[k] = L[k];
       }
     }
   }
 }
 
-// One warp per scan line of the directions dir_first .. dir_last (lines of
-// direction 0 and 1: H each, of 2 and 3: W each), each writing its path
-// costs to o.dir[dir]; COMB (direction 3 alone): the mean of the four into
-// `comb_out` instead.
-template <int KPL, int PF, bool FULL, bool COMB>
+template <int KPL, int PF, bool FULL>
 __global__ void __launch_bounds__(128) sgm4_kernel(SgmGrad g, const float* __restrict__ in, int H,
-                                                   int W, int D, SgmParams sp, SgmOut o, int dir_first,
-                                                   int dir_last, float* comb_out) {
-  int rest = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  for (int dir = dir_first; dir <= dir_last; dir++) {
-    const int lines = dir <= 1 ? H : W;
-    if (rest < lines) {
-      sgm_scan<KPL, PF, FULL, COMB>(g, in, H, W, D, sp, rest, COMB ? comb_out : o.dir[dir], dir, o);
-      return;
-    }
-    rest -= lines;
+                                                   int W, int D, SgmParams sp, SgmOut o) {
+  const int warp = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  int dir = -1, line = 0;
+  if (warp < H) {
+    dir = 0;
+    line = warp;
+  } else if (warp < 2 * H) {
+    dir = 1;
+    line = warp - H;
+  } else if (warp < 2 * H + W) {
+    dir = 2;
+    line = warp - 2 * H;
+  } else if (warp < 2 * H + 2 * W) {
+    dir = 3;
+    line = warp - 2 * H - W;
   }
+  if (dir >= 0) sgm_scan<KPL, PF, FULL>(g, in, H, W, D, sp, line, o.dir[dir], dir);
 }
 
 // out = base + (((L0 + L1) + L2) + L3) * scale over n elements (base may be
@@ -928,49 +914,35 @@ int launch_sgm_grad(const float* imL, const float* imR, int64_t H, int64_t W, Sg
 // prefetch keeps the scan at ~80 registers, measured faster than deeper
 // rings, whose registers cost more occupancy than they hide latency).
 // The results do not depend on it.
-template <int KPL, bool COMB>
+template <int KPL>
 static void sgm4_launch(const SgmGrad& g, const float* in, int H, int W, int D, const SgmParams& sp,
-                        const SgmOut& o, cudaStream_t st, int prefetch, int d0, int d1, float* comb_out) {
-  int lines = 0;
-  for (int dir = d0; dir <= d1; dir++) lines += dir <= 1 ? H : W;
+                        const SgmOut& o, cudaStream_t st, int prefetch) {
+  const int lines = 2 * H + 2 * W;
   const int blocks = (lines * 32 + 127) / 128;
   constexpr int PF0 = KPL <= 2 ? 4 : KPL <= 8 ? 2 : 1;
   const int pf = prefetch > 0 && KPL <= 8 ? prefetch : PF0;
   if (D == 32 * KPL) {  // every lane's disparities exist: no bounds tests on d
-    if (pf >= 4) sgm4_kernel<KPL, KPL <= 8 ? 4 : 1, true, COMB><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o, d0, d1, comb_out);
-    else if (pf >= 2) sgm4_kernel<KPL, KPL <= 8 ? 2 : 1, true, COMB><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o, d0, d1, comb_out);
-    else sgm4_kernel<KPL, 1, true, COMB><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o, d0, d1, comb_out);
+    if (pf >= 4) sgm4_kernel<KPL, KPL <= 8 ? 4 : 1, true><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+    else if (pf >= 2) sgm4_kernel<KPL, KPL <= 8 ? 2 : 1, true><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+    else sgm4_kernel<KPL, 1, true><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
   } else {
-    if (pf >= 4) sgm4_kernel<KPL, KPL <= 8 ? 4 : 1, false, COMB><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o, d0, d1, comb_out);
-    else if (pf >= 2) sgm4_kernel<KPL, KPL <= 8 ? 2 : 1, false, COMB><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o, d0, d1, comb_out);
-    else sgm4_kernel<KPL, 1, false, COMB><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o, d0, d1, comb_out);
+    if (pf >= 4) sgm4_kernel<KPL, KPL <= 8 ? 4 : 1, false><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+    else if (pf >= 2) sgm4_kernel<KPL, KPL <= 8 ? 2 : 1, false><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+    else sgm4_kernel<KPL, 1, false><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
   }
-}
-
-template <bool COMB>
-static void sgm_dispatch(const SgmGrad& g, const float* in, int64_t H, int64_t W, int D, const SgmParams& sp,
-                         const SgmOut& o, cudaStream_t st, int prefetch, int d0, int d1, float* comb_out) {
-  const int kpl = (D + 31) / 32;
-  const int h = (int)H, w = (int)W;
-  if (kpl <= 1) sgm4_launch<1, COMB>(g, in, h, w, D, sp, o, st, prefetch, d0, d1, comb_out);
-  else if (kpl <= 2) sgm4_launch<2, COMB>(g, in, h, w, D, sp, o, st, prefetch, d0, d1, comb_out);
-  else if (kpl <= 4) sgm4_launch<4, COMB>(g, in, h, w, D, sp, o, st, prefetch, d0, d1, comb_out);
-  else if (kpl <= 8) sgm4_launch<8, COMB>(g, in, h, w, D, sp, o, st, prefetch, d0, d1, comb_out);
-  else if (kpl <= 16) sgm4_launch<16, COMB>(g, in, h, w, D, sp, o, st, prefetch, d0, d1, comb_out);
-  else sgm4_launch<32, COMB>(g, in, h, w, D, sp, o, st, prefetch, d0, d1, comb_out);
 }
 
 int launch_sgm4(const SgmGrad& g, const float* in, int64_t H, int64_t W, int D, const SgmParams& sp,
                 const SgmOut& o, cudaStream_t st, int prefetch) {
-  sgm_dispatch<false>(g, in, H, W, D, sp, o, st, prefetch, 0, 3, nullptr);
+  const int kpl = (D + 31) / 32;
+  const int h = (int)H, w = (int)W;
+  if (kpl <= 1) sgm4_launch<1>(g, in, h, w, D, sp, o, st, prefetch);
+  else if (kpl <= 2) sgm4_launch<2>(g, in, h, w, D, sp, o, st, prefetch);
+  else if (kpl <= 4) sgm4_launch<4>(g, in, h, w, D, sp, o, st, prefetch);
+  else if (kpl <= 8) sgm4_launch<8>(g, in, h, w, D, sp, o, st, prefetch);
+  else if (kpl <= 16) sgm4_launch<16>(g, in, h, w, D, sp, o, st, prefetch);
+  else sgm4_launch<32>(g, in, h, w, D, sp, o, st, prefetch);
   return check_launch("sgm4");
-}
-
-int launch_sgm_mean(const SgmGrad& g, const float* in, int64_t H, int64_t W, int D, const SgmParams& sp,
-                    const SgmOut& o, float* out, cudaStream_t st, int prefetch) {
-  sgm_dispatch<false>(g, in, H, W, D, sp, o, st, prefetch, 0, 2, nullptr);
-  sgm_dispatch<true>(g, in, H, W, D, sp, o, st, prefetch, 3, 3, out);
-  return check_launch("sgm_mean");
 }
 
 int launch_sgm_combine(const SgmOut& o, int64_t n, const float* base, float scale, float* out,

@@ -25,12 +25,6 @@ struct SgmOut {
 };
 int launch_sgm4(const SgmGrad& g, const float* in, int64_t H, int64_t W, int D, const SgmParams& sp,
                 const SgmOut& o, cudaStream_t st, int prefetch = 0);
-// One SGM iteration's mean of the four scan directions written to `out`,
-// ((L0 + L1) + L2 + L3) / 4: directions 0..2 into o.dir[0..2] (one launch),
-// then direction 3, whose scan adds its path costs to theirs (o.dir[3] is
-// not used); the same values as launch_sgm4 + launch_sgm_combine.
-int launch_sgm_mean(const SgmGrad& g, const float* in, int64_t H, int64_t W, int D, const SgmParams& sp,
-                    const SgmOut& o, float* out, cudaStream_t st, int prefetch = 0);
 // out = base + (((L0 + L1) + L2) + L3) * scale; base may be null or out.
 int launch_sgm_combine(const SgmOut& o, int64_t n, const float* base, float scale, float* out,
                        cudaStream_t st);

@@ -25,41 +25,44 @@ def relu(x):
     return np.maximum(x, 0.0), (x > 0).astype(np.float64)
 
 
-# the network's GELU polynomial (cbmv_b200/csrc/mlp_net.cuh, gelu_t):
-# x * clamp(0.5 + x p(x^2), 0, 1), p(u) = G[0] + G[1] u + ... + G[4] u^4
-G = np.array([3.9385697e-01, -5.9378225e-02, 6.5808324e-03, -3.9975342e-04, 9.9452836e-06], np.float32)
+def bf16_rn(x):
+    """Round float64 values to bfloat16 directly (round to nearest even), as
+    one bf16 operation rounds its exact result."""
+    a = np.ascontiguousarray(np.asarray(x, np.float64))
+    u = a.view(np.uint64)
+    r = ((u + np.uint64(0xFFFFFFFFFFF) + ((u >> np.uint64(45)) & np.uint64(1))) >> np.uint64(45)) << np.uint64(45)
+    return r.view(np.float64)
+
+
+# the network's GELU coefficients (cbmv_b200/csrc/mlp_net.cuh, gelu_t), bf16 values
+G = np.array([0.373046875, -0.04296875, 0.00238037109375])
+
+
+def gelu_bf16(x):
+    """The network's GELU as the device evaluates it: x rounded from float32
+    to bf16, then u = x*x, p = G2 u + G1, p = p u + G0, q = min(max(x p +
+    0.5, 0), 1), x*q, each operation rounded once to bf16 (mlp_net.cuh
+    gelu_t; the fused kernel's packed form is the same)."""
+    xb = bf16(x)  # through float32, as the device rounds its float32 accumulator
+    u = bf16_rn(xb * xb)
+    p = bf16_rn(G[2] * u + G[1])
+    p = bf16_rn(p * u + G[0])
+    q = np.maximum(bf16_rn(xb * p + 0.5), 0.0)
+    q = np.minimum(q, 1.0)
+    return bf16_rn(xb * q)
 
 
 def gelu(x):
-    """The network's GELU and its derivative, in float64."""
-    x = np.asarray(x, np.float64)
-    g = G.astype(np.float64)
-    u = x * x
-    p = (((g[4] * u + g[3]) * u + g[2]) * u + g[1]) * u + g[0]
-    dp = ((4 * g[4] * u + 3 * g[3]) * u + 2 * g[2]) * u + g[1]
-    qr = 0.5 + x * p
-    q = np.clip(qr, 0.0, 1.0)
-    inside = (qr > 0) & (qr < 1)
-    return x * q, q + np.where(inside, x * (p + 2 * u * dp), 0.0)
-
-
-def _fma32(a, b, c):
-    """float32 fused multiply-add: the exact product and sum (in float64,
-    exact for float32 operands up to one rounding of the sum) rounded once."""
-    return (np.float64(a) * np.float64(b) + np.float64(c)).astype(np.float32)
-
-
-def gelu_f32(x):
-    """The fused kernel's GELU of float32 accumulators, in its float32
-    operations and order (mlp_infer.cuh gelu_bf16x2)."""
-    x = np.asarray(x, np.float32)
-    u = (x * x).astype(np.float32)
-    p = _fma32(G[4], u, G[3])
-    p = _fma32(p, u, G[2])
-    p = _fma32(p, u, G[1])
-    p = _fma32(p, u, G[0])
-    q = np.clip(_fma32(x, p, np.float32(0.5)), 0, 1).astype(np.float32)
-    return (x * q).astype(np.float32)
+    """The network's GELU (bf16 evaluation) and, for the backward pass, the
+    derivative of the smooth function it approximates at bf16(x)."""
+    g = gelu_bf16(x)
+    xb = bf16(x)  # through float32, as the device rounds its float32 accumulator
+    u = xb * xb
+    p = (G[2] * u + G[1]) * u + G[0]
+    qr = 0.5 + xb * p
+    dq = p + 2 * u * (2 * G[2] * u + G[1])
+    d = np.where(qr <= 0, 0.0, np.where(qr >= 1, 1.0, qr + xb * dq))
+    return g, d
 
 
 ACT = {"relu": relu, "gelu": gelu}
@@ -130,12 +133,12 @@ def split_bf16(x):
 def forward_fused(vec, X, act="relu"):
     """The network as the fused inference kernel evaluates it (test
     infrastructure): every bias (and w4) enters as its bf16 high + low
-    parts; hidden activations are ReLU or the float32 GELU of the float32
-    accumulator, rounded to bf16; the output layer runs on those bf16
+    parts; hidden activations are ReLU of the float32 accumulator rounded to
+    bf16, or the bf16 GELU of it; the output layer runs on those bf16
     activations.  Returns z."""
     if act == "gelu":
         def h(s):
-            return bf16(gelu_f32(np.asarray(s, np.float32)))
+            return gelu_bf16(s)
     else:
         def h(s):
             return bf16(np.maximum(s, 0))
