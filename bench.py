@@ -6,11 +6,16 @@ step is the whole test path for that pair: four matchers, 20 features, the
 per-(pixel,d) classifier, then the MC-CNN `_mem` post-processing to the
 disparity map.  Both classifiers are timed: the random forest (50 trees,
 depth <= 20, trained on 30 seeded pairs, tests/golden/make_forest.py) and
-the bf16 MLP (tests/golden/mlp_694x554.npz, cbmv_b200/train_mlp.py).  The
-RF judges the MLP: both run on 20 held-out seeded pairs and the MLP is the
-headline only when its bad-2.0 is within 0.5 percentage points of the RF's.
+the bf16 MLP 20-128-128-64-1 with GELU hidden layers
+(tests/golden/mlp_gelu_694x554.npz, cbmv_b200/train_mlp.py).  The RF judges
+the MLP: both run on 20 held-out seeded pairs and the MLP is the headline
+only when its bad-2.0 is within 0.5 percentage points of the RF's.  Beside
+the headline: the same network with ReLU (a labelled variant), and the
+learned path with the `_interp` post (the reference's LR-check chain).
 With N GPUs (torchrun), every rank processes its own pair (seed = rank):
-weak scaling by independent pairs, no collective on the data path.
+weak scaling by independent pairs, no collective on the data path; with
+--batch, the 64 uneven pairs are split over the ranks (strong scaling) and
+gathered on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cbmv|reference]
 
@@ -18,10 +23,11 @@ weak scaling by independent pairs, no collective on the data path.
 between steps; `e2e` is the same metric through the public call with pinned
 host buffers (H2D of both images and D2H of the disparity inside the timed
 region).  `--impl reference` times the reference's own implementation of the
-path: its C++ matchers and feature extraction compiled unmodified
-(oracle/_ref), scikit-learn's predict_proba on the same forest, and its
-post.cu on the GPU (as shipped; the CPU restatement when that build is
-absent).
+path on whole pairs: its C++ matchers and feature extraction compiled
+unmodified (oracle/_ref) and batched as its test.py does, scikit-learn's
+predict_proba on the same forest, and its post.cu on the GPU (as shipped;
+the CPU restatement when that build is absent) on that classifier's own
+P(class 0).
 """
 import argparse
 import json
