@@ -68,12 +68,10 @@ static __constant__ float kEpsF[4] = {0.01f, 1.01f, 0.01f, 0.01f};
 static __constant__ float kInvSigmaF[4] = {(float)(1.0 / (2.0 * 8 * 8)), (float)(1.0 / 0.02),
                                            (float)(1.0 / (2.0 * 100 * 100)), (float)(1.0 / (2.0 * 100 * 100))};
 
-template <int NT = kGroupThreads>
 __device__ __forceinline__ void group_sync(int g) {
-  asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "n"(NT) : "memory");
+  asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "n"(kGroupThreads) : "memory");
 }
 // barrier of the group that also ANDs a flag over its threads
-template <int NT = kGroupThreads>
 __device__ __forceinline__ bool group_all(int g, bool v) {
   uint32_t r;
   asm volatile(
@@ -82,7 +80,7 @@ __device__ __forceinline__ bool group_all(int g, bool v) {
       "bar.red.and.pred q, %2, %3, p;\n\t"
       "selp.u32 %0, 1, 0, q;\n\t}"
       : "=r"(r)
-      : "r"((uint32_t)v), "r"(g + 1), "n"(NT)
+      : "r"((uint32_t)v), "r"(g + 1), "n"(kGroupThreads)
       : "memory");
   return r != 0;
 }
@@ -140,20 +138,13 @@ __device__ __forceinline__ void split_bf16(float x, float* hi, float* lo) {
 
 // Stage the inference weights from the float32 parameter vector, and the
 // constant tile of the bias MMAs.
-// Input column j of layer 1 holds feature kX0Perm[j] in the kernel with two
-// threads per tile row (each forms the five features of two matchers:
-// matchers 0, 1 in columns 0..9, matchers 2, 3 in 10..19, in the order cost,
-// ratio, likelihood, right-view ratio, right-view likelihood).
-__constant__ int kX0Perm[kF] = {0, 1, 4, 5, 8, 9, 12, 13, 16, 17, 2, 3, 6, 7, 10, 11, 14, 15, 18, 19};
-
-template <bool PERM = false>
 __device__ __forceinline__ void stage_inference_weights(const float* __restrict__ P, unsigned char* sW1, unsigned char* sW2,
                                         unsigned char* sW3, unsigned char* sW4, unsigned char* sOne) {
   for (int q = threadIdx.x; q < 128 * 64; q += blockDim.x) {
     const int r = q >> 6, k = q & 63;
     float v = 0.0f, hi, lo;
     if (k < kF) {
-      v = P[kOffW1 + r * kF + (PERM ? kX0Perm[k] : k)];
+      v = P[kOffW1 + r * kF + k];
     } else if (k == kF || k == kF + 1) {
       split_bf16(P[kOffB1 + r], &hi, &lo);
       v = k == kF ? hi : lo;
@@ -452,247 +443,6 @@ __global__ void __launch_bounds__(kInfThreads, 1)
 #undef DESC
 }
 
-// ---------------------------------------------------------------------
-// The same network with two threads per tile row: eight warps per 128-row
-// group (1024 threads per CTA), warps w and w + 4 of a group sharing the
-// tensor-memory lanes of rows 32 (w % 4) .. +31.  The row's first thread
-// (half 0) forms the features of matchers 0 and 1, the second (half 1)
-// those of matchers 2 and 3 (layer 1's weight columns permuted to match,
-// kX0Perm); in each epilogue half h takes columns [64h, 64h + 64) of the
-// 128-wide layers and [32h, 32h + 32) of layer 3.  Each thread thus carries
-// half the serial work of a tile per layer.
-constexpr int kGroupThreads2 = 2 * kGroupThreads;
-constexpr int kInfThreads2 = kGroupThreads2 * kGroups;
-
-// Columns c0 .. c0+NC-1 (c0 a multiple of 16, run time) of the accumulator.
-template <int NC, int ACT>
-__device__ __forceinline__ void epilogue_span(uint32_t tlane, unsigned char* rowp, int r7s, int c0) {
-  uint32_t ga[16], gb[16];
-  umma::tmem_ld16_issue(tlane + c0, ga);
-  umma::tmem_ld16_wait(ga);
-#pragma unroll
-  for (int c = 0; c < NC; c += 32) {
-    umma::tmem_ld16_issue(tlane + c0 + c + 16, gb);
-    act_store16<ACT>(rowp, r7s, c0 + c, ga);
-    umma::tmem_ld16_wait(gb);
-    if (c + 32 < NC) umma::tmem_ld16_issue(tlane + c0 + c + 32, ga);
-    act_store16<ACT>(rowp, r7s, c0 + c + 16, gb);
-    if (c + 32 < NC) umma::tmem_ld16_wait(ga);
-  }
-}
-
-// One thread's half of a sample's feature inputs: matchers m0 = 2h, m0 + 1.
-struct FeatIn2 {
-  float c[2];
-  float2 sl[2], sr[2];
-};
-
-__device__ __forceinline__ void load_feat_in2(const float* __restrict__ v0, const float* __restrict__ v1,
-                                              const float2* __restrict__ st0, const float2* __restrict__ st1,
-                                              int64_t HW, int64_t N, int64_t t, int64_t p, int d, int64_t x,
-                                              FeatIn2& in) {
-  const bool valid = t < N;
-  const int64_t tv = valid ? t : 0, pv = valid ? p : 0;
-  const int dv = valid ? d : 0;
-  const bool has_right = valid && x >= d;
-  in.c[0] = __ldg(v0 + tv);
-  in.c[1] = __ldg(v1 + tv);
-  in.sl[0] = __ldg(st0 + pv);
-  in.sl[1] = __ldg(st1 + pv);
-  in.sr[0] = has_right ? __ldg(st0 + HW + pv - dv) : make_float2(kRandMaxF, 0.0f);
-  in.sr[1] = has_right ? __ldg(st1 + HW + pv - dv) : make_float2(kRandMaxF, 0.0f);
-}
-
-template <int ACT>
-__global__ void __launch_bounds__(kInfThreads2, 1)
-    features_mlp2_kernel(FeatVolsF fv, const float2* __restrict__ statsf, int64_t H, int64_t W, int D,
-                         const float* __restrict__ P, float* __restrict__ prob0, int* __restrict__ status) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char* sW1 = base;
-  unsigned char* sW2 = sW1 + kSmW1i;
-  unsigned char* sW3 = sW2 + kSmW2i;
-  unsigned char* sW4 = sW3 + kSmW3i;
-  unsigned char* sOne = sW4 + kSmW4i;
-  unsigned char* sTiles = sOne + kSmOne;
-  __shared__ float4 s_nrm[kF];  // per input column: cap, mu, inv_sd of its feature
-  __shared__ float s_b4;
-  __shared__ uint64_t bars[kGroups];
-  __shared__ uint32_t tmem_base;
-  const int tid = threadIdx.x, g = tid / kGroupThreads2, gt = tid % kGroupThreads2;
-  const int row = gt % kGroupThreads, half = gt / kGroupThreads, wq = row >> 5;
-
-  if (tid < 32) umma::tmem_alloc(&tmem_base, 128 * kGroups);
-  if (tid < kGroups) umma::mbar_init(&bars[tid], 1);
-  stage_inference_weights<true>(P, sW1, sW2, sW3, sW4, sOne);
-  for (int i = tid; i < kF; i += kInfThreads2) {
-    const int f = kX0Perm[i];
-    s_nrm[i] = make_float4(P[f], P[kF + f], P[2 * kF + f], 0.0f);
-  }
-  if (tid == 0) s_b4 = P[kOffB4];
-  umma::fence_async_smem();
-  umma::tc_fence_before();
-  __syncthreads();
-  umma::tc_fence_after();
-
-  unsigned char* sA = sTiles + g * kSmTile;
-  unsigned char* rowp = sA + (row >> 3) * 1024 + (row & 7) * 128;
-  const int r7s = (row & 7) << 4;
-  uint64_t* bar0 = &bars[g];
-  const uint32_t tacc = tmem_base + (uint32_t)(g * 128);
-  const uint32_t tlane = tacc + ((uint32_t)(wq * 32) << 16);
-  const bool leader = gt == 0;
-  constexpr uint32_t id128 = umma::idesc_bf16(128, 128), id64 = umma::idesc_bf16(128, 64),
-                     id16 = umma::idesc_bf16(128, 16);
-#define DESC(ptr) umma::sw128_desc(umma::smem_u32(ptr))
-
-  const int64_t HW = H * W, N = HW * D;
-  // this half's matchers m0 = 2 half, m0 + 1: volumes and statistics
-  const int m0 = 2 * half;
-  const float* v0 = half ? fv.v[2] : fv.v[0];
-  const float* v1 = half ? fv.v[3] : fv.v[1];
-  const float2* st0 = statsf + (int64_t)(2 * m0) * HW;  // left view; the right view follows at + HW
-  const float2* st1 = statsf + (int64_t)(2 * m0 + 2) * HW;
-  const float e0 = kEpsF[m0], e1 = kEpsF[m0 + 1], is0 = kInvSigmaF[m0], is1 = kInvSigmaF[m0 + 1];
-
-  const int64_t tiles = (N + 127) / 128;
-  const int64_t tstride = (int64_t)gridDim.x * kGroups;
-  int64_t tile = (int64_t)blockIdx.x * kGroups + g;
-  int64_t t = tile * 128 + row;
-  int64_t p = t / D;
-  int d = (int)(t - p * D);
-  int64_t x = p % W;
-  const int64_t step = tstride * 128;
-  const int64_t sp = step / D;
-  const int sd = (int)(step - sp * D);
-  const int64_t sx = sp % W;
-  uint32_t ph0 = 0;
-  bool ok = true;
-  auto wait = [&](uint64_t* b, uint32_t& ph) {
-    const bool r = group_all<kGroupThreads2>(g, leader ? umma::mbar_wait(b, ph, kWaitLimit) : true);
-    ph ^= 1u;
-    umma::tc_fence_after();
-    return r;
-  };
-  auto handoff = [&]() {
-    umma::fence_async_smem();
-    umma::tc_fence_before();
-    group_sync<kGroupThreads2>(g);
-    umma::tc_fence_after();
-  };
-
-  FeatIn2 in;
-  load_feat_in2(v0, v1, st0, st1, HW, N, t, p, d, x, in);
-  for (; tile < tiles; tile += tstride) {
-    // 1. this half's ten features -> its input columns (in the tile's
-    //    second atom): half 0 columns 0..9, half 1 columns 10..19 and the
-    //    bias inputs 20, 21 (ones), the rest zero
-    {
-      float f[10];  // per matcher: cost, ratio, likelihood, right ratio, right likelihood
-      const float i0 = __fdividef(1.0f, in.c[0] + e0), i1 = __fdividef(1.0f, in.c[1] + e1);
-      f[0] = in.c[0];
-      f[1] = in.c[1];
-      conf_f32(in.c[0], i0, in.sl[0], e0, is0, &f[2], &f[4]);
-      conf_f32(in.c[1], i1, in.sl[1], e1, is1, &f[3], &f[5]);
-      conf_f32(in.c[0], i0, in.sr[0], e0, is0, &f[6], &f[8]);
-      conf_f32(in.c[1], i1, in.sr[1], e1, is1, &f[7], &f[9]);
-      uint32_t u[5];
-      const int j0 = 10 * half;
-#pragma unroll
-      for (int k = 0; k < 10; k += 2) {
-        const float4 na = s_nrm[j0 + k], nb = s_nrm[j0 + k + 1];
-        u[k >> 1] = pack_bf16x2((fminf(f[k], na.x) - na.y) * na.z, (fminf(f[k + 1], nb.x) - nb.y) * nb.z);
-      }
-      uint32_t* c1 = reinterpret_cast<uint32_t*>(tile_chunk(rowp, r7s, 1, 1));
-      if (half == 0) {
-        *tile_chunk(rowp, r7s, 1, 0) = make_uint4(u[0], u[1], u[2], u[3]);
-        c1[0] = u[4];
-      } else {
-        c1[1] = u[0];
-        c1[2] = u[1];
-        c1[3] = u[2];
-        *tile_chunk(rowp, r7s, 1, 2) = make_uint4(u[3], u[4], kBf16OneOne, 0u);
-        *tile_chunk(rowp, r7s, 1, 3) = make_uint4(0u, 0u, 0u, 0u);
-      }
-    }
-    const int64_t t_cur = t;
-    t += step;
-    p += sp;
-    d += sd;
-    x += sx;
-    if (d >= D) {
-      d -= D;
-      p += 1;
-      x += 1;
-    }
-    if (x >= W) x -= W;
-    if (tile + tstride < tiles) load_feat_in2(v0, v1, st0, st1, HW, N, t, p, d, x, in);
-    handoff();
-    // 2. layer 1 (K = 32) -> accumulator columns 0..127
-    if (leader) {
-      const uint64_t dX = DESC(sA + 128 * 128), dW1 = DESC(sW1);
-      umma::mma_bf16(tacc, dX, dW1, id128, false);
-      umma::mma_bf16(tacc, dX + 2, dW1 + 2, id128, true);
-      umma::mma_commit(bar0);
-    }
-    if (!(ok = wait(bar0, ph0))) break;
-    epilogue_span<64, ACT>(tlane, rowp, r7s, 64 * half);
-    handoff();
-    // 3. layer 2 (K = 128) onto the bias b2
-    if (leader) {
-      const uint64_t dA0 = DESC(sA), dA1 = DESC(sA + 128 * 128), dW20 = DESC(sW2), dW21 = DESC(sW2 + 128 * 128);
-      umma::mma_bf16(tacc, DESC(sOne), DESC(sW1) + 2 * (kColB2 / 16), id128, false);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA0 + 2 * kk, dW20 + 2 * kk, id128, true);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA1 + 2 * kk, dW21 + 2 * kk, id128, true);
-      umma::mma_commit(bar0);
-    }
-    if (!(ok = wait(bar0, ph0))) break;
-    epilogue_span<64, ACT>(tlane, rowp, r7s, 64 * half);
-    handoff();
-    // 4. layer 3 (N = 64) onto the bias b3
-    if (leader) {
-      const uint64_t dA0 = DESC(sA), dA1 = DESC(sA + 128 * 128), dW30 = DESC(sW3), dW31 = DESC(sW3 + 64 * 128);
-      umma::mma_bf16(tacc, DESC(sOne), DESC(sW1) + 2 * (kColB3 / 16), id64, false);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA0 + 2 * kk, dW30 + 2 * kk, id64, true);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA1 + 2 * kk, dW31 + 2 * kk, id64, true);
-      umma::mma_commit(bar0);
-    }
-    if (!(ok = wait(bar0, ph0))) break;
-    epilogue_span<32, ACT>(tlane, rowp, r7s, 32 * half);
-    handoff();
-    // 5. output layer (N = 16, rows 0/1 = high/low parts of w4) -> columns 64..79
-    if (leader) {
-      const uint64_t dA0 = DESC(sA), dW4 = DESC(sW4);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc + 64, dA0 + 2 * kk, dW4 + 2 * kk, id16, kk > 0);
-      umma::mma_commit(bar0);
-    }
-    if (!(ok = wait(bar0, ph0))) break;
-    if (half == 0) {
-      uint32_t z2[2];
-      asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];"
-                   : "=r"(z2[0]), "=r"(z2[1])
-                   : "r"(tlane + 64));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(z2[0]), "+r"(z2[1]) : : "memory");
-      const float z = (__uint_as_float(z2[0]) + __uint_as_float(z2[1])) + s_b4;
-      if (t_cur < N) prob0[t_cur] = 1.0f / (1.0f + __expf(z));
-    }
-    umma::tc_fence_before();
-  }
-  if (!ok && leader) {
-    atomicExch(status, 1);
-    umma::mbar_wait(bar0, ph0 ^ 1u, kWaitLimit);
-  }
-  umma::tc_fence_before();
-  __syncthreads();
-  if (tid < 32) umma::tmem_dealloc(tmem_base, 128 * kGroups);
-#undef DESC
-}
-
 }  // namespace
 
 // Launch shape of the fused kernel; returns the grid (CTAs).
@@ -701,21 +451,6 @@ inline int features_mlp_grid(int64_t H, int64_t W, int D, int max_ctas, int sms)
   const int64_t need = (tiles + kGroups - 1) / kGroups;
   const int cap = max_ctas > 0 && max_ctas < sms ? max_ctas : sms;
   return (int)(need < cap ? need : cap);
-}
-
-template <int ACT>
-int launch_features_mlp2_act(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
-                             const cbmv_mlp* m, float* prob0, cudaStream_t st, int max_ctas) {
-  int dev = 0, sms = 0;
-  CBMV_CUDA(cudaGetDevice(&dev));
-  CBMV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  CBMV_CUDA(cudaFuncSetAttribute(features_mlp2_kernel<ACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kSmInf));
-  CBMV_REQUIRE(((uintptr_t)statsf & 7) == 0, CBMV_EINVAL, "feature statistics must be 8-byte aligned");
-  const int grid = features_mlp_grid(H, W, D, max_ctas, sms);
-  FeatVolsF fv = {{vols[0], vols[1], vols[2], vols[3]}};
-  features_mlp2_kernel<ACT><<<grid, kInfThreads2, kSmInf, st>>>(fv, statsf, H, W, D, m->P, prob0, m->status);
-  return check_launch("features_mlp2");
 }
 
 template <int ACT>

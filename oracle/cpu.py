@@ -251,9 +251,22 @@ class _Post:
 
     Shapes follow the reference's bookkeeping: swap_axis / swap_axis_back /
     CUDA_copy_double change the destination's shape (post.cu:612-614,
-    663-665, 702-704)."""
+    663-665, 702-704).
+
+    as_shipped=False (`post`): swap_axis_back is the transpose it is meant
+    to be.  as_shipped=True (`post_as_shipped`): it also restates the
+    reference kernel's store condition, `(Col + d) < cols*rows` with Col
+    already the pixel index (post.cu:645-646): the pixel p of disparity d is
+    not written when p + 16 * floor((d mod 64) / 16) >= H*W, so the last
+    16..48 pixels of those disparities keep the destination's previous
+    contents (in the reference's drivers, the same buffer in the [H,W,D]
+    layout).  That is what the reference computes; the fused path computes
+    the transpose."""
     CUDA_double_array = CUDA_double_array
     CUDA_float_array = CUDA_float_array
+
+    def __init__(self, as_shipped=False):
+        self.as_shipped = as_shipped
 
     def InitCUDA(self):
         return True
@@ -285,7 +298,18 @@ class _Post:
         out.a = np.ascontiguousarray(np.transpose(a.a, (1, 2, 0)))
 
     def swap_axis_back(self, a, out):
-        out.a = np.ascontiguousarray(np.transpose(a.a, (2, 0, 1)))
+        res = np.ascontiguousarray(np.transpose(a.a, (2, 0, 1)))  # [D,H,W]
+        if self.as_shipped:
+            D = res.shape[0]
+            HW = res.shape[1] * res.shape[2]
+            prev = out.a.reshape(-1)
+            flat = res.reshape(D, HW)
+            for d in range(D):
+                skip = 16 * ((d % 64) // 16)
+                if skip:
+                    lo = max(HW - skip, 0)
+                    flat[d, lo:] = prev[d * HW + lo:(d + 1) * HW]
+        out.a = res
 
     def CUDA_copy_double(self, a, out):
         out.a = a.a.copy()
@@ -335,6 +359,7 @@ class _Post:
 
 
 post = _Post()
+post_as_shipped = _Post(as_shipped=True)
 
 
 def wta(cost_dhw):

@@ -200,3 +200,27 @@ def test_support_words_reproduce_separable_model(oracle_cpu):
         got = post_model.cbca_from_words(words, vol)
         ref = post_model.cbca_separable(lc.a, rc.a, vol, direction, 5)
         assert np.array_equal(got, ref)
+
+
+def test_swap_axis_back_as_shipped_leaves_the_tail_unwritten():
+    """The as-shipped restatement of the reference's swap_axis_back (its
+    store condition tests Col + d with Col already the pixel,
+    post.cu:645-646): disparity d keeps the destination's previous contents
+    in its last 16 * floor((d mod 64) / 16) pixels, everything else is the
+    transpose."""
+    from oracle import cpu
+    H, W, D = 3, 7, 70
+    rng = np.random.default_rng(0)
+    hwd = rng.random((H, W, D))
+    prev = rng.random((D, H, W)) + 10  # distinguishable
+    a, out = cpu.post_as_shipped.CUDA_double_array(hwd), cpu.post_as_shipped.CUDA_double_array(prev)
+    cpu.post_as_shipped.swap_axis_back(a, out)
+    meant = np.transpose(hwd, (2, 0, 1)).reshape(D, -1)
+    got = out.a.reshape(D, -1)
+    for d in range(D):
+        k = min(16 * ((d % 64) // 16), H * W)
+        assert np.array_equal(got[d, :H * W - k], meant[d, :H * W - k]), d
+        assert np.array_equal(got[d, H * W - k:], prev.reshape(D, -1)[d, H * W - k:]), d
+    b, out2 = cpu.post.CUDA_double_array(hwd), cpu.post.CUDA_double_array(prev)
+    cpu.post.swap_axis_back(b, out2)
+    assert np.array_equal(out2.a.reshape(D, -1), meant)
