@@ -316,7 +316,17 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
   RC(cost_chain(p, w, H, W, D, w.crossL, w.crossR, p->direction, w.volA, w.volB, &res, st));
   float* d0 = w.dtmp;
   float* d1 = w.dtmp2;
-  RC(launch_wta_subpixel(res, H, W, D, nullptr, d0, st));
+  if (p->interpolate) {
+    // The _interp chain checks and fills the integer winner-take-all
+    // disparity: its subpixel step writes disp_temp (test.py:293), the
+    // left-right check reads disp_d, still the argmin (test.py:297), and
+    // interpolate_mismatch then overwrites every pixel of disp_temp
+    // (test.py:299, post.cu:757-827), so the subpixel result never reaches
+    // the output and is not formed here.
+    RC(launch_wta_subpixel(res, H, W, D, d0, nullptr, st));
+  } else {
+    RC(launch_wta_subpixel(res, H, W, D, nullptr, d0, st));
+  }
   if (p->interpolate) {
     // left-right check and fills (test.py:295-303, post.cu:717-869)
     RC(launch_outlier(d0, w.dright, H, W, D, w.outlier, st));

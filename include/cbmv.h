@@ -325,10 +325,12 @@ typedef struct cbmv_params {
    * test.py:143-149): 0 (default) the _mem post (test.py:341-449); 1 the
    * _interp post (test.py:153-338): the right view's cost
    * (get_right_cost) through the same chain with the arms swapped and the
-   * direction negated, then after the left view's subpixel step the
-   * left-right check (outlier_detection) and its fills
-   * (interpolate_mismatch, interpolate_occlusion).  Needs one more float32
-   * [H,W,D] volume of workspace.  cbmv_batch_run_mlp accepts 0 only. */
+   * direction negated, then the left-right check (outlier_detection) and
+   * its fills (interpolate_mismatch, interpolate_occlusion) on the left
+   * view's integer winner-take-all disparity, as the reference's chain
+   * does (its subpixel result is overwritten, test.py:293-300); median and
+   * blur follow.  Needs one more float32 [H,W,D] volume of workspace.
+   * cbmv_batch_run_mlp accepts 0 only. */
   int interpolate;
 } cbmv_params;
 void cbmv_params_default(cbmv_params* p);
