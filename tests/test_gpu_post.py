@@ -84,6 +84,34 @@ def test_sgm_close(gpu, oracle_cpu, scene):
     np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=2e-5, atol=2e-4)
 
 
+@pytest.mark.parametrize("D", [68, 128, 200])
+@pytest.mark.parametrize("direction", [-1, 1])
+def test_sgm_consecutive_lanes_equal_strided(gpu, scene, D, direction):
+    """The SGM scan with KPL consecutive disparities per lane (float4 path
+    costs, taken for D % 4 == 0 in (64, 512] on 16-byte aligned volumes)
+    and the strided scan (lane = d mod 32, taken otherwise) agree bit for
+    bit: same per-element arithmetic in the same order.  An input volume
+    4 bytes off a 16-byte boundary selects the strided scan."""
+    from cbmv_b200 import _lib
+    imgl, imgr, _, _ = scene
+    H, W = imgl.shape
+    rng = np.random.default_rng(D)
+    vol = rng.random((H, W, D)).astype(np.float32)
+    a, b = _t(imgl), _t(imgr)
+    buf = torch.zeros(H * W * D + 4, device="cuda")
+    outs = []
+    for off in (0, 1):  # 16-byte aligned (consecutive lanes), then 4 bytes off (strided)
+        v = buf[off:off + H * W * D]
+        v.copy_(torch.from_numpy(vol.reshape(-1)).cuda())
+        assert (v.data_ptr() % 16 == 0) == (off == 0)
+        out = torch.zeros((H, W, D), device="cuda")
+        _lib.call("cbmv_sgm", a.data_ptr(), b.data_ptr(), v.data_ptr(), H, W, D, 1.3, 10,
+                  .12, 1.4, 2.2, 3, direction, out.data_ptr(), None)
+        outs.append(out.cpu().numpy())
+    assert np.isfinite(outs[0]).all()
+    assert np.array_equal(outs[0], outs[1])
+
+
 def test_wta_subpixel_median_mean2d_exact(gpu, oracle_cpu, scene):
     from oracle import glue
     from cbmv_b200 import _lib
