@@ -94,6 +94,37 @@ __global__ void census_cost_kernel(const ulonglong2* __restrict__ dl,
   out[vol_index(layout, c.y, c.x, c.d, H, W, D)] = cvt_out<T>(v);
 }
 
+// The float32 [H,W,D] census volume of the learned path, without a
+// division per element: a CTA owns 16 columns of one row and 128
+// disparities (lane = d), so the left descriptor is one broadcast load per
+// column and the right one a coalesced run along d.  Same values and
+// sentinels as census_cost_kernel (the popcount sum is exact in float32).
+__global__ void __launch_bounds__(128) census_cost_hwd_f32_kernel(const ulonglong2* __restrict__ dl,
+                                                                  const ulonglong2* __restrict__ dr, int64_t H,
+                                                                  int64_t W, int D, int w, float* __restrict__ out) {
+  const int64_t y = blockIdx.y;
+  const int64_t x0 = (int64_t)blockIdx.x * 16;
+  const int d = blockIdx.z * 128 + threadIdx.x;
+  if (d >= D) return;
+  const int wc = w / 2;
+  const int64_t i = y - wc;
+  const bool row_ok = i >= 0 && i < H - w;
+#pragma unroll 4
+  for (int s = 0; s < 16; s++) {
+    const int64_t x = x0 + s;
+    if (x >= W) break;
+    const int64_t j = x - wc;
+    float v = kRandMaxF;
+    // matchers.cpp:312-316: rows i < H-w, cols j < W-w, d < min(D, j+1)
+    if (row_ok && j >= 0 && j < W - w && d <= j) {
+      const ulonglong2 a = dl[y * W + x];
+      const ulonglong2 b = dr[y * W + x - d];
+      v = (float)(__popcll(a.x ^ b.x) + __popcll(a.y ^ b.y));
+    }
+    out[(y * W + x) * D + d] = v;
+  }
+}
+
 // ------------------------------------------------------------------- NCC
 // Window sum A and 1/sqrt(w^2 B - A^2) (matchers.cpp:115-131); B is exact.
 __global__ void ncc_stats_kernel(const uint8_t* __restrict__ img, int64_t H, int64_t W, int w,
@@ -390,6 +421,11 @@ int launch_census_desc(const uint8_t* img, int64_t H, int64_t W, int w, ulonglon
 template <class T>
 int launch_census_cost(const ulonglong2* dl, const ulonglong2* dr, int64_t H, int64_t W, int D,
                        int w, int layout, T* out, cudaStream_t st) {
+  if (std::is_same<T, float>::value && layout == CBMV_HWD) {
+    const dim3 grid((unsigned)((W + 15) / 16), (unsigned)H, (unsigned)((D + 127) / 128));
+    census_cost_hwd_f32_kernel<<<grid, 128, 0, st>>>(dl, dr, H, W, D, w, reinterpret_cast<float*>(out));
+    return check_launch("census_cost");
+  }
   census_cost_kernel<T><<<vol_grid(layout, H, W, D), kBlock, 0, st>>>(dl, dr, H, W, D, w, layout, out);
   return check_launch("census_cost");
 }

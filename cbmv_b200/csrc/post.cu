@@ -195,9 +195,12 @@ __device__ __noinline__ void sgm_scan(const SgmGrad& g, const float* __restrict_
 // costs are KPL/4 float4 loads and stores per lane, the d-1 / d+1
 // neighbours are in the lane's own registers except at its two ends (two
 // shuffles per step instead of two per register), and the minimum over d
-// is one `redux.sync.min.f32`.  Per element the arithmetic and its order
-// are those of sgm_scan, so the results are the same bit for bit.
-template <int KPL, int PF>
+// is one `redux.sync.min.f32`.  The matching direction S (+-1) and FULL
+// (D == 32 * KPL) are compile-time, the step's addresses advance by
+// constant strides, and step 0 (whose path cost is its cost) loads no
+// image terms.  Per element the arithmetic and its order are those of
+// sgm_scan, so the results are the same bit for bit.
+template <int KPL, int PF, bool FULL, int S>
 __device__ __noinline__ void sgm_scan_c(const SgmGrad& g, const float* __restrict__ in, int H, int W, int D,
                                         const SgmParams& sp, int line, float* __restrict__ out, const int DIR) {
   static_assert(KPL % 4 == 0, "float4 path costs");
@@ -223,91 +226,114 @@ __device__ __noinline__ void sgm_scan_c(const SgmGrad& g, const float* __restric
                               : (int64_t)(H - 1) * W + line;
   const int64_t pstep = DIR == 0 ? 1 : DIR == 1 ? -1 : DIR == 2 ? (int64_t)W : -(int64_t)W;
   const int x0 = DIR == 0 ? 0 : DIR == 1 ? W - 1 : line;
-  const int s = sp.direction;
   const int xlo = max(0, dx);
   const unsigned xspan = (unsigned)(min(W, W + dx) - xlo);
   const int d0 = KPL * lane;  // this lane's first disparity
-  const bool lane_on = d0 < D;  // D % 4 == 0: a float4 is all in or all out
+  const bool lane_on = FULL || d0 < D;  // D % 4 == 0: a float4 is all in or all out
 
   struct Step {
     float cost[KPL], d2[KPL];
     float d1;
   };
-  auto load = [&](int step, Step& st) {
-    const int64_t ind2 = p0 + step * pstep;
-    const int xl = x0 + step * dx + d0 * s - xlo;
-    const float* grp = gr + ind2 + gshift + d0 * s;
-    st.d1 = step > 0 ? gl[ind2 + gshift] : 0.0f;
-    const float4* src = reinterpret_cast<const float4*>(in + ind2 * D + d0);
+  // the next step to load: its pixel's path-cost row, its image terms
+  // (D1 at gl[.], D2 at gr[. + d*S]) and the matching column of its first
+  // disparity relative to the span where D2 exists
+  const float* lsrc = in + p0 * D + d0;
+  const float* lgl = gl + p0 + gshift;
+  const float* lgr = gr + p0 + gshift + d0 * S;
+  int lxl = x0 + d0 * S - xlo;
+  const int64_t vstride = pstep * D;
+  auto load_costs = [&](Step& st) {
+    const float4* src = reinterpret_cast<const float4*>(lsrc);
 #pragma unroll
     for (int v = 0; v < NV; v++) {
-      const bool on = lane_on && d0 + 4 * v < D;
+      const bool on = lane_on && (FULL || d0 + 4 * v < D);
       const float4 c = on ? src[v] : make_float4(inf, inf, inf, inf);
       st.cost[4 * v] = c.x;
       st.cost[4 * v + 1] = c.y;
       st.cost[4 * v + 2] = c.z;
       st.cost[4 * v + 3] = c.w;
     }
+    lsrc += vstride;
+  };
+  // a step >= 1: costs, D1 and the per-d D2 (10 where the matching pixel
+  // or its predecessor leaves the image, post.cu:232-237)
+  auto load = [&](Step& st) {
+    load_costs(st);
+    st.d1 = *lgl;
 #pragma unroll
     for (int k = 0; k < KPL; k++) {
-      const bool dk = d0 + k < D;
-      const bool inside = (unsigned)(xl + k * s) < xspan;
-      st.d2[k] = (step > 0 && dk && inside) ? grp[k * s] : 10.0f;
+      const bool inside = (FULL || d0 + k < D) && (unsigned)(lxl + k * S) < xspan;
+      st.d2[k] = inside ? lgr[k * S] : 10.0f;
     }
+    lgl += pstep;
+    lgr += pstep;
+    lxl += dx;
   };
   float prev[KPL];
   Step ring[PF];
+  {
+    // step 0: the path cost is the cost
+    Step st0;
+    load_costs(st0);
+    lgl += pstep;
+    lgr += pstep;
+    lxl += dx;
+#pragma unroll
+    for (int k = 0; k < KPL; k++) prev[k] = st0.cost[k];
+    float4* dst = reinterpret_cast<float4*>(out + p0 * D + d0);
+#pragma unroll
+    for (int v = 0; v < NV; v++)
+      if (lane_on && (FULL || d0 + 4 * v < D))
+        dst[v] = make_float4(prev[4 * v], prev[4 * v + 1], prev[4 * v + 2], prev[4 * v + 3]);
+  }
 #pragma unroll
   for (int i = 0; i < PF; i++)
-    if (i < nsteps) load(i, ring[i]);
-  for (int s0 = 0; s0 < nsteps; s0 += PF) {
+    if (1 + i < nsteps) load(ring[i]);
+  float* ldst = out + (p0 + pstep) * D + d0;
+  for (int s0 = 1; s0 < nsteps; s0 += PF) {
 #pragma unroll
     for (int i = 0; i < PF; i++) {
       const int step = s0 + i;
       if (step >= nsteps) break;
       const Step cur = ring[i];
-      if (step + PF < nsteps) load(step + PF, ring[i]);
+      if (step + PF < nsteps) load(ring[i]);
+      float m = fminf(fminf(prev[0], prev[1]), fminf(prev[2], prev[3]));
+#pragma unroll
+      for (int k = 4; k < KPL; k++) m = fminf(m, prev[k]);
+      float mn;
+      asm volatile("redux.sync.min.f32 %0, %1, 0xffffffff;" : "=f"(mn) : "f"(m));
+      // the neighbours across the lane's ends: d0 - 1 from the previous
+      // lane's last register, d0 + KPL from the next lane's first
+      const float lo0 = __shfl_up_sync(0xffffffffu, prev[KPL - 1], 1);
+      const float hiL = __shfl_down_sync(0xffffffffu, prev[0], 1);
+      const bool d1lo = cur.d1 < sp.tau_so, d1hi = cur.d1 > sp.tau_so;
+      const float a2 = d1lo ? p2[0] : p2[1], a1lo = d1lo ? p1lo[0] : p1lo[1], a1hi = d1lo ? p1hi[0] : p1hi[1];
       float L[KPL];
-      if (step == 0) {
 #pragma unroll
-        for (int k = 0; k < KPL; k++) L[k] = cur.cost[k];
-      } else {
-        float m = prev[0];
-#pragma unroll
-        for (int k = 1; k < KPL; k++) m = fminf(m, prev[k]);
-        float mn;
-        asm volatile("redux.sync.min.f32 %0, %1, 0xffffffff;" : "=f"(mn) : "f"(m));
-        // the neighbours across the lane's ends: d0 - 1 from the previous
-        // lane's last register, d0 + KPL from the next lane's first
-        const float lo0 = __shfl_up_sync(0xffffffffu, prev[KPL - 1], 1);
-        const float hiL = __shfl_down_sync(0xffffffffu, prev[0], 1);
-        const bool d1lo = cur.d1 < sp.tau_so, d1hi = cur.d1 > sp.tau_so;
-        const float a2 = d1lo ? p2[0] : p2[1], a1lo = d1lo ? p1lo[0] : p1lo[1],
-                    a1hi = d1lo ? p1hi[0] : p1hi[1];
-#pragma unroll
-        for (int k = 0; k < KPL; k++) {
-          const int d = d0 + k;
-          const float lo = k > 0 ? prev[k - 1] : lo0;
-          const float hi = k + 1 < KPL ? prev[k + 1] : hiL;
-          const float D2 = cur.d2[k];
-          const bool ca = d1lo ? D2 < sp.tau_so : (d1hi && D2 > sp.tau_so);
-          float cost = fminf(prev[k], mn + (ca ? a2 : p2[2]));
-          if (d - 1 >= 0) cost = fminf(cost, lo + (ca ? a1lo : p1lo[2]));
-          if (d + 1 < D) cost = fminf(cost, hi + (ca ? a1hi : p1hi[2]));
-          L[k] = d < D ? cur.cost[k] + cost - mn : inf;
-        }
+      for (int k = 0; k < KPL; k++) {
+        const int d = d0 + k;
+        const float lo = k > 0 ? prev[k - 1] : lo0;
+        const float hi = k + 1 < KPL ? prev[k + 1] : hiL;
+        const float D2 = cur.d2[k];
+        const bool ca = d1lo ? D2 < sp.tau_so : (d1hi && D2 > sp.tau_so);
+        float cost = fminf(prev[k], mn + (ca ? a2 : p2[2]));
+        if (k > 0 || d - 1 >= 0) cost = fminf(cost, lo + (ca ? a1lo : p1lo[2]));
+        if (FULL ? (k + 1 < KPL || lane < 31) : d + 1 < D) cost = fminf(cost, hi + (ca ? a1hi : p1hi[2]));
+        L[k] = (FULL || d < D) ? cur.cost[k] + cost - mn : inf;
       }
-      float4* dst = reinterpret_cast<float4*>(out + (p0 + step * pstep) * D + d0);
+      float4* dst = reinterpret_cast<float4*>(ldst);
 #pragma unroll
       for (int v = 0; v < NV; v++)
-        if (lane_on && d0 + 4 * v < D) dst[v] = make_float4(L[4 * v], L[4 * v + 1], L[4 * v + 2], L[4 * v + 3]);
+        if (lane_on && (FULL || d0 + 4 * v < D)) dst[v] = make_float4(L[4 * v], L[4 * v + 1], L[4 * v + 2], L[4 * v + 3]);
+      ldst += vstride;
 #pragma unroll
       for (int k = 0; k < KPL; k++) prev[k] = L[k];
     }
   }
 }
 
-template <int KPL, int PF>
+template <int KPL, int PF, bool FULL, int S>
 __global__ void __launch_bounds__(128) sgm4c_kernel(SgmGrad g, const float* __restrict__ in, int H, int W,
                                                     int D, SgmParams sp, SgmOut o) {
   const int warp = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -325,7 +351,7 @@ __global__ void __launch_bounds__(128) sgm4c_kernel(SgmGrad g, const float* __re
     dir = 3;
     line = warp - 2 * H - W;
   }
-  if (dir >= 0) sgm_scan_c<KPL, PF>(g, in, H, W, D, sp, line, o.dir[dir], dir);
+  if (dir >= 0) sgm_scan_c<KPL, PF, FULL, S>(g, in, H, W, D, sp, line, o.dir[dir], dir);
 }
 
 template <int KPL, int PF, bool FULL>
@@ -1078,10 +1104,16 @@ static void sgm4c_launch(const SgmGrad& g, const float* in, int H, int W, int D,
                          const SgmOut& o, cudaStream_t st, int prefetch) {
   const int lines = 2 * H + 2 * W;
   const int blocks = (lines * 32 + 127) / 128;
-  if (prefetch == 1)
-    sgm4c_kernel<KPL, 1><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
-  else
-    sgm4c_kernel<KPL, 2><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o);
+  const bool full = D == 32 * KPL;
+#define SGM4C(PF_, FULL_, S_) sgm4c_kernel<KPL, PF_, FULL_, S_><<<blocks, 128, 0, st>>>(g, in, H, W, D, sp, o)
+  if (sp.direction > 0) {
+    if (prefetch == 1) { if (full) SGM4C(1, true, 1); else SGM4C(1, false, 1); }
+    else { if (full) SGM4C(2, true, 1); else SGM4C(2, false, 1); }
+  } else {
+    if (prefetch == 1) { if (full) SGM4C(1, true, -1); else SGM4C(1, false, -1); }
+    else { if (full) SGM4C(2, true, -1); else SGM4C(2, false, -1); }
+  }
+#undef SGM4C
 }
 
 static bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
@@ -1255,6 +1287,7 @@ extern "C" int cbmv_sgm(const float* imL, const float* imR, const float* in, int
   REQ_HW(H, W);
   CBMV_REQUIRE(D > 0 && D <= 1024, CBMV_ERANGE, "D=%d not in 1..1024", D);
   CBMV_REQUIRE(in != out, CBMV_EINVAL, "sgm: in and out must differ");
+  CBMV_REQUIRE(direction == 1 || direction == -1, CBMV_EINVAL, "direction must be +-1");
   cudaStream_t st = as_stream(stream);
   const int64_t HW = H * W, V = HW * D;
   float* scratch = nullptr;

@@ -43,6 +43,11 @@ def test_layouts_and_float32(gpu, oracle_cpu, small_pair):
     cref = oracle_cpu.mtc.census(L, R, D, 11)
     assert np.array_equal(c32, np.transpose(cref, (2, 0, 1)).astype(np.float32))
     assert c32.max() == np.float32(RAND_MAX)
+    # the [H,W,D] float32 census (the learned path's layout, its own kernel),
+    # also with more than 128 disparities (two disparity blocks)
+    for d in (D, 140):
+        h32 = mtc.census(L, R, d, 11, dtype=np.float32, layout="HWD")
+        assert np.array_equal(h32, oracle_cpu.mtc.census(L, R, d, 11).astype(np.float32)), d
 
 
 def test_device_tensors_stay_on_device(gpu, oracle_cpu, small_pair):
