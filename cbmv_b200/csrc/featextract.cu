@@ -356,16 +356,116 @@ __global__ void __launch_bounds__(RS_PIX) stats_f32_right_kernel(VolsF vols, int
   if (xr < W) statsf[(int64_t)(m * 2 + 1) * H * W + y * W + xr] = stats_pair(mn, den);
 }
 
+// view 0 for D a multiple of 4 up to 128: a pixel's row is one float4 per
+// lane, the minimum one `redux.sync.min.f32`, and each warp works on two
+// pixels at a time; the per-lane sum and the shuffle tree are those of
+// stats_f32_left_kernel, so the results are the same bit for bit.
+__global__ void __launch_bounds__(256) stats_f32_left_q_kernel(VolsF vols, int64_t HW, int D,
+                                                               float2* __restrict__ statsf) {
+  const int m = blockIdx.y;
+  const float inv_sigma = kInvSigmaF32[m];
+  const int lane = threadIdx.x & 31;
+  const int nq = D >> 2;  // float4s per row, <= 32
+  const bool on = lane < nq;
+  const float4* __restrict__ rows = reinterpret_cast<const float4*>(vols.v[m]) + lane;
+  float2* __restrict__ out = statsf + (int64_t)(m * 2) * HW;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const float4 big = make_float4(kRandMaxF, kRandMaxF, kRandMaxF, kRandMaxF);
+  auto den4 = [&](float4 v, float mn) {
+    const float tx = v.x - mn, ty = v.y - mn, tz = v.z - mn, tw = v.w - mn;
+    return (__expf(-(tx * tx) * inv_sigma) + __expf(-(ty * ty) * inv_sigma)) +
+           (__expf(-(tz * tz) * inv_sigma) + __expf(-(tw * tw) * inv_sigma));
+  };
+  for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < HW; p += 2 * nw) {
+    const int64_t p2 = p + nw;
+    const bool two = p2 < HW;
+    const float4 va = on ? __ldg(rows + p * nq) : big;
+    const float4 vb = on && two ? __ldg(rows + p2 * nq) : big;
+    float ma = fminf(fminf(va.x, va.y), fminf(va.z, va.w));
+    float mb = fminf(fminf(vb.x, vb.y), fminf(vb.z, vb.w));
+    asm volatile("redux.sync.min.f32 %0, %0, 0xffffffff;" : "+f"(ma));
+    asm volatile("redux.sync.min.f32 %0, %0, 0xffffffff;" : "+f"(mb));
+    float da = on ? den4(va, ma) : 0.0f, db = on ? den4(vb, mb) : 0.0f;
+    for (int o = 16; o; o >>= 1) {
+      da += __shfl_xor_sync(0xffffffffu, da, o);
+      db += __shfl_xor_sync(0xffffffffu, db, o);
+    }
+    if (lane == 0) out[p] = stats_pair(ma, da);
+    if (lane == 1 && two) out[p2] = stats_pair(mb, db);
+  }
+}
+
+// view 1 for D a multiple of 4: as stats_f32_right_kernel, the staging
+// loads one float4 (4 disparities) per thread and step with 32-bit row
+// offsets; the diagonal walk, and so the order of the sums, is unchanged.
+__global__ void __launch_bounds__(RS_PIX) stats_f32_right_q_kernel(VolsF vols, int64_t H, int64_t W, int D,
+                                                                   float2* __restrict__ statsf) {
+  __shared__ float tile[(RS_PIX + 32) * 33];
+  const int m = blockIdx.y;
+  const float* __restrict__ vol = vols.v[m];
+  const float fill = __ldg(vol);
+  const float inv_sigma = kInvSigmaF32[m];
+  const int64_t nxb = (W + RS_PIX - 1) / RS_PIX;
+  const int64_t y = blockIdx.x / nxb;
+  const int X0 = (int)((blockIdx.x % nxb) * RS_PIX);
+  const int Wi = (int)W;
+  const float* __restrict__ rowp = vol + y * W * D;  // C[y, 0, 0]
+  const int tid = threadIdx.x;
+  const int xr = X0 + tid;
+  float mn = kRandMaxF, den = 0.0f;
+  for (int pass = 0; pass < 2; pass++) {
+    for (int d0 = 0; d0 < D; d0 += 32) {
+      __syncthreads();
+#pragma unroll
+      for (int it = 0; it < (RS_PIX + 32) * 8 / RS_PIX; it++) {
+        const int q = tid + it * RS_PIX;
+        const int i = q >> 3, j4 = (q & 7) * 4;
+        const int x = X0 + d0 + i;
+        float4 v = make_float4(fill, fill, fill, fill);
+        if (x < Wi && d0 + j4 < D) v = __ldg(reinterpret_cast<const float4*>(rowp + (int64_t)x * D + d0 + j4));
+        float* t = tile + i * 33 + j4;
+        t[0] = v.x;
+        t[1] = v.y;
+        t[2] = v.z;
+        t[3] = v.w;
+      }
+      __syncthreads();
+      if (xr < Wi) {
+        const int nj = D - d0 < 32 ? D - d0 : 32;
+        if (pass == 0) {
+          for (int j = 0; j < nj; j++) mn = fminf(mn, tile[(tid + j) * 33 + j]);
+        } else {
+          for (int j = 0; j < nj; j++) {
+            const float t = tile[(tid + j) * 33 + j] - mn;
+            den += __expf(-(t * t) * inv_sigma);
+          }
+        }
+      }
+    }
+  }
+  if (xr < Wi) statsf[(int64_t)(m * 2 + 1) * H * W + y * W + xr] = stats_pair(mn, den);
+}
+
 int launch_feature_stats_f32(const float* const* vols, int64_t H, int64_t W, int D, float2* statsf,
                              cudaStream_t st) {
   const VolsF v = {{vols[0], vols[1], vols[2], vols[3]}};
   const int64_t HW = H * W;
   const int64_t lblocks = (HW + 7) / 8;  // 8 warps per block, one pixel each
-  stats_f32_left_kernel<<<dim3((unsigned)(lblocks < 65535 * 16 ? lblocks : 65535 * 16), 4), 256, 0, st>>>(
-      v, HW, D, statsf);
+  const bool q = D % 4 == 0 && ((uintptr_t)vols[0] | (uintptr_t)vols[1] | (uintptr_t)vols[2] | (uintptr_t)vols[3]) % 16 == 0;
+  if (q && D <= 128) {
+    const int64_t qblocks = (HW + 15) / 16;  // 8 warps per block, two pixels each
+    stats_f32_left_q_kernel<<<dim3((unsigned)(qblocks < 65535 * 16 ? qblocks : 65535 * 16), 4), 256, 0, st>>>(
+        v, HW, D, statsf);
+  } else {
+    stats_f32_left_kernel<<<dim3((unsigned)(lblocks < 65535 * 16 ? lblocks : 65535 * 16), 4), 256, 0, st>>>(
+        v, HW, D, statsf);
+  }
   const int64_t rblocks = H * ((W + RS_PIX - 1) / RS_PIX);
   CBMV_REQUIRE(rblocks < ((int64_t)1 << 31), CBMV_ERANGE, "image too large for the statistics grid");
-  stats_f32_right_kernel<<<dim3((unsigned)rblocks, 4), RS_PIX, 0, st>>>(v, H, W, D, statsf);
+  if (q && W < ((int64_t)1 << 30))
+    stats_f32_right_q_kernel<<<dim3((unsigned)rblocks, 4), RS_PIX, 0, st>>>(v, H, W, D, statsf);
+  else
+    stats_f32_right_kernel<<<dim3((unsigned)rblocks, 4), RS_PIX, 0, st>>>(v, H, W, D, statsf);
   return check_launch("feature_stats_f32");
 }
 
