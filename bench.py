@@ -221,15 +221,17 @@ def forest_visits_per_unit(pipe, gf, flat, l, r, n=65536):
 
 
 def launches_per_pair(prm):
-    """Kernel launches of one cbmv_run_mlp / cbmv_run_rf call (pipeline.cu)
-    for parameters prm: 8 per-pixel terms (census descriptors, NCC sums,
-    ZSAD means, Sobel; both images), 4 cost volumes, 2 row statistics,
-    1 features+classifier; post: 4 image normalisation, 2 cross, 1 SGM
-    neighbour differences, 2 per SGM iteration, 1 CBCA support build and 1
-    per CBCA pass, WTA+subpixel, median per iteration, mean2d."""
+    """Kernel launches of one cbmv_run_mlp call (pipeline.cu) for parameters
+    prm: 6 per-pixel terms (census descriptors, NCC sums, Sobel; both
+    images; the ZSAD strip kernel of window 5 forms its window means itself,
+    another window adds their 2 launches), 4 cost volumes, 2 row
+    statistics, 1 features+classifier; post: 4 image normalisation, 2
+    cross, 1 SGM neighbour differences, 2 per SGM iteration, 1 CBCA support
+    build and 1 per CBCA pass, WTA+subpixel, median per iteration,
+    mean2d."""
     post = 4 + 2 + (1 + 2 * prm.sgm_i if prm.sgm_i else 0) + (1 + prm.cbca_i2 if prm.cbca_i2 else 0) \
         + (1 + prm.cbca_i1 if prm.cbca_i1 else 0) + 1 + prm.median_i + 1
-    return 8 + 4 + 2 + 1 + post
+    return (6 if prm.sadw == 5 else 8) + 4 + 2 + 1 + post
 
 
 def run_cbmv(a, ws, rank, local):

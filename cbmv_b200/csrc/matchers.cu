@@ -314,6 +314,9 @@ __global__ void __launch_bounds__(128) matcher_strip_kernel(
   // per window row
   int col[WIN];
   int dif[MODE == kStripZsad ? WIN : 1][WIN];
+  // ZSAD: the column's sum of L minus its sum of R (the window's sum of
+  // these is sum L - sum R, exact: 25 x its mean difference)
+  int cdm[MODE == kStripZsad ? WIN : 1];
   auto load_col = [&](int slot, int64_t c) {
     const int64_t cl = c < 0 ? 0 : (c >= W ? W - 1 : c);
     int64_t cr = c - d;
@@ -324,8 +327,12 @@ __global__ void __launch_bounds__(128) matcher_strip_kernel(
       const int a = (int)__ldg(L + rowoff[wh] + cl), b = (int)__ldg(R + rowoff[wh] + cr);
       if (MODE == kStripSadSob) sum += abs(a - b);
       else if (MODE == kStripNcc) sum += a * b;
-      else dif[MODE == kStripZsad ? slot : 0][wh] = (WIN * WIN) * (a - b);
+      else {
+        dif[MODE == kStripZsad ? slot : 0][wh] = (WIN * WIN) * (a - b);
+        sum += a - b;
+      }
     }
+    if (MODE == kStripZsad) cdm[MODE == kStripZsad ? slot : 0] = sum;
     col[slot] = sum;
   };
 #pragma unroll
@@ -345,13 +352,16 @@ __global__ void __launch_bounds__(128) matcher_strip_kernel(
         for (int k = 0; k < WIN; k++) acc += col[(s + k) % WIN];
         v = (float)acc;
       } else if (MODE == kStripZsad) {
-        const int64_t pl = y * W + x;
-        const int m = (int)llrint(ml[pl] * (WIN * WIN)) - (int)llrint(mr[pl - d] * (WIN * WIN));
-        int acc = 0;
+        // 25 x (mean L - mean R) over the window, exactly (the window lies
+        // inside both images here, so no column or row was clamped)
+        int m = 0;
+#pragma unroll
+        for (int k = 0; k < WIN; k++) m += cdm[MODE == kStripZsad ? (s + k) % WIN : 0];
+        unsigned acc = 0;
 #pragma unroll
         for (int k = 0; k < WIN; k++)
 #pragma unroll
-          for (int wh = 0; wh < WIN; wh++) acc += abs(dif[MODE == kStripZsad ? (s + k) % WIN : 0][wh] - m);
+          for (int wh = 0; wh < WIN; wh++) acc = __sad(dif[MODE == kStripZsad ? (s + k) % WIN : 0][wh], m, acc);
         v = (float)((double)acc / (double)(WIN * WIN));
       } else {
         const int64_t pl = y * W + x, pr = pl - d;

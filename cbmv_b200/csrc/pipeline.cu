@@ -362,8 +362,12 @@ static int run_front(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const 
   RC(launch_census_desc(R, H, W, p->censw, w.descR, st));
   RC(launch_ncc_stats(L, H, W, p->nccw, w.AL, w.CL, st));
   RC(launch_ncc_stats(R, H, W, p->nccw, w.AR, w.CR, st));
-  RC(launch_zsad_means(L, H, W, p->sadw, w.muL, st));
-  RC(launch_zsad_means(R, H, W, p->sadw, w.muR, st));
+  // the learned path's ZSAD strip kernel (window 5) forms the window means
+  // itself, from the column sums it holds anyway
+  if (!(f32 && p->sadw == 5)) {
+    RC(launch_zsad_means(L, H, W, p->sadw, w.muL, st));
+    RC(launch_zsad_means(R, H, W, p->sadw, w.muR, st));
+  }
   RC(launch_sobel_i32(L, H, W, w.sobL, st));
   RC(launch_sobel_i32(R, H, W, w.sobR, st));
   if (f32) {

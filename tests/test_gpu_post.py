@@ -185,17 +185,22 @@ def test_dropin_post_module_runs_reference_driver(gpu, oracle_cpu, scene):
     assert close_i >= 0.999, close_i
 
 
-@pytest.mark.parametrize("direction,L1", [(-1, 6), (1, 6), (-1, 9)])
-def test_cbca_separable_matches_model_exactly(gpu, oracle_cpu, scene, direction, L1):
+@pytest.mark.parametrize("direction,L1,D70", [(-1, 6, False), (1, 6, False), (-1, 9, False), (-1, 6, True),
+                                               (1, 6, True)])
+def test_cbca_separable_matches_model_exactly(gpu, oracle_cpu, scene, direction, L1, D70):
     """cbmv_cbca_separable (the fused pipeline's default CBCA: with L1 <= 6
     its supports precomputed once and read by the pass; with L1 = 9 the
     arms are built with L1 = 9, reach up to 8 pixels and the pass reads the
     arms themselves) against the oracle's float32 model of its summation
     order with a halo of L1 - 1: bit-exact; against the reference-order
-    cbca: relative 1e-5."""
+    cbca: relative 1e-5.  D70: 70 disparities (three 32-wide disparity
+    tiles, the last one partial)."""
     from cbmv_b200 import _lib
     from oracle import post_model
     imgl, imgr, vol, D = scene
+    if D70:
+        D = 70
+        vol = np.random.default_rng(70).random((imgl.shape[0], imgl.shape[1], D)).astype(np.float32)
     lc, rc = _crosses(oracle_cpu, imgl, imgr, L1)
     H, W = imgl.shape
     reach = max(int(np.max(np.abs(lc[0] - np.arange(W)[None, :]))), int(np.max(np.abs(lc[2] - np.arange(H)[:, None]))))
