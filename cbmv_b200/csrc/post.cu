@@ -656,14 +656,34 @@ int launch_cbca_sep_h(const float* lc, const float* rc, const float* in, int64_t
 constexpr int kMaskHalo = kCbcaMaskMaxHalo;
 constexpr uint32_t kMaskCopy = 1u << 31;
 
+// Relative arms of one pixel packed as four int8: arm a minus the pixel's
+// x (arms 0, 1) or y (arms 2, 3).  cross_kernel's arms lie within L1 of
+// their pixel; anything beyond 127 is clamped (the taps stop at +-5 anyway).
+__device__ __forceinline__ int clamp_i8(int v) { return min(max(v, -128), 127); }
+__device__ __forceinline__ uint32_t pack_rel_arms(const float* __restrict__ c, int64_t HW, int64_t o, int x, int y) {
+  const int a0 = clamp_i8((int)__ldg(c + o) - x), a1 = clamp_i8((int)__ldg(c + HW + o) - x);
+  const int a2 = clamp_i8((int)__ldg(c + 2 * HW + o) - y), a3 = clamp_i8((int)__ldg(c + 3 * HW + o) - y);
+  return (uint32_t)(a0 & 0xFF) | ((uint32_t)(a1 & 0xFF) << 8) | ((uint32_t)(a2 & 0xFF) << 16) |
+         ((uint32_t)(a3 & 0xFF) << 24);
+}
+template <int B>
+__device__ __forceinline__ int rel_arm(uint32_t w) {
+  return (int)((int32_t)(w << (24 - 8 * B)) >> 24);
+}
+
 template <int CS_TY>
 __global__ void __launch_bounds__(256) cbca_mask_build_kernel(const float* __restrict__ lc,
                                                               const float* __restrict__ rc, int H, int W, int D,
                                                               int direction, uint32_t* __restrict__ mask) {
   constexpr int HALO = kMaskHalo;
   constexpr int SR = CS_TY + 2 * HALO;
-  __shared__ uint8_t sC[SR][CS_TX][CS_TD];     // support-row lengths
+  constexpr int NXM = CS_TX + CS_TD - 1;  // matching columns x + d * direction of the tile
+  // support-row lengths of rows 0..SR-1 in sP[1..SR], then (in place)
+  // their prefix sums over the rows: sP[r] = lengths of rows 0..r-1
+  __shared__ uint16_t sP[SR + 1][CS_TX][CS_TD];
   __shared__ uint16_t sH[CS_TY][CS_TX][CS_TD];  // support-row taps of the tile's own rows
+  __shared__ uint32_t sAL[SR][CS_TX];           // packed relative arms, left view at (yy, x)
+  __shared__ uint32_t sAR[SR][NXM];             // right view at (yy, xm)
   const int ntd = (D + CS_TD - 1) / CS_TD, ntx = (W + CS_TX - 1) / CS_TX;
   const int64_t t = blockIdx.x;
   const int td = (int)(t % ntd), tx = (int)((t / ntd) % ntx), ty = (int)(t / ((int64_t)ntd * ntx));
@@ -672,50 +692,80 @@ __global__ void __launch_bounds__(256) cbca_mask_build_kernel(const float* __res
   const int d = td * CS_TD + lane, dd = d * direction;
   const bool dok = d < D;
   const int64_t HW = (int64_t)H * W;
+  // the tile's matching columns: X0 + d * direction over its disparities
+  const int xm_lo = direction > 0 ? X0 + td * CS_TD : X0 - (td * CS_TD + CS_TD - 1);
+  // 0. the arms the tile needs, converted once per pixel (rows and columns
+  //    outside the image are never read back)
+  for (int q = threadIdx.x; q < SR * (CS_TX + NXM); q += blockDim.x) {
+    const int r = q / (CS_TX + NXM), j = q - r * (CS_TX + NXM);
+    const int yy = Y0 - HALO + r;
+    if (yy < 0 || yy >= H) continue;
+    if (j < CS_TX) {
+      const int x = X0 + j;
+      if (x < W) sAL[r][j] = pack_rel_arms(lc, HW, (int64_t)yy * W + x, x, yy);
+    } else {
+      const int xm = xm_lo + (j - CS_TX);
+      if (xm >= 0 && xm < W) sAR[r][j - CS_TX] = pack_rel_arms(rc, HW, (int64_t)yy * W + xm, xm, yy);
+    }
+  }
+  __syncthreads();
   // 1. support rows of the tile's rows and HALO rows above and below
   for (int r = warp; r < SR; r += 8) {
     const int yy = Y0 - HALO + r;
     const bool rok = yy >= 0 && yy < H && dok;
-    const int64_t o = (int64_t)(rok ? yy : 0) * W;
 #pragma unroll
     for (int c = 0; c < CS_TX; c++) {
       const int x = X0 + c, xm = x + dd;
       int cnt = 0;
       uint32_t hm = 0;
       if (rok && x < W && xm >= 0 && xm < W) {
-        const int ks = max((int)__ldg(lc + o + x), (int)__ldg(rc + o + xm) - dd) - x;
-        const int kt = min((int)__ldg(lc + HW + o + x), (int)__ldg(rc + HW + o + xm) - dd) - x;
+        const uint32_t wl = sAL[r][c], wr = sAR[r][xm - xm_lo];
+        // max(lc0[x], rc0[xm] - dd) - x and min(lc1[x], rc1[xm] - dd) - x
+        const int ks = max(rel_arm<0>(wl), rel_arm<0>(wr));
+        const int kt = min(rel_arm<1>(wl), rel_arm<1>(wr));
         cnt = max(kt - ks - 1, 0);
         const int lo = max(ks + 1, -HALO), hi = min(kt - 1, HALO);
         if (hi >= lo) hm = ((1u << (hi - lo + 1)) - 1u) << (lo + HALO);
       }
-      sC[r][c][lane] = (uint8_t)cnt;
+      sP[r + 1][c][lane] = (uint16_t)cnt;
       if (r >= HALO && r < HALO + CS_TY) sH[r - HALO][c][lane] = (uint16_t)hm;
     }
   }
   __syncthreads();
-  // 2. support columns: warp c owns tile column c
+  // 2. support columns: warp c owns tile column c; the thread first forms
+  //    the prefix sums of its (column, disparity)'s support-row lengths, so
+  //    a support of rows lo..hi counts sP[hi + 1] - sP[lo] pixels (exact
+  //    integers, the same count as adding them row by row)
   const int c = warp, x = X0 + c, xm = x + dd;
+  {
+    uint32_t run = 0;
+    sP[0][c][lane] = 0;
+    for (int r = 1; r <= SR; r++) {
+      run += sP[r][c][lane];
+      sP[r][c][lane] = (uint16_t)run;
+    }
+  }
   if (x >= W || !dok) return;
   const bool xok = xm >= 0 && xm < W;
   for (int cy = 0; cy < CS_TY; cy++) {
     const int y = Y0 + cy;
     if (y >= H) break;
-    const int64_t o = (int64_t)y * W;
-    const int64_t id = (o + x) * D + d;
+    const int64_t id = ((int64_t)y * W + x) * D + d;
     if (!xok) {
       mask[id] = kMaskCopy;
       continue;
     }
-    const int ks = max((int)__ldg(lc + 2 * HW + o + x), (int)__ldg(rc + 2 * HW + o + xm)) - y;
-    const int kt = min((int)__ldg(lc + 3 * HW + o + x), (int)__ldg(rc + 3 * HW + o + xm)) - y;
+    const uint32_t wl = sAL[cy + HALO][c], wr = sAR[cy + HALO][xm - xm_lo];
+    // max(lc2[x], rc2[xm]) - y and min(lc3[x], rc3[xm]) - y: the support
+    // rows are the taps k with ks < k < kt, within +-HALO
+    const int ks = max(rel_arm<2>(wl), rel_arm<2>(wr));
+    const int kt = min(rel_arm<3>(wl), rel_arm<3>(wr));
+    const int lo = max(ks + 1, -HALO), hi = min(kt - 1, HALO);
     uint32_t vm = 0, cnt = 0;
-#pragma unroll
-    for (int k = -HALO; k <= HALO; k++)
-      if (k > ks && k < kt) {
-        vm |= 1u << (k + HALO);
-        cnt += sC[cy + HALO + k][c][lane];
-      }
+    if (hi >= lo) {
+      vm = ((1u << (hi - lo + 1)) - 1u) << (lo + HALO);
+      cnt = (uint32_t)sP[cy + HALO + hi + 1][c][lane] - (uint32_t)sP[cy + HALO + lo][c][lane];
+    }
     mask[id] = (uint32_t)sH[cy][c][lane] | (vm << 11) | ((cnt & 0x7Fu) << 22);
   }
 }
