@@ -6,7 +6,7 @@ step is the whole test path for that pair: four matchers, 20 features, the
 per-(pixel,d) classifier, then the MC-CNN `_mem` post-processing to the
 disparity map.  Both classifiers are timed: the random forest (50 trees,
 depth <= 20, trained on 30 seeded pairs, tests/golden/make_forest.py) and
-the bf16 MLP 20-128-128-64-1 with GELU hidden layers
+the 16-bit MLP 20-128-128-64-1 with GELU hidden layers (f16 inference)
 (tests/golden/mlp_gelu_694x554.npz, cbmv_b200/train_mlp.py).  The RF judges
 the MLP: both run on 20 held-out seeded pairs and the MLP is the headline
 only when its bad-2.0 is within 0.5 percentage points of the RF's.  Beside
@@ -364,13 +364,13 @@ def run_cbmv(a, ws, rank, local):
     roof = res[head]["roofline"]
 
     classifier = {"rf": "random_forest (50 trees, depth<=20)",
-                  "mlp": "bf16 MLP 20-128-128-64-1 (%s) on tcgen05 (RF as judge)"
+                  "mlp": "f16 MLP 20-128-128-64-1 (%s) on tcgen05 (RF as judge)"
                          % (net.activation.upper() if net is not None else "")}[head]
     line = {
         "metric": METRIC, "value": units * ws / (h["ms"] / 1e3), "unit": "pixel·disparities/s",
         "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": h["ms"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "bf16/f32" if head == "mlp" else "f64/f32",
+        "dtype": "f16/f32" if head == "mlp" else "f64/f32",
         "data": "synthetic (seeded 694x554 pair per rank; L2 flushed between steps)",
         "config": {"workload": "694x554 D=128 test path: 4 matchers, 20 features, %s, MC-CNN _mem post"
                                % classifier, "width": W0, "height": int(L.shape[0]), "ndisp": D0,

@@ -3,7 +3,7 @@
 // (mlp_infer_relu.cu, mlp_infer_gelu.cu), so that neither instantiation
 // changes how the compiler allocates the other's registers.
 #pragma once
-#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "features.cuh"
 #include "mlp_net.cuh"
@@ -26,21 +26,21 @@
 // spinning), which also hands them the poll's result.
 //
 // Arithmetic, per layer (the float32 accumulator in tensor memory); every
-// bias enters as bf16 high + low parts multiplied by constant ones:
+// bias enters as f16 high + low parts multiplied by constant ones:
 //   layer 1  K = 32: 20 normalised features, two constant-one columns whose
 //            weights are b1's parts, zeros;
 //   layers 2, 3: a first K = 16 MMA of a constant tile (ones in columns 0
 //            and 1) against b2's / b3's parts (stored in the unused K
 //            columns 32..63 of layer 1's weight tile) initialises the
 //            accumulator, the layer's MMAs accumulate onto it;
-//   hidden activations: ReLU and the bf16 rounding in one instruction
-//            (cvt.rn.relu.bf16x2.f32) per pair of columns, or the GELU in
-//            packed bf16 arithmetic (seven instructions per pair);
+//   hidden activations: ReLU and the f16 rounding in one instruction
+//            (cvt.rn.relu.f16x2.f32) per pair of columns, or the GELU in
+//            packed f16 arithmetic (six instructions per pair);
 //   output   layer 4 is an MMA too: N = 16, rows 0 and 1 of its weight tile
-//            are the high and low bf16 parts of w4, z = D[0] + D[1] + b4,
+//            are the high and low f16 parts of w4, z = D[0] + D[1] + b4,
 //            cost = 1 - sigmoid(z) = 1 / (1 + exp(z)).
 // The features themselves are formed in float32 (they enter the network as
-// bf16), from float32 cost volumes and float32 row statistics (min, 1/den),
+// f16), from float32 cost volumes and float32 row statistics (min, 1/den),
 // with one reciprocal 1/(c + e) shared by the left and right ratio.
 // ====================================================================
 
@@ -62,7 +62,7 @@ constexpr size_t kSmOne = 128 * 128;      // [128 x 64], ones in columns 0 and 1
 constexpr size_t kSmTile = 2 * 128 * 128; // a group's activation tile [128 x 128]
 constexpr size_t kSmInf = 1024 + kSmW1i + kSmW2i + kSmW3i + kSmW4i + kSmOne + kGroups * kSmTile;
 constexpr int kColB2 = 32, kColB3 = 48;  // K columns of layer 1's weight tile holding b2, b3
-constexpr uint32_t kBf16OneOne = 0x3F803F80u;  // two bf16 ones
+constexpr uint32_t kF16OneOne = 0x3C003C00u;  // two f16 ones
 
 static __constant__ float kEpsF[4] = {0.01f, 1.01f, 0.01f, 0.01f};
 static __constant__ float kInvSigmaF[4] = {(float)(1.0 / (2.0 * 8 * 8)), (float)(1.0 / 0.02),
@@ -85,35 +85,37 @@ __device__ __forceinline__ bool group_all(int g, bool v) {
   return r != 0;
 }
 
-// Two float32 values as a packed bf16 pair (low = a), round to nearest even
-__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
-  const __nv_bfloat162 x = __floats2bfloat162_rn(a, b);
-  return *reinterpret_cast<const uint32_t*>(&x);
-}
-
-// ReLU of two float32 pre-activations, as a packed bf16 pair (low = a),
-// round to nearest even
-__device__ __forceinline__ uint32_t relu_bf16x2(float a, float b) {
+// Two float32 values as a packed f16 pair (low = a), round to nearest even,
+// saturated to the largest finite f16 (+-65504)
+__device__ __forceinline__ uint32_t pack_f16x2(float a, float b) {
   uint32_t r;
-  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+  asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
   return r;
 }
 
-// GELU (gelu_t) of two float32 pre-activations as a packed bf16 pair (low =
-// a): the same bf16 operations as gelu_t, both lanes per instruction --
-// seven instructions per pair, the conversion included.
-__device__ __forceinline__ uint32_t gelu_bf16x2(float a, float b) {
-  const __nv_bfloat162 g0 = __bfloat162bfloat162(bf16_bits(kG0Bits)),
-                       g1 = __bfloat162bfloat162(bf16_bits(kG1Bits)),
-                       g2 = __bfloat162bfloat162(bf16_bits(kG2Bits));
-  const __nv_bfloat162 half = __float2bfloat162_rn(0.5f), one = __float2bfloat162_rn(1.0f);
-  const __nv_bfloat162 x = __floats2bfloat162_rn(a, b);
-  const __nv_bfloat162 u = __hmul2(x, x);
-  __nv_bfloat162 p = __hfma2(g2, u, g1);
+// ReLU of two float32 pre-activations, as a packed f16 pair (low = a),
+// round to nearest even, saturated to 65504
+__device__ __forceinline__ uint32_t relu_f16x2(float a, float b) {
+  uint32_t r;
+  asm("cvt.rn.relu.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+  return r;
+}
+
+// GELU (gelu_t) of two float32 pre-activations as a packed f16 pair (low =
+// a): the same f16 operations as gelu_t, both lanes per instruction -- six
+// instructions per pair, the conversion included, the clamp of q to [0, 1]
+// folded into its FMA (`fma.rn.sat.f16x2`).
+__device__ __forceinline__ uint32_t gelu_f16x2(float a, float b) {
+  const __half2 g0 = __half2half2(f16_bits(kG0Bits)), g1 = __half2half2(f16_bits(kG1Bits)),
+                g2 = __half2half2(f16_bits(kG2Bits));
+  const __half2 half = __float2half2_rn(0.5f);
+  const uint32_t xb = pack_f16x2(a, b);
+  const __half2 x = *reinterpret_cast<const __half2*>(&xb);
+  const __half2 u = __hmul2(x, x);
+  __half2 p = __hfma2(g2, u, g1);
   p = __hfma2(p, u, g0);
-  __nv_bfloat162 q = __hfma2_relu(x, p, half);
-  q = __hmin2(q, one);
-  const __nv_bfloat162 g = __hmul2(x, q);
+  const __half2 q = __hfma2_sat(x, p, half);
+  const __half2 g = __hmul2(x, q);
   return *reinterpret_cast<const uint32_t*>(&g);
 }
 
@@ -130,9 +132,9 @@ __device__ __forceinline__ void conf_f32(float c, float inv_ce, float2 st, float
   *lik = __expf(-(t * t) * inv_sigma) * st.y;  // 1/den = 0 on sentinel rows
 }
 
-// bf16 high part of x and the bf16 rounding of the rest: x ~ hi + lo
-__device__ __forceinline__ void split_bf16(float x, float* hi, float* lo) {
-  *hi = __bfloat162float(__float2bfloat16_rn(x));
+// f16 high part of x and the f16 rounding of the rest: x ~ hi + lo
+__device__ __forceinline__ void split_f16(float x, float* hi, float* lo) {
+  *hi = __half2float(__float2half_rn(x));
   *lo = x - *hi;
 }
 
@@ -146,31 +148,31 @@ __device__ __forceinline__ void stage_inference_weights(const float* __restrict_
     if (k < kF) {
       v = P[kOffW1 + r * kF + k];
     } else if (k == kF || k == kF + 1) {
-      split_bf16(P[kOffB1 + r], &hi, &lo);
+      split_f16(P[kOffB1 + r], &hi, &lo);
       v = k == kF ? hi : lo;
     } else if (k == kColB2 || k == kColB2 + 1) {
-      split_bf16(P[kOffB2 + r], &hi, &lo);
+      split_f16(P[kOffB2 + r], &hi, &lo);
       v = k == kColB2 ? hi : lo;
     } else if (r < kH3 && (k == kColB3 || k == kColB3 + 1)) {
-      split_bf16(P[kOffB3 + r], &hi, &lo);
+      split_f16(P[kOffB3 + r], &hi, &lo);
       v = k == kColB3 ? hi : lo;
     }
-    *reinterpret_cast<uint16_t*>(sW1 + umma::sw128_offset(128, r, k)) = to_bf16(v);
-    *reinterpret_cast<uint16_t*>(sOne + umma::sw128_offset(128, r, k)) = to_bf16(k < 2 ? 1.0f : 0.0f);
+    *reinterpret_cast<uint16_t*>(sW1 + umma::sw128_offset(128, r, k)) = to_f16(v);
+    *reinterpret_cast<uint16_t*>(sOne + umma::sw128_offset(128, r, k)) = to_f16(k < 2 ? 1.0f : 0.0f);
   }
   for (int q = threadIdx.x; q < 128 * 128; q += blockDim.x) {
     const int r = q >> 7, k = q & 127;
-    *reinterpret_cast<uint16_t*>(sW2 + umma::sw128_offset(128, r, k)) = to_bf16(P[kOffW2 + q]);
+    *reinterpret_cast<uint16_t*>(sW2 + umma::sw128_offset(128, r, k)) = to_f16(P[kOffW2 + q]);
   }
   for (int q = threadIdx.x; q < 64 * 128; q += blockDim.x) {
     const int r = q >> 7, k = q & 127;
-    *reinterpret_cast<uint16_t*>(sW3 + umma::sw128_offset(64, r, k)) = to_bf16(P[kOffW3 + q]);
+    *reinterpret_cast<uint16_t*>(sW3 + umma::sw128_offset(64, r, k)) = to_f16(P[kOffW3 + q]);
   }
   for (int q = threadIdx.x; q < 16 * 64; q += blockDim.x) {
     const int r = q >> 6, k = q & 63;
     float hi, lo;
-    split_bf16(P[kOffW4 + k], &hi, &lo);
-    *reinterpret_cast<uint16_t*>(sW4 + umma::sw128_offset(16, r, k)) = to_bf16(r == 0 ? hi : r == 1 ? lo : 0.0f);
+    split_f16(P[kOffW4 + k], &hi, &lo);
+    *reinterpret_cast<uint16_t*>(sW4 + umma::sw128_offset(16, r, k)) = to_f16(r == 0 ? hi : r == 1 ? lo : 0.0f);
   }
 }
 
@@ -189,9 +191,9 @@ __device__ __forceinline__ void act_store16(unsigned char* rowp, int r7s, int c,
 #pragma unroll
   for (int i = 0; i < 8; i++) {
     if constexpr (ACT == CBMV_ACT_GELU)
-      h[i] = gelu_bf16x2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
+      h[i] = gelu_f16x2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
     else
-      h[i] = relu_bf16x2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
+      h[i] = relu_f16x2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
   }
 #pragma unroll
   for (int q = 0; q < 2; q++)
@@ -305,8 +307,8 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   const uint32_t tacc = tmem_base + (uint32_t)(g * 128);
   const uint32_t tlane = tacc + ((uint32_t)(wq * 32) << 16);
   const bool leader = row == 0;
-  constexpr uint32_t id128 = umma::idesc_bf16(128, 128), id64 = umma::idesc_bf16(128, 64),
-                     id16 = umma::idesc_bf16(128, 16);
+  constexpr uint32_t id128 = umma::idesc_f16(128, 128), id64 = umma::idesc_f16(128, 64),
+                     id16 = umma::idesc_f16(128, 16);
   // operand descriptors, formed where the leader issues (keeps them out of the other threads' registers)
 #define DESC(ptr) umma::sw128_desc(umma::smem_u32(ptr))
 
@@ -353,11 +355,11 @@ __global__ void __launch_bounds__(kInfThreads, 1)
 #pragma unroll
       for (int k = 0; k < 20; k += 2) {
         const float4 na = s_nrm[k], nb = s_nrm[k + 1];
-        u[k >> 1] = pack_bf16x2((fminf(f[k], na.x) - na.y) * na.z, (fminf(f[k + 1], nb.x) - nb.y) * nb.z);
+        u[k >> 1] = pack_f16x2((fminf(f[k], na.x) - na.y) * na.z, (fminf(f[k + 1], nb.x) - nb.y) * nb.z);
       }
       *tile_chunk(rowp, r7s, 1, 0) = make_uint4(u[0], u[1], u[2], u[3]);
       *tile_chunk(rowp, r7s, 1, 1) = make_uint4(u[4], u[5], u[6], u[7]);
-      *tile_chunk(rowp, r7s, 1, 2) = make_uint4(u[8], u[9], kBf16OneOne, 0u);
+      *tile_chunk(rowp, r7s, 1, 2) = make_uint4(u[8], u[9], kF16OneOne, 0u);
       *tile_chunk(rowp, r7s, 1, 3) = make_uint4(0u, 0u, 0u, 0u);
     }
     // advance to this thread's next sample (tile + tstride) and load its
@@ -378,8 +380,8 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     // 2. layer 1 (K = 32) -> accumulator columns 0..127
     if (leader) {
       const uint64_t dX = DESC(sA + 128 * 128), dW1 = DESC(sW1);
-      umma::mma_bf16(tacc, dX, dW1, id128, false);
-      umma::mma_bf16(tacc, dX + 2, dW1 + 2, id128, true);
+      umma::mma_f16(tacc, dX, dW1, id128, false);
+      umma::mma_f16(tacc, dX + 2, dW1 + 2, id128, true);
       umma::mma_commit(bar0);
     }
     if (!(ok = wait(bar0, ph0))) break;
@@ -388,11 +390,11 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     // 3. layer 2 (K = 128) onto the bias b2
     if (leader) {
       const uint64_t dA0 = DESC(sA), dA1 = DESC(sA + 128 * 128), dW20 = DESC(sW2), dW21 = DESC(sW2 + 128 * 128);
-      umma::mma_bf16(tacc, DESC(sOne), DESC(sW1) + 2 * (kColB2 / 16), id128, false);
+      umma::mma_f16(tacc, DESC(sOne), DESC(sW1) + 2 * (kColB2 / 16), id128, false);
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA0 + 2 * kk, dW20 + 2 * kk, id128, true);
+      for (int kk = 0; kk < 4; kk++) umma::mma_f16(tacc, dA0 + 2 * kk, dW20 + 2 * kk, id128, true);
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA1 + 2 * kk, dW21 + 2 * kk, id128, true);
+      for (int kk = 0; kk < 4; kk++) umma::mma_f16(tacc, dA1 + 2 * kk, dW21 + 2 * kk, id128, true);
       umma::mma_commit(bar0);
     }
     if (!(ok = wait(bar0, ph0))) break;
@@ -401,11 +403,11 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     // 4. layer 3 (N = 64) onto the bias b3
     if (leader) {
       const uint64_t dA0 = DESC(sA), dA1 = DESC(sA + 128 * 128), dW30 = DESC(sW3), dW31 = DESC(sW3 + 64 * 128);
-      umma::mma_bf16(tacc, DESC(sOne), DESC(sW1) + 2 * (kColB3 / 16), id64, false);
+      umma::mma_f16(tacc, DESC(sOne), DESC(sW1) + 2 * (kColB3 / 16), id64, false);
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA0 + 2 * kk, dW30 + 2 * kk, id64, true);
+      for (int kk = 0; kk < 4; kk++) umma::mma_f16(tacc, dA0 + 2 * kk, dW30 + 2 * kk, id64, true);
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc, dA1 + 2 * kk, dW31 + 2 * kk, id64, true);
+      for (int kk = 0; kk < 4; kk++) umma::mma_f16(tacc, dA1 + 2 * kk, dW31 + 2 * kk, id64, true);
       umma::mma_commit(bar0);
     }
     if (!(ok = wait(bar0, ph0))) break;
@@ -415,7 +417,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     if (leader) {
       const uint64_t dA0 = DESC(sA), dW4 = DESC(sW4);
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++) umma::mma_bf16(tacc + 64, dA0 + 2 * kk, dW4 + 2 * kk, id16, kk > 0);
+      for (int kk = 0; kk < 4; kk++) umma::mma_f16(tacc + 64, dA0 + 2 * kk, dW4 + 2 * kk, id16, kk > 0);
       umma::mma_commit(bar0);
     }
     if (!(ok = wait(bar0, ph0))) break;

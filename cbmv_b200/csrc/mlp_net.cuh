@@ -4,6 +4,7 @@
 // state of a network (struct cbmv_mlp).
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "common.cuh"
 
@@ -26,36 +27,40 @@ __device__ __forceinline__ float relu_t(float x, float* drelu) {
 }
 
 // The network's GELU, x * Phi(x) with Phi the standard normal CDF, computed
-// in bfloat16 arithmetic (the activation is stored as bf16 anyway), on the
-// packed half-precision FMA pipe, without the special-function unit:
-//   x <- bf16(x);  u = x * x;  p = G2 u + G1;  p = p u + G0;
-//   q = min(max(x p + 0.5, 0), 1);  gelu = x * q
-// every operation one bf16 rounding (round to nearest even), q ~ Phi(x).
-// G0..G2 (bf16) are a minimax fit of x * clamp(0.5 + x (G0 + G1 x^2 + G2 x^4),
-// 0, 1) to x * Phi(x), then the bf16 coefficients searched for the smallest
-// error of this bf16 evaluation: over every bf16 x, |gelu(x) - x Phi(x)|
-// <= 1.21e-2 (rounding x Phi(x) itself to bf16 costs up to 7.8e-3); the
-// clamp makes it x for x >= 3.5 and 0 (-0) for x <= -3.5.  Training and
-// the fused inference kernel (two lanes at a time) evaluate it identically.
-constexpr uint16_t kG0Bits = 0x3ebf, kG1Bits = 0xbd30, kG2Bits = 0x3b1c;  // 0.373046875, -0.04296875, 0.00238037109375
+// in half-precision (binary16) arithmetic (the fused inference stores its
+// activations as f16 anyway), on the packed half-precision FMA pipe,
+// without the special-function unit:
+//   x <- f16(x);  u = x * x;  p = G2 u + G1;  p = p u + G0;
+//   q = sat(x p + 0.5) (clamped to [0, 1]);  gelu = x * q
+// every operation one f16 rounding (round to nearest even), q ~ Phi(x).
+// G0..G2 (f16) are a minimax fit of x * clamp(0.5 + x (G0 + G1 x^2 + G2 x^4),
+// 0, 1) to x * Phi(x), then the f16 coefficients searched for the smallest
+// error of this f16 evaluation: over every finite f16 x, |gelu(x) - x Phi(x)|
+// <= 8.32e-3 (the polynomial itself is within 7.7e-3; rounding x Phi(x) to
+// f16 costs up to 9.8e-4 below 8); the clamp makes it x for x >= 3.5 and 0
+// (-0) for x <= -3.5; x is saturated to +-65504 when it is rounded to f16,
+// and where x * x overflows q is 1 or 0, so the value stays finite (x or
+// -0).  Training and the fused inference
+// kernel (two lanes at a time, `fma.rn.sat.f16x2` for the clamp) evaluate
+// it identically.
+constexpr uint16_t kG0Bits = 0x35fe, kG1Bits = 0xa977, kG2Bits = 0x18a7;  // 0.37451171875, -0.042694091796875, 0.0022716522216796875
 
-__device__ __forceinline__ __nv_bfloat16 bf16_bits(uint16_t b) { return __ushort_as_bfloat16(b); }
+__device__ __forceinline__ __half f16_bits(uint16_t b) { return __ushort_as_half(b); }
 
-// GELU of x (float32 in, its bf16 rounding used) and, for the backward pass,
+// GELU of x (float32 in, its f16 rounding used) and, for the backward pass,
 // the derivative of the smooth function it approximates at that point:
 // q + x (p + 2 u p'(u)) where 0 < x p + 0.5 < 1, else q (0 or 1), in float32.
 __device__ __forceinline__ float gelu_t(float x, float* dgelu) {
-  const __nv_bfloat16 xb = __float2bfloat16_rn(x);
-  const __nv_bfloat16 u = __hmul(xb, xb);
-  __nv_bfloat16 p = __hfma(bf16_bits(kG2Bits), u, bf16_bits(kG1Bits));
-  p = __hfma(p, u, bf16_bits(kG0Bits));
-  __nv_bfloat16 q = __hfma_relu(xb, p, __float2bfloat16_rn(0.5f));
-  q = __hmin(q, __float2bfloat16_rn(1.0f));
-  const float g = __bfloat162float(__hmul(xb, q));
+  const __half xh = __float2half_rn(fminf(fmaxf(x, -65504.0f), 65504.0f));  // saturated, as the fused kernel's cvt
+  const __half u = __hmul(xh, xh);
+  __half p = __hfma(f16_bits(kG2Bits), u, f16_bits(kG1Bits));
+  p = __hfma(p, u, f16_bits(kG0Bits));
+  const __half q = __hfma_sat(xh, p, __float2half_rn(0.5f));
+  const float g = __half2float(__hmul(xh, q));
   if (dgelu) {
-    const float xf = __bfloat162float(xb), uf = xf * xf;
-    const float g0 = __bfloat162float(bf16_bits(kG0Bits)), g1 = __bfloat162float(bf16_bits(kG1Bits)),
-                g2 = __bfloat162float(bf16_bits(kG2Bits));
+    const float xf = __half2float(xh), uf = xf * xf;
+    const float g0 = __half2float(f16_bits(kG0Bits)), g1 = __half2float(f16_bits(kG1Bits)),
+                g2 = __half2float(f16_bits(kG2Bits));
     const float pf = fmaf(fmaf(g2, uf, g1), uf, g0);
     const float qr = fmaf(xf, pf, 0.5f);
     const float dq = fmaf(2.0f * uf, fmaf(2.0f * g2, uf, g1), pf);  // d(x p(x^2))/dx
@@ -71,6 +76,10 @@ __device__ __forceinline__ float act_t(int act, float x, float* d) {
 
 __device__ __forceinline__ uint16_t to_bf16(float x) {
   return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+}
+// float32 -> f16 bits, round to nearest even, saturated to +-65504
+__device__ __forceinline__ uint16_t to_f16(float x) {
+  return __half_as_ushort(__float2half_rn(fminf(fmaxf(x, -65504.0f), 65504.0f)));
 }
 
 }  // namespace

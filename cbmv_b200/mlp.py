@@ -1,4 +1,5 @@
-"""The learned classifier: a BF16 MLP standing in for the reference's random
+"""The learned classifier: a 16-bit MLP (bf16 training, f16 fused inference)
+standing in for the reference's random
 forest (test.py:603-620) as the per-(pixel, d) matching-probability model.
 
     net = MlpParams.init(seed, stats)        # fresh weights + input transform

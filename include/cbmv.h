@@ -231,10 +231,12 @@ int cbmv_mlp_gradients(cbmv_mlp* m, const float* X, const float* y, float* grads
 int cbmv_mlp_status(const cbmv_mlp* m, int* status);
 /* Hidden-layer activation, CBMV_ACT_RELU or CBMV_ACT_GELU, used by training
  * and by the fused inference of cbmv_run_mlp alike.  The GELU is x * Phi(x)
- * evaluated in bfloat16 operations as x * clamp(0.5 + x p(x^2), 0, 1) with a
- * fixed quadratic p (within 1.21e-2 of the exact erf form on every bf16 x;
- * the bf16 rounding of the exact value alone costs up to 7.8e-3); it runs
- * on the packed half-precision FMA pipe, not the special-function unit.  No
+ * evaluated in IEEE half-precision operations as x * clamp(0.5 + x p(x^2),
+ * 0, 1) with a fixed quadratic p (within 8.32e-3 of the exact erf form on
+ * every finite f16 x; the polynomial itself is within 7.7e-3); it runs on
+ * the packed half-precision FMA pipe, not the special-function unit.  The
+ * fused inference runs the network on f16 operands (inputs, weights,
+ * activations; float32 accumulation, biases as f16 high + low parts).  No
  * counterpart in the reference (its classifier is the random forest). */
 int cbmv_mlp_set_activation(cbmv_mlp* m, int act);
 int cbmv_mlp_get_activation(const cbmv_mlp* m, int* act);

@@ -34,29 +34,51 @@ def bf16_rn(x):
     return r.view(np.float64)
 
 
-# the network's GELU coefficients (cbmv_b200/csrc/mlp_net.cuh, gelu_t), bf16 values
-G = np.array([0.373046875, -0.04296875, 0.00238037109375])
+def f16(x):
+    """Round float64/float32 values to IEEE binary16 directly (round to
+    nearest even; beyond 65504 to infinity), returned as float64."""
+    with np.errstate(over="ignore"):
+        return np.asarray(x, np.float64).astype(np.float16).astype(np.float64)
 
 
-def gelu_bf16(x):
+def f16_sat(x):
+    """f16 rounding saturated to the largest finite value, +-65504 (the
+    device's `cvt.rn.satfinite` of its float32 accumulators)."""
+    return np.clip(f16(x), -65504.0, 65504.0)
+
+
+def f16_acc(x):
+    """A float32 accumulator's value rounded to f16 as the device converts
+    it: through float32, saturated."""
+    return f16_sat(np.asarray(x, np.float32))
+
+
+# the network's GELU coefficients (cbmv_b200/csrc/mlp_net.cuh, gelu_t), f16 values
+G = np.array([0.37451171875, -0.042694091796875, 0.0022716522216796875])
+
+
+def gelu_f16(x):
     """The network's GELU as the device evaluates it: x rounded from float32
-    to bf16, then u = x*x, p = G2 u + G1, p = p u + G0, q = min(max(x p +
-    0.5, 0), 1), x*q, each operation rounded once to bf16 (mlp_net.cuh
-    gelu_t; the fused kernel's packed form is the same)."""
-    xb = bf16(x)  # through float32, as the device rounds its float32 accumulator
-    u = bf16_rn(xb * xb)
-    p = bf16_rn(G[2] * u + G[1])
-    p = bf16_rn(p * u + G[0])
-    q = np.maximum(bf16_rn(xb * p + 0.5), 0.0)
-    q = np.minimum(q, 1.0)
-    return bf16_rn(xb * q)
+    to f16, then u = x*x, p = G2 u + G1, p = p u + G0, q = x p + 0.5
+    clamped to [0, 1], x*q, each operation rounded once to f16 (mlp_net.cuh
+    gelu_t; the fused kernel's packed form is the same, its clamp folded
+    into the FMA).  Every product of two f16 values, and the FMAs here, are
+    exact in float64 before that one rounding."""
+    xh = f16_acc(x)
+    with np.errstate(over="ignore", invalid="ignore"):
+        u = f16(xh * xh)
+        p = f16(G[2] * u + G[1])
+        p = f16(p * u + G[0])
+        q = f16(xh * p + 0.5)
+    q = np.where(np.isnan(q), 0.0, np.clip(q, 0.0, 1.0))
+    return f16(xh * q)
 
 
 def gelu(x):
-    """The network's GELU (bf16 evaluation) and, for the backward pass, the
-    derivative of the smooth function it approximates at bf16(x)."""
-    g = gelu_bf16(x)
-    xb = bf16(x)  # through float32, as the device rounds its float32 accumulator
+    """The network's GELU (f16 evaluation) and, for the backward pass, the
+    derivative of the smooth function it approximates at f16(x)."""
+    g = gelu_f16(x)
+    xb = f16_acc(x)
     u = xb * xb
     p = (G[2] * u + G[1]) * u + G[0]
     qr = 0.5 + xb * p
@@ -123,33 +145,34 @@ def loss_and_grads(vec, X, y, act="relu"):
     return loss, g, prob
 
 
-def split_bf16(x):
-    """bf16 high part of float32 x and the bf16 rounding of the rest."""
+def split_f16(x):
+    """f16 high part of float32 x and the f16 rounding of the rest (the
+    rest formed in float32)."""
     x = np.asarray(x, np.float32)
-    hi = bf16(x)
-    return hi, bf16(x - np.float32(hi))
+    hi = f16_sat(x)
+    return hi, f16_sat(x - np.float32(hi))
 
 
 def forward_fused(vec, X, act="relu"):
     """The network as the fused inference kernel evaluates it (test
-    infrastructure): every bias (and w4) enters as its bf16 high + low
-    parts; hidden activations are ReLU of the float32 accumulator rounded to
-    bf16, or the bf16 GELU of it; the output layer runs on those bf16
-    activations.  Returns z."""
+    infrastructure): f16 operands throughout -- the normalised inputs, the
+    weights, the hidden activations (ReLU of the float32 accumulator rounded
+    to f16, or the f16 GELU of it) -- every bias (and w4) as its f16 high +
+    low parts; the output layer runs on those f16 activations.  Returns z."""
     if act == "gelu":
         def h(s):
-            return gelu_bf16(s)
+            return gelu_f16(s)
     else:
         def h(s):
-            return bf16(np.maximum(s, 0))
+            return f16_sat(np.maximum(np.asarray(s, np.float32), 0))
     p = unpack(vec)
     c32, m32, s32 = (np.float32(p[k]) for k in ("cap", "mu", "inv_sd"))
-    X0 = bf16((np.minimum(np.asarray(X, np.float32), c32) - m32) * s32)
-    b1h, b1l = split_bf16(p["b1"])
-    b2h, b2l = split_bf16(p["b2"])
-    b3h, b3l = split_bf16(p["b3"])
-    wh, wl = split_bf16(p["w4"])
-    A1 = h(X0 @ bf16(p["W1"]).T + (b1h + b1l))
-    A2 = h(A1 @ bf16(p["W2"]).T + (b2h + b2l))
-    A3 = h(A2 @ bf16(p["W3"]).T + (b3h + b3l))
+    X0 = f16_sat((np.minimum(np.asarray(X, np.float32), c32) - m32) * s32)
+    b1h, b1l = split_f16(p["b1"])
+    b2h, b2l = split_f16(p["b2"])
+    b3h, b3l = split_f16(p["b3"])
+    wh, wl = split_f16(p["w4"])
+    A1 = h(X0 @ f16_sat(np.float32(p["W1"])).T + (b1h + b1l))
+    A2 = h(A1 @ f16_sat(np.float32(p["W2"])).T + (b2h + b2l))
+    A3 = h(A2 @ f16_sat(np.float32(p["W3"])).T + (b3h + b3l))
     return A3 @ (wh + wl) + p["b4"][0]

@@ -81,12 +81,12 @@ def test_mlp_training_reduces_loss(gpu, act):
 @pytest.mark.parametrize("act", ["relu", "gelu"])
 def test_fused_inference_matches_oracle_forward(gpu, small_pair, act):
     """cbmv_run_mlp's matching cost (float32 features + four tcgen05 layers
-    fused, bf16 ReLU or GELU activations, biases as bf16 high + low parts) against
-    (a) the oracle's model of the same arithmetic: max 5e-3, mean 3e-4 on P
-    -- the kernel's float32 features and accumulation order move a bf16
-    rounding of an input or activation here and there; (b) the float64
-    network on the same features: max 3e-2, mean 2e-3 -- the cost of bf16
-    activations."""
+    fused on f16 operands, f16 ReLU or GELU activations, biases as f16 high
+    + low parts) against (a) the oracle's model of the same arithmetic: max
+    5e-3, mean 3e-4 on P -- the kernel's float32 features and accumulation
+    order move an f16 rounding of an input or activation here and there;
+    (b) the float64 network on the same features: max 3e-2, mean 2e-3 --
+    the cost of 16-bit activations."""
     from cbmv_b200.mlp import GpuMlp, MlpParams, input_stats
     from cbmv_b200.pipeline import StereoPipeline
     from oracle import mlp_ref

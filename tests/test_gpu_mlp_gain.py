@@ -3,7 +3,7 @@
 On held-out seeded 694x554, D=128 pairs, the same test path (matchers, 20
 features, classifier, MC-CNN `_mem` post) is run three ways:
 
-- with the trained bf16 GELU network (tests/golden/mlp_gelu_694x554.npz,
+- with the trained GELU network (tests/golden/mlp_gelu_694x554.npz,
   trained by cbmv_b200/train_mlp.py on GPU-emitted samples of pairs
   2000..2199);
 - with the same network before training (its random initialisation, same

@@ -138,7 +138,7 @@ def test_learned_path_matches_reference_path(gpu, oracle_cpu, W, H, D, net_kind)
     then eval_prob with the _mem post in the reference's summation order):
     disparities within 0.5 px on >= 99.9 % of pixels, the bar for final
     disparity maps (the device forms the features in float32 and rounds
-    activations to bf16; the oracle models that arithmetic from the
+    activations to f16; the oracle models that arithmetic from the
     float64 features)."""
     import os
     from oracle import glue, mlp_ref

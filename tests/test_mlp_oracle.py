@@ -1,32 +1,36 @@
 """The float64 network restatement (oracle/mlp_ref.py) is itself checked
-against central finite differences of its own loss (no bf16 rounding in
-this check), so the GPU gradient test rests on a verified backward pass."""
+against central finite differences of its own loss (no bf16 or f16
+rounding in this check), so the GPU gradient test rests on a verified
+backward pass."""
 import numpy as np
 import pytest
 
 
-def test_gelu_against_erf_and_bf16_emulation():
-    """The network's GELU, evaluated in bf16 operations, is within 1.21e-2 of
-    x * Phi(x) on every bf16 value (rounding x * Phi(x) to bf16 alone costs
-    up to 7.8e-3), exactly x / 0 in the tails; its emulation rounds float64
-    to bf16 directly (no detour through float32); the backward pass's
-    derivative is the smooth function's (central differences)."""
+def test_gelu_against_erf_and_f16_emulation():
+    """The network's GELU, evaluated in f16 operations, is within 8.32e-3 of
+    x * Phi(x) on every finite f16 value (the clamped polynomial itself is
+    within 7.7e-3), exactly x / 0 in the tails and finite up to +-65504
+    (saturated input, overflowing x*x); its emulation rounds float64 to f16
+    directly (ties to even); the backward pass's derivative is the smooth
+    function's (central differences)."""
     from scipy.special import erf
     from oracle import mlp_ref
-    mant = np.arange(128)
-    xs = np.unique(np.concatenate([s * (1 + mant / 128.0) * 2.0 ** e for e in range(-30, 7) for s in (1, -1)]))
+    xs = np.arange(65536, dtype=np.uint16).view(np.float16).astype(np.float64)
+    xs = np.unique(xs[np.isfinite(xs)])
     exact = 0.5 * xs * (1 + erf(xs / np.sqrt(2)))
-    g = mlp_ref.gelu_bf16(xs)
-    assert np.max(np.abs(g - exact)) <= 1.21e-2
-    assert np.all(g[xs >= 3.5] == mlp_ref.bf16(xs[xs >= 3.5])) and np.all(g[xs <= -3.5] == 0)
-    assert np.array_equal(mlp_ref.bf16_rn(g), g)                      # bf16 values
-    v = np.array([1 + 2.0 ** -8, 1 + 3 * 2.0 ** -8, 1 + 2.0 ** -8 + 2.0 ** -40])
-    assert list(mlp_ref.bf16_rn(v)) == [1.0, 1 + 2.0 ** -6, 1 + 2.0 ** -7]  # ties to even; above a tie rounds up
+    g = mlp_ref.gelu_f16(xs)
+    assert np.isfinite(g).all()
+    assert np.max(np.abs(g - exact)) <= 8.32e-3
+    assert np.all(g[xs >= 3.5] == xs[xs >= 3.5]) and np.all(g[xs <= -3.5] == 0)
+    assert np.array_equal(mlp_ref.f16(g), g)                          # f16 values
+    v = np.array([1 + 2.0 ** -11, 1 + 3 * 2.0 ** -11, 1 + 2.0 ** -11 + 2.0 ** -40])
+    assert list(mlp_ref.f16(v)) == [1.0, 1 + 2.0 ** -9, 1 + 2.0 ** -10]   # ties to even; above a tie rounds up
+    assert list(mlp_ref.f16_sat(np.array([7e4, -7e4]))) == [65504.0, -65504.0]
+    assert list(mlp_ref.gelu_f16(np.array([1e6, -1e6]))) == [65504.0, 0.0]
     h = 1e-6
     xm = np.linspace(-3.2, 3.2, 1001)
     smooth = lambda x: x * np.clip(0.5 + x * ((mlp_ref.G[2] * x * x + mlp_ref.G[1]) * x * x + mlp_ref.G[0]), 0, 1)
-    fd = (smooth(xm + h) - smooth(xm - h)) / (2 * h)
-    xb = mlp_ref.bf16(xm.astype(np.float32))
+    xb = mlp_ref.f16(xm.astype(np.float32))
     fdb = (smooth(xb + h) - smooth(xb - h)) / (2 * h)
     assert np.max(np.abs(fdb - mlp_ref.gelu(xm)[1])) < 1e-5
 
@@ -34,8 +38,8 @@ def test_gelu_against_erf_and_bf16_emulation():
 @pytest.mark.parametrize("act", ["relu", "gelu"])
 def test_oracle_backward_matches_finite_differences(monkeypatch, act):
     from oracle import mlp_ref
-    monkeypatch.setattr(mlp_ref, "bf16", lambda x: np.asarray(x, np.float64))
-    monkeypatch.setattr(mlp_ref, "bf16_rn", lambda x: np.asarray(x, np.float64))
+    for name in ("bf16", "bf16_rn", "f16", "f16_sat", "f16_acc"):
+        monkeypatch.setattr(mlp_ref, name, lambda x: np.asarray(x, np.float64))
     rng = np.random.default_rng(0)
     n = 37
     X = rng.normal(size=(n, 20))
@@ -59,10 +63,10 @@ def test_oracle_backward_matches_finite_differences(monkeypatch, act):
 
 @pytest.mark.parametrize("act", ["relu", "gelu"])
 def test_fused_model_close_to_float64_network(act):
-    """The oracle's model of the fused inference kernel (bf16 inputs,
-    weights and ReLU activations, biases as bf16 high + low parts) stays
-    within bf16 rounding of the float64 network, and the high + low split
-    reproduces each bias to 2^-16 relative."""
+    """The oracle's model of the fused inference kernel (f16 inputs, weights
+    and activations, biases as f16 high + low parts) stays within f16
+    rounding of the float64 network, and the high + low split reproduces
+    each bias to 2^-21 relative (above the f16 subnormal range)."""
     from oracle import mlp_ref
     rng = np.random.default_rng(1)
     sizes = [20, 20, 20, 128 * 20, 128, 128 * 128, 128, 64 * 128, 64, 64, 1]
@@ -75,5 +79,5 @@ def test_fused_model_close_to_float64_network(act):
     assert np.abs(z_model - z_exact).max() < 0.05 * scale
     assert np.abs(z_model - z_exact).mean() < 0.01 * scale
     b = mlp_ref.unpack(vec)["b2"].astype(np.float32)
-    hi, lo = mlp_ref.split_bf16(b)
-    assert np.all(np.abs((hi + lo) - b) <= 2.0 ** -16 * np.abs(b) + 1e-30)
+    hi, lo = mlp_ref.split_f16(b)
+    assert np.all(np.abs((hi + lo) - b) <= 2.0 ** -21 * np.abs(b) + 2.0 ** -25)
