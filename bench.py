@@ -226,10 +226,11 @@ def launches_per_pair(prm):
     images; the ZSAD strip kernel of window 5 forms its window means itself,
     another window adds their 2 launches), 4 cost volumes, 2 row
     statistics, 1 features+classifier; post: 4 image normalisation, 2
-    cross, 1 SGM neighbour differences, 2 per SGM iteration, 1 CBCA support
-    build and 1 per CBCA pass, WTA+subpixel, median per iteration,
-    mean2d."""
-    post = 4 + 2 + (1 + 2 * prm.sgm_i if prm.sgm_i else 0) + (1 + prm.cbca_i2 if prm.cbca_i2 else 0) \
+    cross, 2 SGM neighbour differences (one per image), 2 per SGM
+    iteration, 1 CBCA support build and 1 per CBCA pass, WTA+subpixel,
+    median per iteration, mean2d (33 with the defaults, as an ncu launch
+    list of the headline step counts them per pass)."""
+    post = 4 + 2 + (2 + 2 * prm.sgm_i if prm.sgm_i else 0) + (1 + prm.cbca_i2 if prm.cbca_i2 else 0) \
         + (1 + prm.cbca_i1 if prm.cbca_i1 else 0) + 1 + prm.median_i + 1
     return (6 if prm.sadw == 5 else 8) + 4 + 2 + 1 + post
 

@@ -860,16 +860,31 @@ __global__ void wta_subpixel_hwd_kernel(const float* __restrict__ c, int64_t HW,
   const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < HW; p += nw) {
     const float* r = c + p * D;
-    float bv = __int_as_float(0x7f800000);
     int bd = 0x7fffffff;
-    for (int d = lane; d < D; d += 32) {
-      const float v = r[d];
-      if (v < bv) { bv = v; bd = d; }
-    }
-    for (int o = 16; o; o >>= 1) {
-      const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
-      const int od = __shfl_xor_sync(0xffffffffu, bd, o);
-      if (ov < bv || (ov == bv && od < bd)) { bv = ov; bd = od; }
+    if (D <= 128) {
+      // the minimum over d (NaN ignored), then the first d that holds it;
+      // as in the loop below, +inf is never a winner
+      float v[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) v[k] = lane + 32 * k < D ? r[lane + 32 * k] : __int_as_float(0x7fc00000);
+      float mn = fminf(fminf(v[0], v[1]), fminf(v[2], v[3]));
+      asm volatile("redux.sync.min.f32 %0, %0, 0xffffffff;" : "+f"(mn));
+      unsigned first = 0x7fffffffu;
+#pragma unroll
+      for (int k = 3; k >= 0; k--)
+        if (v[k] == mn && mn < __int_as_float(0x7f800000)) first = (unsigned)(lane + 32 * k);
+      bd = (int)__reduce_min_sync(0xffffffffu, first);
+    } else {
+      float bv = __int_as_float(0x7f800000);
+      for (int d = lane; d < D; d += 32) {
+        const float v = r[d];
+        if (v < bv) { bv = v; bd = d; }
+      }
+      for (int o = 16; o; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int od = __shfl_xor_sync(0xffffffffu, bd, o);
+        if (ov < bv || (ov == bv && od < bd)) { bv = ov; bd = od; }
+      }
     }
     if (bd == 0x7fffffff) bd = 0;  // all NaN: np.argmin would return 0 for a NaN at 0
     if (lane == 0) {
@@ -969,6 +984,46 @@ __global__ void mean2d_kernel(const float* __restrict__ img, int64_t H, int64_t 
         }
     out[id] = sum / cnt;
   }
+}
+
+// mean2d for kernels up to 15 x 15 (the pipeline's: blur_sigma <= 2.33):
+// a 16 x 16 block of pixels stages its (16 + 2r)^2 window of the image in
+// shared memory, pixels outside the image as NaN (so the |v - c| < alpha2
+// test drops them, as mean2d_kernel's bounds test does), and the weights;
+// the taps run in mean2d_kernel's order (xx outer, yy inner) with the same
+// fused multiply-add, so the results are the same bit for bit.
+constexpr int kMeanTile = 16, kMeanMaxR = 7;
+__global__ void __launch_bounds__(kMeanTile * kMeanTile) mean2d_tiled_kernel(const float* __restrict__ img, int H,
+                                                                           int W, const float* __restrict__ kernel,
+                                                                           int r, float alpha2, float* __restrict__ out) {
+  constexpr int TS = kMeanTile + 2 * kMeanMaxR;
+  __shared__ float tile[TS][TS + 1];
+  __shared__ float kw[(2 * kMeanMaxR + 1) * (2 * kMeanMaxR + 1)];
+  const int ks = 2 * r + 1, span = kMeanTile + 2 * r;
+  const int X0 = blockIdx.x * kMeanTile, Y0 = blockIdx.y * kMeanTile;
+  const int tx = threadIdx.x % kMeanTile, ty = threadIdx.x / kMeanTile;
+  for (int q = threadIdx.x; q < ks * ks; q += blockDim.x) kw[q] = kernel[q];
+  const float nan = __int_as_float(0x7fc00000);
+  for (int q = threadIdx.x; q < span * span; q += blockDim.x) {
+    const int ry = q / span, rx = q - ry * span;
+    const int yy = Y0 - r + ry, xx = X0 - r + rx;
+    tile[ry][rx] = (yy >= 0 && yy < H && xx >= 0 && xx < W) ? img[(int64_t)yy * W + xx] : nan;
+  }
+  __syncthreads();
+  const int x = X0 + tx, y = Y0 + ty;
+  if (x >= W || y >= H) return;
+  const float c = tile[ty + r][tx + r];
+  float sum = 0.0f, cnt = 0.0f;
+  int i = 0;
+  for (int xo = 0; xo < ks; xo++)
+    for (int yo = 0; yo < ks; yo++, i++) {
+      const float v = tile[ty + yo][tx + xo];
+      if (fabsf(v - c) < alpha2) {
+        sum = fmaf(v, kw[i], sum);
+        cnt += kw[i];
+      }
+    }
+  out[(int64_t)y * W + x] = sum / cnt;
 }
 
 // outlier_detection (post.cu:717-754)
@@ -1267,6 +1322,11 @@ int launch_median(const float* in, int64_t H, int64_t W, int k, float* out, cuda
 
 int launch_mean2d(const float* in, int64_t H, int64_t W, const float* kernel, int ks, float alpha2,
                   float* out, cudaStream_t st) {
+  if (ks / 2 <= kMeanMaxR && H < 65536 * kMeanTile && W < ((int64_t)1 << 30)) {
+    const dim3 grid((unsigned)((W + kMeanTile - 1) / kMeanTile), (unsigned)((H + kMeanTile - 1) / kMeanTile));
+    mean2d_tiled_kernel<<<grid, kMeanTile * kMeanTile, 0, st>>>(in, (int)H, (int)W, kernel, ks / 2, alpha2, out);
+    return check_launch("mean2d");
+  }
   mean2d_kernel<<<grid_for(H * W, kBlock), kBlock, 0, st>>>(in, H, W, kernel, ks / 2, alpha2, out);
   return check_launch("mean2d");
 }

@@ -143,6 +143,25 @@ def test_wta_subpixel_median_mean2d_exact(gpu, oracle_cpu, scene):
     np.testing.assert_allclose(mean.cpu().numpy(), mean_ref, rtol=1e-6, atol=1e-6)
 
 
+@pytest.mark.parametrize("D", [24, 128, 160])
+def test_wta_first_minimum_ties_and_inf_rows(gpu, D):
+    """Winner-take-all is np.argmin along d (test.py:408-409): the first of
+    tied minima, 0 for a row of +inf, at D <= 128 (one reduction of the
+    minimum and one of its first index) and above (the per-lane loop)."""
+    from cbmv_b200 import _lib
+    rng = np.random.default_rng(D)
+    H, W = 6, 40
+    vol = rng.integers(0, 5, (H, W, D)).astype(np.float32)  # many ties
+    vol[0, 0, :] = np.inf
+    vol[0, 1, :] = 7.0
+    vol[0, 2, :] = np.inf
+    vol[0, 2, D - 1] = 1.0  # the only finite value, last
+    ref = np.argmin(vol, axis=2).astype(np.float32)
+    d = torch.empty((H, W), device="cuda")
+    _lib.call("cbmv_wta", _t(vol).data_ptr(), H, W, D, _lib.HWD, d.data_ptr(), None)
+    assert np.array_equal(d.cpu().numpy(), ref)
+
+
 def test_lr_check_and_interpolation_exact(gpu, oracle_cpu):
     from cbmv_b200 import _lib
     rng = np.random.default_rng(4)
