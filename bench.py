@@ -604,7 +604,7 @@ def run_batch(a, ws, rank, local):
         "value": units / (ms / 1e3), "unit": "pixel·disparities/s", "n_gpus": ws, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "strong" if ws > 1 else "weak", "vs_baseline": None,
-        "dtype": "bf16/f32", "data": "synthetic (seeded uneven pairs, seeds 4000+)",
+        "dtype": "f16/f32", "data": "synthetic (seeded uneven pairs, seeds 4000+)",
         "config": {"workload": "%d pairs W~U[320,1500] H~U[240,1000] D in {64,128,192,256}" % n,
                    "units": units,
                    "autotune": {k: tune.get(k) for k in ("streams", "mlp_ctas", "cbca_rows", "sgm_prefetch", "ms",

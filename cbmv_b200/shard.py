@@ -34,6 +34,15 @@ def pair_work(shapes):
     return [int(h) * int(w) * int(d) for h, w, d in shapes]
 
 
+def _distributed(group=None):
+    """(rank, world size) of this process, (0, 1) when no process group is
+    initialised (a single-process run)."""
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized():
+        return 0, 1
+    return dist.get_rank(group), dist.get_world_size(group)
+
+
 def gather_maps(maps, assign, shapes, device=None, group=None):
     """Disparity maps of every pair on rank 0.
 
@@ -42,8 +51,7 @@ def gather_maps(maps, assign, shapes, device=None, group=None):
     returns the list of all maps in pair order; the other ranks None."""
     import torch
     import torch.distributed as dist
-    rank = dist.get_rank(group)
-    ws = dist.get_world_size(group)
+    rank, ws = _distributed(group)
     if len(maps) != len(assign[rank]):
         raise ValueError("rank %d holds %d maps for %d pairs" % (rank, len(maps), len(assign[rank])))
     if rank != 0:
@@ -67,11 +75,12 @@ def gather_values(values, assign, n, device=None, group=None):
     combines them.  values: this rank's numbers in assign[rank] order."""
     import torch
     import torch.distributed as dist
-    rank = dist.get_rank(group)
+    rank, ws = _distributed(group)
     t = torch.zeros(n, dtype=torch.float64, device=device)
     for i, v in zip(assign[rank], values):
         t[i] = float(v)
-    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     return t.cpu().numpy()
 
 
@@ -80,7 +89,7 @@ def max_over_ranks(x, device=None, group=None):
     slowest rank)."""
     import torch
     import torch.distributed as dist
-    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size(group) == 1:
+    if _distributed(group)[1] == 1:
         return float(x)
     t = torch.tensor([float(x)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)

@@ -88,3 +88,19 @@ def test_two_ranks_shard_gather_and_reduce():
     owner = {i: r for r in range(2) for i in a0[r]}
     assert lat0 == lat1 == [10.0 * i + owner[i] for i in range(len(specs))]
     assert t0 == t1 == 6.0                             # both see the slower rank's time
+
+
+def test_shard_functions_without_a_process_group():
+    """A single-process run (no torch.distributed group): the gather
+    returns the maps in pair order, the values as given, the maximum the
+    value itself."""
+    import torch
+    from cbmv_b200 import shard
+    shapes = [(3, 4, 8), (2, 5, 8), (4, 4, 8)]
+    assign = shard.lpt_assign(shard.pair_work(shapes), 1)
+    maps = [torch.full((shapes[i][0], shapes[i][1]), float(i)) for i in assign[0]]
+    out = shard.gather_maps(maps, assign, shapes)
+    assert [float(m[0, 0]) for m in out] == [0.0, 1.0, 2.0]
+    vals = shard.gather_values([10.0 * i for i in assign[0]], assign, 3)
+    assert list(vals) == [0.0, 10.0, 20.0]
+    assert shard.max_over_ranks(2.5) == 2.5
