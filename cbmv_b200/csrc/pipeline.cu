@@ -59,6 +59,10 @@ extern "C" void cbmv_params_default(cbmv_params* p) {
 
 struct cbmv_ctx {
   cudaStream_t stream = nullptr;
+  // a second stream for work that overlaps the main one inside a call (the
+  // CBCA support build runs beside the SGM), ordered by the two events
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   void* ws = nullptr;
   size_t ws_bytes = 0;
   cudaEvent_t ev[6] = {};
@@ -109,6 +113,7 @@ struct Work {
   float* volC;  // the right view's cost of the _interp post (else null)
   float *imL, *imR, *crossL, *crossR, *dtmp, *dtmp2, *dright, *outlier;
   float* grad;  // SGM neighbour differences: left h/v, right h/v
+  uint32_t* masks;  // CBCA support words, 4 B per (p,d), live beside the SGM volumes
   double* mom;
 };
 
@@ -145,6 +150,10 @@ Work carve(void* base, int64_t H, int64_t W, int D, size_t* bytes, bool f32, boo
   w.dright = c.take<float>(HW);
   w.outlier = c.take<float>(HW);
   w.grad = c.take<float>(4 * HW);
+  // the support words: their own volume on the float32 path (the SGM's four
+  // direction volumes take all four matcher volumes), the third float64
+  // matcher volume otherwise (the SGM uses only the first two)
+  w.masks = f32 ? c.take<uint32_t>(V) : reinterpret_cast<uint32_t*>(w.vol[2]);
   w.mom = c.take<double>(4);
   *bytes = c.off + 256;
   return w;
@@ -182,6 +191,12 @@ extern "C" int cbmv_ctx_create(void* stream, cbmv_ctx** out) {
       return set_error(CBMV_ECUDA, "cudaEventCreate failed");
     }
   }
+  if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess) {
+    cbmv_ctx_destroy(c);
+    return set_error(CBMV_ECUDA, "cudaStreamCreate / cudaEventCreate failed");
+  }
   *out = c;
   return CBMV_OK;
 }
@@ -189,9 +204,14 @@ extern "C" int cbmv_ctx_create(void* stream, cbmv_ctx** out) {
 extern "C" int cbmv_ctx_destroy(cbmv_ctx* c) {
   if (!c) return CBMV_OK;
   cudaStreamSynchronize(c->stream);
+  if (c->side) cudaStreamSynchronize(c->side);
   if (c->ws) cudaFree(c->ws);
   if (c->gauss) cudaFree(c->gauss);
-  for (int i = 0; i < 6; i++) cudaEventDestroy(c->ev[i]);
+  for (int i = 0; i < 6; i++)
+    if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+  if (c->join_ev) cudaEventDestroy(c->join_ev);
+  if (c->side) cudaStreamDestroy(c->side);
   delete c;
   return CBMV_OK;
 }
@@ -247,14 +267,27 @@ static int ensure_gaussian(cbmv_ctx* c, float sigma) {
 // the _interp post (test.py:176-251) passes (right, left, -direction), and
 // its SGM keeps the images in their order (test.py:203-207).  `oth` is a
 // second volume; *result receives the buffer holding the result.
-static int cost_chain(const cbmv_params* p, Work& w, int64_t H, int64_t W, int D, const float* crossA,
-                      const float* crossB, int direction, float* cur, float* oth, float** result,
-                      cudaStream_t st) {
+static int cost_chain(cbmv_ctx* c, const cbmv_params* p, Work& w, int64_t H, int64_t W, int D,
+                      const float* crossA, const float* crossB, int direction, float* cur, float* oth,
+                      float** result) {
+  cudaStream_t st = c->stream;
   const int64_t HW = H * W;
-  // the separable form's supports, shared by a run of passes, in the first
-  // matcher volume (dead during the post; the SGM reuses it in between)
+  // the separable form's supports, built once for all the chain's passes
+  // (they depend on the arms only); when every pass follows the SGM, the
+  // build runs on the side stream beside it (the SGM keeps most of the GPU
+  // idle: one warp per scan line) and the main stream waits for it before
+  // the first pass
   const bool masked = !p->exact_cbca && p->L1 - 1 <= kCbcaMaskMaxHalo;
-  uint32_t* masks = reinterpret_cast<uint32_t*>(w.vol[0]);
+  uint32_t* masks = w.masks;
+  const bool beside = masked && p->cbca_i1 == 0 && p->cbca_i2 > 0 && p->sgm_i > 0;
+  if (beside) {
+    CBMV_CUDA(cudaEventRecord(c->fork_ev, st));
+    CBMV_CUDA(cudaStreamWaitEvent(c->side, c->fork_ev, 0));
+    RC(launch_cbca_mask_build(crossA, crossB, H, W, D, direction, masks, c->side));
+    CBMV_CUDA(cudaEventRecord(c->join_ev, c->side));
+  } else if (masked && p->cbca_i1 + p->cbca_i2 > 0) {
+    RC(launch_cbca_mask_build(crossA, crossB, H, W, D, direction, masks, st));
+  }
   auto cbca = [&](const float* in, float* out) {
     const int rows = p->cbca_rows == 16 ? 16 : 32;
     if (p->exact_cbca)
@@ -262,7 +295,6 @@ static int cost_chain(const cbmv_params* p, Work& w, int64_t H, int64_t W, int D
     if (masked) return launch_cbca_masked(masks, in, H, W, D, out, st, rows);
     return launch_cbca_sep(crossA, crossB, in, H, W, D, direction, out, st, p->L1 - 1, rows);
   };
-  if (masked && p->cbca_i1 > 0) RC(launch_cbca_mask_build(crossA, crossB, H, W, D, direction, masks, st));
   for (int i = 0; i < p->cbca_i1; i++) {
     RC(cbca(cur, oth));
     float* t = cur; cur = oth; oth = t;
@@ -279,7 +311,7 @@ static int cost_chain(const cbmv_params* p, Work& w, int64_t H, int64_t W, int D
     RC(launch_sgm_combine(so, V, nullptr, 0.25f, oth, st));
     float* t = cur; cur = oth; oth = t;
   }
-  if (masked && p->cbca_i2 > 0) RC(launch_cbca_mask_build(crossA, crossB, H, W, D, direction, masks, st));
+  if (beside) CBMV_CUDA(cudaStreamWaitEvent(st, c->join_ev, 0));
   for (int i = 0; i < p->cbca_i2; i++) {
     RC(cbca(cur, oth));
     float* t = cur; cur = oth; oth = t;
@@ -310,10 +342,10 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
   if (p->interpolate) {
     // right view (test.py:154, 176-255): its cost, its chain, its argmin
     RC(launch_right_cost_f32(w.volA, H, W, D, w.volC, st));
-    RC(cost_chain(p, w, H, W, D, w.crossR, w.crossL, -p->direction, w.volC, w.volB, &res, st));
+    RC(cost_chain(c, p, w, H, W, D, w.crossR, w.crossL, -p->direction, w.volC, w.volB, &res));
     RC(launch_wta_subpixel(res, H, W, D, w.dright, nullptr, st));
   }
-  RC(cost_chain(p, w, H, W, D, w.crossL, w.crossR, p->direction, w.volA, w.volB, &res, st));
+  RC(cost_chain(c, p, w, H, W, D, w.crossL, w.crossR, p->direction, w.volA, w.volB, &res));
   float* d0 = w.dtmp;
   float* d1 = w.dtmp2;
   if (p->interpolate) {
