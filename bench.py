@@ -30,6 +30,8 @@ the CPU restatement when that build is absent) on that classifier's own
 P(class 0).
 """
 import argparse
+import contextlib
+import ctypes
 import json
 import os
 import subprocess
@@ -623,6 +625,26 @@ def run_batch(a, ws, rank, local):
     }
 
 
+@contextlib.contextmanager
+def native_stdout_to_stderr():
+    """Text that compiled code prints on file descriptor 1 (the reference's
+    post module announces "CUDA initialized.") goes to stderr instead, so
+    that stdout carries only the JSON line."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        yield
+    finally:
+        try:
+            ctypes.CDLL(None).fflush(None)  # C stdio buffers, before fd 1 is restored
+        except OSError:
+            pass
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -651,7 +673,8 @@ def main():
     a = ap.parse_args()
     ws, rank, local = dist_init()
     if a.impl == "reference":
-        line = run_reference(a, ws, rank, local)
+        with native_stdout_to_stderr():
+            line = run_reference(a, ws, rank, local)
     elif a.batch:
         line = run_batch(a, ws, rank, local)
     else:

@@ -62,7 +62,7 @@ struct cbmv_ctx {
   // a second stream for work that overlaps the main one inside a call (the
   // CBCA support build runs beside the SGM), ordered by the two events
   cudaStream_t side = nullptr;
-  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr, prep_ev = nullptr;
   void* ws = nullptr;
   size_t ws_bytes = 0;
   cudaEvent_t ev[6] = {};
@@ -114,6 +114,7 @@ struct Work {
   float *imL, *imR, *crossL, *crossR, *dtmp, *dtmp2, *dright, *outlier;
   float* grad;  // SGM neighbour differences: left h/v, right h/v
   uint32_t* masks;  // CBCA support words, 4 B per (p,d), live beside the SGM volumes
+  bool prepped = false;  // the post's image terms were launched on the side stream (prep_ev)
   double* mom;
 };
 
@@ -193,7 +194,8 @@ extern "C" int cbmv_ctx_create(void* stream, cbmv_ctx** out) {
   }
   if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->prep_ev, cudaEventDisableTiming) != cudaSuccess) {
     cbmv_ctx_destroy(c);
     return set_error(CBMV_ECUDA, "cudaStreamCreate / cudaEventCreate failed");
   }
@@ -211,6 +213,7 @@ extern "C" int cbmv_ctx_destroy(cbmv_ctx* c) {
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->fork_ev) cudaEventDestroy(c->fork_ev);
   if (c->join_ev) cudaEventDestroy(c->join_ev);
+  if (c->prep_ev) cudaEventDestroy(c->prep_ev);
   if (c->side) cudaStreamDestroy(c->side);
   delete c;
   return CBMV_OK;
@@ -226,6 +229,7 @@ extern "C" int cbmv_ctx_timings(cbmv_ctx* c, float* ms5) {
 static int ensure_workspace(cbmv_ctx* c, size_t bytes) {
   if (c->ws_bytes >= bytes) return CBMV_OK;
   CBMV_CUDA(cudaStreamSynchronize(c->stream));
+  CBMV_CUDA(cudaStreamSynchronize(c->side));
   if (c->ws) cudaFree(c->ws);
   c->ws = nullptr;
   c->ws_bytes = 0;
@@ -327,17 +331,30 @@ static int cost_chain(cbmv_ctx* c, const cbmv_params* p, Work& w, int64_t H, int
 // is the right disparity) and after the left view's subpixel step marks
 // occlusions and mismatches (left-right check) and fills them
 // (interpolate_mismatch, then interpolate_occlusion) before the median.
+// The post's image terms (do_post's normalisation, test.py:485-504; the
+// cross arms; the SGM's neighbour differences): they depend on the images
+// only, so the fused paths launch them on the side stream at the start of
+// the call, beside the matchers.
+static int post_prep(const cbmv_params* p, const uint8_t* L, const uint8_t* R, int64_t H, int64_t W, Work& w,
+                     cudaStream_t s) {
+  const int64_t HW = H * W;
+  RC(launch_normalise(L, HW, w.mom, w.imL, s));
+  RC(launch_normalise(R, HW, w.mom + 2, w.imR, s));
+  RC(launch_cross(w.imL, H, W, p->L1, p->tau1, w.crossL, s));
+  RC(launch_cross(w.imR, H, W, p->L1, p->tau1, w.crossR, s));
+  SgmGrad g{w.grad, w.grad + HW, w.grad + 2 * HW, w.grad + 3 * HW};
+  if (p->sgm_i > 0) RC(launch_sgm_grad(w.imL, w.imR, H, W, &g, s));
+  return CBMV_OK;
+}
+
 static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
                     int64_t H, int64_t W, int D, Work& w, float* disp) {
   cudaStream_t st = c->stream;
-  const int64_t HW = H * W;
   RC(ensure_gaussian(c, p->blur_sigma));
-  RC(launch_normalise(L, HW, w.mom, w.imL, st));
-  RC(launch_normalise(R, HW, w.mom + 2, w.imR, st));
-  RC(launch_cross(w.imL, H, W, p->L1, p->tau1, w.crossL, st));
-  RC(launch_cross(w.imR, H, W, p->L1, p->tau1, w.crossR, st));
-  SgmGrad g{w.grad, w.grad + HW, w.grad + 2 * HW, w.grad + 3 * HW};
-  if (p->sgm_i > 0) RC(launch_sgm_grad(w.imL, w.imR, H, W, &g, st));
+  if (w.prepped)
+    CBMV_CUDA(cudaStreamWaitEvent(st, c->prep_ev, 0));
+  else
+    RC(post_prep(p, L, R, H, W, w, st));
   float* res = nullptr;
   if (p->interpolate) {
     // right view (test.py:154, 176-255): its cost, its chain, its argmin
@@ -379,7 +396,7 @@ static int run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const u
 // and of the training samples); f32 = true: float32 volumes (in the first
 // half of each float64 buffer) and float32 statistics only, for the network.
 static int run_front(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R,
-                     int64_t H, int64_t W, int D, Work* wout, bool f32 = false) {
+                     int64_t H, int64_t W, int D, Work* wout, bool f32 = false, bool prep = false) {
   RC(check_params(p));
   CBMV_REQUIRE(H > p->censw && W > p->censw, CBMV_EINVAL, "image %lldx%lld smaller than the census window",
                (long long)W, (long long)H);
@@ -390,6 +407,14 @@ static int run_front(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const 
   Work w = carve(c->ws, H, W, D, &bytes, f32, p->interpolate != 0);
   cudaStream_t st = c->stream;
   CBMV_CUDA(cudaEventRecord(c->ev[0], st));
+  if (prep) {  // the post's image terms beside the matchers; run_post waits for prep_ev
+    RC(ensure_gaussian(c, p->blur_sigma));
+    CBMV_CUDA(cudaEventRecord(c->fork_ev, st));
+    CBMV_CUDA(cudaStreamWaitEvent(c->side, c->fork_ev, 0));
+    RC(post_prep(p, L, R, H, W, w, c->side));
+    CBMV_CUDA(cudaEventRecord(c->prep_ev, c->side));
+    w.prepped = true;
+  }
   RC(launch_census_desc(L, H, W, p->censw, w.descL, st));
   RC(launch_census_desc(R, H, W, p->censw, w.descR, st));
   RC(launch_ncc_stats(L, H, W, p->nccw, w.AL, w.CL, st));
@@ -441,7 +466,7 @@ extern "C" int cbmv_run_rf(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params*
   p = params_or_default(p, &def);
   CBMV_REQUIRE(forest_view(f)->n_features == 20, CBMV_EINVAL, "the forest must take the 20 CBMV features");
   Work w;
-  RC(run_front(c, p, L, R, H, W, D, &w));
+  RC(run_front(c, p, L, R, H, W, D, &w, false, true));
   cudaStream_t st = c->stream;
   const double* vols[4] = {w.vol[0], w.vol[1], w.vol[2], w.vol[3]};
   RC(launch_features_rf(vols, w.stats, H, W, D, f, w.volA, st));
@@ -459,7 +484,7 @@ extern "C" int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p
   cbmv_params def;
   p = params_or_default(p, &def);
   Work w;
-  RC(run_front(c, p, L, R, H, W, D, &w, true));
+  RC(run_front(c, p, L, R, H, W, D, &w, true, true));
   cudaStream_t st = c->stream;
   const float* vols[4] = {(float*)w.vol[0], (float*)w.vol[1], (float*)w.vol[2], (float*)w.vol[3]};
   RC(launch_features_mlp(vols, w.statsf, H, W, D, m, w.volA, st, p->mlp_ctas));

@@ -340,7 +340,12 @@ void cbmv_params_default(cbmv_params* p);
 typedef struct cbmv_ctx cbmv_ctx;
 
 /* A context owns the device workspaces of one pair shape and one stream;
- * it grows them on demand.  Not thread-safe: one context per host thread. */
+ * it grows them on demand.  Not thread-safe: one context per host thread.
+ * Inside cbmv_run_rf / cbmv_run_mlp / cbmv_run_post some independent work
+ * (the post's image terms beside the matchers, the CBCA supports beside the
+ * SGM) runs on a second stream the context creates; events order it with
+ * `stream` both ways, so every call's work is complete once `stream` has
+ * passed the call (also under stream capture). */
 int cbmv_ctx_create(void* stream, cbmv_ctx** out);
 int cbmv_ctx_destroy(cbmv_ctx* c);
 
