@@ -395,6 +395,44 @@ __global__ void __launch_bounds__(256) stats_f32_left_q_kernel(VolsF vols, int64
   }
 }
 
+// view 0 for D = 128 exactly (the headline's disparity count): eight lanes
+// per pixel, four pixels per warp at a time, each lane four float4 of its
+// pixel's row; the minimum and the denominator reduce over the eight lanes
+// in three shuffle steps.  (Its denominator adds in another order than
+// stats_f32_left_q_kernel: the same value to float32 rounding.)
+__global__ void __launch_bounds__(256) stats_f32_left_g8_kernel(VolsF vols, int64_t HW,
+                                                                float2* __restrict__ statsf) {
+  const int m = blockIdx.y;
+  const float inv_sigma = kInvSigmaF32[m];
+  const int lane = threadIdx.x & 31, gi = lane >> 3, li = lane & 7;
+  const float4* __restrict__ rows = reinterpret_cast<const float4*>(vols.v[m]);
+  float2* __restrict__ out = statsf + (int64_t)(m * 2) * HW;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t p0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4; p0 < HW; p0 += 4 * nw) {
+    const int64_t p = p0 + gi;
+    const bool on = p < HW;
+    float4 v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      v[k] = on ? __ldg(rows + p * 32 + li + 8 * k) : make_float4(kRandMaxF, kRandMaxF, kRandMaxF, kRandMaxF);
+    float mn = kRandMaxF;
+#pragma unroll
+    for (int k = 0; k < 4; k++) mn = fminf(mn, fminf(fminf(v[k].x, v[k].y), fminf(v[k].z, v[k].w)));
+#pragma unroll
+    for (int o = 4; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    float den = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const float tx = v[k].x - mn, ty = v[k].y - mn, tz = v[k].z - mn, tw = v[k].w - mn;
+      den += (__expf(-(tx * tx) * inv_sigma) + __expf(-(ty * ty) * inv_sigma)) +
+             (__expf(-(tz * tz) * inv_sigma) + __expf(-(tw * tw) * inv_sigma));
+    }
+#pragma unroll
+    for (int o = 4; o; o >>= 1) den += __shfl_xor_sync(0xffffffffu, den, o);
+    if (li == 0 && on) out[p] = stats_pair(mn, den);
+  }
+}
+
 // view 1 for D a multiple of 4: as stats_f32_right_kernel, the staging
 // loads one float4 (4 disparities) per thread and step with 32-bit row
 // offsets; the diagonal walk, and so the order of the sums, is unchanged.
@@ -452,7 +490,11 @@ int launch_feature_stats_f32(const float* const* vols, int64_t H, int64_t W, int
   const int64_t HW = H * W;
   const int64_t lblocks = (HW + 7) / 8;  // 8 warps per block, one pixel each
   const bool q = D % 4 == 0 && ((uintptr_t)vols[0] | (uintptr_t)vols[1] | (uintptr_t)vols[2] | (uintptr_t)vols[3]) % 16 == 0;
-  if (q && D <= 128) {
+  if (q && D == 128) {
+    const int64_t gblocks = (HW + 31) / 32;  // 8 warps per block, four pixels each
+    stats_f32_left_g8_kernel<<<dim3((unsigned)(gblocks < 65535 * 16 ? gblocks : 65535 * 16), 4), 256, 0, st>>>(
+        v, HW, statsf);
+  } else if (q && D <= 128) {
     const int64_t qblocks = (HW + 15) / 16;  // 8 warps per block, two pixels each
     stats_f32_left_q_kernel<<<dim3((unsigned)(qblocks < 65535 * 16 ? qblocks : 65535 * 16), 4), 256, 0, st>>>(
         v, HW, D, statsf);
