@@ -84,14 +84,15 @@ def test_sgm_close(gpu, oracle_cpu, scene):
     np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=2e-5, atol=2e-4)
 
 
-@pytest.mark.parametrize("D", [68, 128, 200])
+@pytest.mark.parametrize("D", [68, 128, 200, 256])
 @pytest.mark.parametrize("direction", [-1, 1])
 def test_sgm_consecutive_lanes_equal_strided(gpu, scene, D, direction):
     """The SGM scan with KPL consecutive disparities per lane (float4 path
-    costs, taken for D % 4 == 0 in (64, 512] on 16-byte aligned volumes)
-    and the strided scan (lane = d mod 32, taken otherwise) agree bit for
-    bit: same per-element arithmetic in the same order.  An input volume
-    4 bytes off a 16-byte boundary selects the strided scan."""
+    costs, taken for D % 4 == 0 in (64, 512] on 16-byte aligned volumes:
+    KPL 4 and 8 here) and the strided scan (lane = d mod 32, taken
+    otherwise) agree bit for bit: same per-element arithmetic in the same
+    order.  An input volume 4 bytes off a 16-byte boundary selects the
+    strided scan."""
     from cbmv_b200 import _lib
     imgl, imgr, _, _ = scene
     H, W = imgl.shape
