@@ -10,8 +10,10 @@ the 16-bit MLP 20-128-128-64-1 with GELU hidden layers (f16 inference)
 (tests/golden/mlp_gelu_694x554.npz, cbmv_b200/train_mlp.py).  The RF judges
 the MLP: both run on 20 held-out seeded pairs and the MLP is the headline
 only when its bad-2.0 is within 0.5 percentage points of the RF's.  Beside
-the headline: the same network with ReLU (a labelled variant), and the
-learned path with the `_interp` post (the reference's LR-check chain).
+the headline: the same network with ReLU (a labelled variant), the
+headline network with bf16 operands in its fused inference (a labelled
+variant), and the learned path with the `_interp` post (the reference's
+LR-check chain).
 With N GPUs (torchrun), every rank processes its own pair (seed = rank):
 weak scaling by independent pairs, no collective on the data path; with
 --batch, the 64 uneven pairs are split over the ranks (strong scaling) and
@@ -257,7 +259,7 @@ def run_cbmv(a, ws, rank, local):
     units = L.shape[0] * W0 * D0
     flat = FlatForest.load(a.forest) if have_forest else None
     gf = GpuForest(flat) if have_forest else None
-    net = GpuMlp.load(a.mlp) if os.path.exists(a.mlp) else None
+    net = GpuMlp.load(a.mlp, a.mlp_precision) if os.path.exists(a.mlp) else None
     pipe = StereoPipeline(gf)
     l = torch.from_numpy(L).to(dev)
     r = torch.from_numpy(R).to(dev)
@@ -276,7 +278,7 @@ def run_cbmv(a, ws, rank, local):
         paths["mlp"] = (lambda: pipe.run_mlp(net, l, r, D0, disp_out=disp),
                         lambda: pipe.run_mlp(net, Lh, Rh, D0))
     res = {}
-    relu = None
+    relu = bf16v = None
     with Clocks(local) as clk:
         for name, (run_dev, run_host) in paths.items():
             ms, stage = _time_path(run_dev, a, ws, flush, st, pipe)
@@ -290,6 +292,16 @@ def run_cbmv(a, ws, rank, local):
                     "stage_ms": stage_r, "bad2_nonocc": evaluate.bad_x(disp.cpu().numpy(), gt, nonocc),
                     "classify_tflops": FLOPS_PER_UNIT_MLP * units / (stage_r["classify"] / 1e3) / 1e12}
             net_r.close()
+        # the headline network with bf16 operands in the fused inference, a labelled variant
+        if net is not None and a.classifier in ("both", "mlp") and not a.device_only \
+                and a.mlp_precision == "f16":
+            net.set_precision("bf16")
+            ms_b, stage_b = _time_path(lambda: pipe.run_mlp(net, l, r, D0, disp_out=disp), a, ws, flush, st, pipe)
+            bf16v = {"precision": "bf16", "activation": net.activation, "ms_per_step": ms_b,
+                     "value": units * ws / (ms_b / 1e3), "stage_ms": stage_b,
+                     "bad2_nonocc": evaluate.bad_x(disp.cpu().numpy(), gt, nonocc),
+                     "classify_tflops": FLOPS_PER_UNIT_MLP * units / (stage_b["classify"] / 1e3) / 1e12}
+            net.set_precision("f16")
     for name, (_, run_host) in paths.items():
         res[name]["e2e_ms"] = _time_e2e(run_host, a, ws, flush, st) if not a.device_only else None
     # the _interp post (test.py:153-338: the right view's chain, the left-right
@@ -373,7 +385,7 @@ def run_cbmv(a, ws, rank, local):
         "metric": METRIC, "value": units * ws / (h["ms"] / 1e3), "unit": "pixel·disparities/s",
         "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": h["ms"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f16/f32" if head == "mlp" else "f64/f32",
+        "dtype": ("%s/f32" % a.mlp_precision) if head == "mlp" else "f64/f32",
         "data": "synthetic (seeded 694x554 pair per rank; L2 flushed between steps)",
         "config": {"workload": "694x554 D=128 test path: 4 matchers, 20 features, %s, MC-CNN _mem post"
                                % classifier, "width": W0, "height": int(L.shape[0]), "ndisp": D0,
@@ -402,6 +414,7 @@ def run_cbmv(a, ws, rank, local):
         "matched_bad2": matched,
         "interp_variant": interp,
         "relu_variant": relu,
+        "bf16_variant": bf16v,
         "clocks": clk.summary(),
     }
     if rank == 0 and ws == 1 and not a.no_cpu_baseline and not a.device_only and have_forest:
@@ -549,7 +562,7 @@ def run_batch(a, ws, rank, local):
     units = int(sum(h * w * d for h, w, d in all_shapes))
     lefts = [torch.from_numpy(p[0]).to(dev) for p in pairs]
     rights = [torch.from_numpy(p[1]).to(dev) for p in pairs]
-    net = GpuMlp.load(a.mlp)
+    net = GpuMlp.load(a.mlp, a.mlp_precision)
     t_tune = time.perf_counter()
     tune = tune_batch(shapes, net, lefts, rights, log=lambda m: print(m, file=sys.stderr))
     t_tune = time.perf_counter() - t_tune
@@ -606,7 +619,7 @@ def run_batch(a, ws, rank, local):
         "value": units / (ms / 1e3), "unit": "pixel·disparities/s", "n_gpus": ws, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "strong" if ws > 1 else "weak", "vs_baseline": None,
-        "dtype": "f16/f32", "data": "synthetic (seeded uneven pairs, seeds 4000+)",
+        "dtype": "%s/f32" % a.mlp_precision, "data": "synthetic (seeded uneven pairs, seeds 4000+)",
         "config": {"workload": "%d pairs W~U[320,1500] H~U[240,1000] D in {64,128,192,256}" % n,
                    "units": units,
                    "autotune": {k: tune.get(k) for k in ("streams", "mlp_ctas", "cbca_rows", "sgm_prefetch", "ms",
@@ -654,6 +667,9 @@ def main():
     ap.add_argument("--forest", default=FOREST)
     ap.add_argument("--mlp", default=MLP, help="trained MLP parameters (cbmv_b200.train_mlp)")
     ap.add_argument("--mlp-relu", default=MLP_RELU, help="the ReLU network, timed as a variant")
+    ap.add_argument("--mlp-precision", choices=["f16", "bf16"], default="f16",
+                    help="operand type of the network's fused inference (bf16 is also timed as a "
+                         "variant of the f16 default)")
     ap.add_argument("--classifier", choices=["both", "rf", "mlp"], default="both",
                     help="classifier paths to time (both: the MLP is the headline when it matches "
                          "the RF's held-out bad-2.0)")

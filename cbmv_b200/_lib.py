@@ -77,6 +77,8 @@ SIGNATURES = {
     "cbmv_mlp_status": [_vp, ctypes.POINTER(_int)],
     "cbmv_mlp_set_activation": [_vp, _int],
     "cbmv_mlp_get_activation": [_vp, _vp],
+    "cbmv_mlp_set_precision": [_vp, _int],
+    "cbmv_mlp_get_precision": [_vp, _vp],
     "cbmv_cross": [_vp, _i64, _i64, _int, _flt, _vp, _vp],
     "cbmv_sgm": [_vp, _vp, _vp, _i64, _i64, _int, _flt, _flt, _flt, _flt, _flt, _flt, _int, _vp, _vp],
     "cbmv_cbca": [_vp, _vp, _vp, _i64, _i64, _int, _int, _int, _vp, _vp],

@@ -500,6 +500,19 @@ extern "C" int cbmv_mlp_set_activation(cbmv_mlp* n, int act) {
   return CBMV_OK;
 }
 
+extern "C" int cbmv_mlp_set_precision(cbmv_mlp* n, int prec) {
+  CBMV_REQUIRE(n, CBMV_EINVAL, "null pointer argument");
+  CBMV_REQUIRE(prec == CBMV_PREC_F16 || prec == CBMV_PREC_BF16, CBMV_EINVAL, "unknown precision %d", prec);
+  n->prec = prec;
+  return CBMV_OK;
+}
+
+extern "C" int cbmv_mlp_get_precision(const cbmv_mlp* n, int* prec) {
+  CBMV_REQUIRE(n && prec, CBMV_EINVAL, "null pointer argument");
+  *prec = n->prec;
+  return CBMV_OK;
+}
+
 extern "C" int cbmv_mlp_get_activation(const cbmv_mlp* n, int* act) {
   CBMV_REQUIRE(n && act, CBMV_EINVAL, "null pointer argument");
   *act = n->act;

@@ -3,6 +3,7 @@
 // (mlp_infer_relu.cu, mlp_infer_gelu.cu), so that neither instantiation
 // changes how the compiler allocates the other's registers.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include "features.cuh"
@@ -25,22 +26,24 @@
 // others wait on the group's named barrier (no issue slots spent
 // spinning), which also hands them the poll's result.
 //
-// Arithmetic, per layer (the float32 accumulator in tensor memory); every
-// bias enters as f16 high + low parts multiplied by constant ones:
+// Arithmetic, per layer (the float32 accumulator in tensor memory), with
+// 16-bit operands of the network's precision (f16 by default, bf16 on
+// request; "16-bit" below); every bias enters as 16-bit high + low parts
+// multiplied by constant ones:
 //   layer 1  K = 32: 20 normalised features, two constant-one columns whose
 //            weights are b1's parts, zeros;
 //   layers 2, 3: a first K = 16 MMA of a constant tile (ones in columns 0
 //            and 1) against b2's / b3's parts (stored in the unused K
 //            columns 32..63 of layer 1's weight tile) initialises the
 //            accumulator, the layer's MMAs accumulate onto it;
-//   hidden activations: ReLU and the f16 rounding in one instruction
-//            (cvt.rn.relu.f16x2.f32) per pair of columns, or the GELU in
-//            packed f16 arithmetic (six instructions per pair);
+//   hidden activations: ReLU and the 16-bit rounding in one instruction
+//            per pair of columns, or the GELU in packed 16-bit arithmetic
+//            (six instructions per pair in f16, seven in bf16);
 //   output   layer 4 is an MMA too: N = 16, rows 0 and 1 of its weight tile
-//            are the high and low f16 parts of w4, z = D[0] + D[1] + b4,
+//            are the high and low 16-bit parts of w4, z = D[0] + D[1] + b4,
 //            cost = 1 - sigmoid(z) = 1 / (1 + exp(z)).
-// The features themselves are formed in float32 (they enter the network as
-// f16), from float32 cost volumes and float32 row statistics (min, 1/den),
+// The features themselves are formed in float32 (they enter the network in
+// 16 bits), from float32 cost volumes and float32 row statistics (min, 1/den),
 // with one reciprocal 1/(c + e) shared by the left and right ratio.
 // ====================================================================
 
@@ -62,7 +65,6 @@ constexpr size_t kSmOne = 128 * 128;      // [128 x 64], ones in columns 0 and 1
 constexpr size_t kSmTile = 2 * 128 * 128; // a group's activation tile [128 x 128]
 constexpr size_t kSmInf = 1024 + kSmW1i + kSmW2i + kSmW3i + kSmW4i + kSmOne + kGroups * kSmTile;
 constexpr int kColB2 = 32, kColB3 = 48;  // K columns of layer 1's weight tile holding b2, b3
-constexpr uint32_t kF16OneOne = 0x3C003C00u;  // two f16 ones
 
 static __constant__ float kEpsF[4] = {0.01f, 1.01f, 0.01f, 0.01f};
 static __constant__ float kInvSigmaF[4] = {(float)(1.0 / (2.0 * 8 * 8)), (float)(1.0 / 0.02),
@@ -85,39 +87,88 @@ __device__ __forceinline__ bool group_all(int g, bool v) {
   return r != 0;
 }
 
-// Two float32 values as a packed f16 pair (low = a), round to nearest even,
-// saturated to the largest finite f16 (+-65504)
-__device__ __forceinline__ uint32_t pack_f16x2(float a, float b) {
-  uint32_t r;
-  asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
-  return r;
-}
+// The network's 16-bit operand type in the fused kernel (cbmv_mlp_set_precision):
+// F16 = true, IEEE half (the default), F16 = false, bfloat16.  Per type: the
+// packed conversion of two float32 values (low = a), round to nearest even
+// (f16: saturated to +-65504); ReLU of two pre-activations in the same
+// instruction; the GELU of two pre-activations; the bits of one value and
+// its high + low split; the instruction descriptor of the MMAs.
+template <bool F16>
+struct Op16;
 
-// ReLU of two float32 pre-activations, as a packed f16 pair (low = a),
-// round to nearest even, saturated to 65504
-__device__ __forceinline__ uint32_t relu_f16x2(float a, float b) {
-  uint32_t r;
-  asm("cvt.rn.relu.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
-  return r;
-}
+template <>
+struct Op16<true> {
+  static constexpr uint32_t kOneOne = 0x3C003C00u;  // two f16 ones
+  static __device__ __forceinline__ uint32_t pack(float a, float b) {
+    uint32_t r;
+    asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+    return r;
+  }
+  static __device__ __forceinline__ uint32_t relu(float a, float b) {
+    uint32_t r;
+    asm("cvt.rn.relu.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+    return r;
+  }
+  // gelu_t's f16 operations, both lanes per instruction: six instructions
+  // per pair, the conversion included, the clamp of q to [0, 1] folded into
+  // its FMA (`fma.rn.sat.f16x2`)
+  static __device__ __forceinline__ uint32_t gelu(float a, float b) {
+    const __half2 g0 = __half2half2(f16_bits(kG0Bits)), g1 = __half2half2(f16_bits(kG1Bits)),
+                  g2 = __half2half2(f16_bits(kG2Bits));
+    const __half2 half = __float2half2_rn(0.5f);
+    const uint32_t xb = pack(a, b);
+    const __half2 x = *reinterpret_cast<const __half2*>(&xb);
+    const __half2 u = __hmul2(x, x);
+    __half2 p = __hfma2(g2, u, g1);
+    p = __hfma2(p, u, g0);
+    const __half2 q = __hfma2_sat(x, p, half);
+    const __half2 g = __hmul2(x, q);
+    return *reinterpret_cast<const uint32_t*>(&g);
+  }
+  static __device__ __forceinline__ uint16_t bits(float x) { return to_f16(x); }
+  static __device__ __forceinline__ void split(float x, float* hi, float* lo) {
+    *hi = __half2float(__float2half_rn(fminf(fmaxf(x, -65504.0f), 65504.0f)));
+    *lo = x - *hi;
+  }
+  static __host__ __device__ constexpr uint32_t idesc(int M, int N) { return umma::idesc_f16(M, N); }
+};
 
-// GELU (gelu_t) of two float32 pre-activations as a packed f16 pair (low =
-// a): the same f16 operations as gelu_t, both lanes per instruction -- six
-// instructions per pair, the conversion included, the clamp of q to [0, 1]
-// folded into its FMA (`fma.rn.sat.f16x2`).
-__device__ __forceinline__ uint32_t gelu_f16x2(float a, float b) {
-  const __half2 g0 = __half2half2(f16_bits(kG0Bits)), g1 = __half2half2(f16_bits(kG1Bits)),
-                g2 = __half2half2(f16_bits(kG2Bits));
-  const __half2 half = __float2half2_rn(0.5f);
-  const uint32_t xb = pack_f16x2(a, b);
-  const __half2 x = *reinterpret_cast<const __half2*>(&xb);
-  const __half2 u = __hmul2(x, x);
-  __half2 p = __hfma2(g2, u, g1);
-  p = __hfma2(p, u, g0);
-  const __half2 q = __hfma2_sat(x, p, half);
-  const __half2 g = __hmul2(x, q);
-  return *reinterpret_cast<const uint32_t*>(&g);
-}
+template <>
+struct Op16<false> {
+  static constexpr uint32_t kOneOne = 0x3F803F80u;  // two bf16 ones
+  static __device__ __forceinline__ uint32_t pack(float a, float b) {
+    const __nv_bfloat162 x = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&x);
+  }
+  static __device__ __forceinline__ uint32_t relu(float a, float b) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+    return r;
+  }
+  // the same polynomial form in bf16 operations with its own coefficients
+  // (gelu_bf16_t): seven instructions per pair -- bf16 has no saturating
+  // FMA, so the clamp is a `.relu` FMA and a min
+  static __device__ __forceinline__ uint32_t gelu(float a, float b) {
+    const __nv_bfloat162 g0 = __bfloat162bfloat162(bf16_bits(kGB0Bits)),
+                         g1 = __bfloat162bfloat162(bf16_bits(kGB1Bits)),
+                         g2 = __bfloat162bfloat162(bf16_bits(kGB2Bits));
+    const __nv_bfloat162 half = __float2bfloat162_rn(0.5f), one = __float2bfloat162_rn(1.0f);
+    const __nv_bfloat162 x = __floats2bfloat162_rn(a, b);
+    const __nv_bfloat162 u = __hmul2(x, x);
+    __nv_bfloat162 p = __hfma2(g2, u, g1);
+    p = __hfma2(p, u, g0);
+    __nv_bfloat162 q = __hfma2_relu(x, p, half);
+    q = __hmin2(q, one);
+    const __nv_bfloat162 g = __hmul2(x, q);
+    return *reinterpret_cast<const uint32_t*>(&g);
+  }
+  static __device__ __forceinline__ uint16_t bits(float x) { return to_bf16(x); }
+  static __device__ __forceinline__ void split(float x, float* hi, float* lo) {
+    *hi = __bfloat162float(__float2bfloat16_rn(x));
+    *lo = x - *hi;
+  }
+  static __host__ __device__ constexpr uint32_t idesc(int M, int N) { return umma::idesc_bf16(M, N); }
+};
 
 // ratio and likelihood of cost c (featextract.cpp:333 and :440) in float32
 // against its row statistics st = (min, 1/den); inv_ce = 1 / (c + e).
@@ -132,14 +183,9 @@ __device__ __forceinline__ void conf_f32(float c, float inv_ce, float2 st, float
   *lik = __expf(-(t * t) * inv_sigma) * st.y;  // 1/den = 0 on sentinel rows
 }
 
-// f16 high part of x and the f16 rounding of the rest: x ~ hi + lo
-__device__ __forceinline__ void split_f16(float x, float* hi, float* lo) {
-  *hi = __half2float(__float2half_rn(x));
-  *lo = x - *hi;
-}
-
 // Stage the inference weights from the float32 parameter vector, and the
 // constant tile of the bias MMAs.
+template <bool F16>
 __device__ __forceinline__ void stage_inference_weights(const float* __restrict__ P, unsigned char* sW1, unsigned char* sW2,
                                         unsigned char* sW3, unsigned char* sW4, unsigned char* sOne) {
   for (int q = threadIdx.x; q < 128 * 64; q += blockDim.x) {
@@ -148,31 +194,31 @@ __device__ __forceinline__ void stage_inference_weights(const float* __restrict_
     if (k < kF) {
       v = P[kOffW1 + r * kF + k];
     } else if (k == kF || k == kF + 1) {
-      split_f16(P[kOffB1 + r], &hi, &lo);
+      Op16<F16>::split(P[kOffB1 + r], &hi, &lo);
       v = k == kF ? hi : lo;
     } else if (k == kColB2 || k == kColB2 + 1) {
-      split_f16(P[kOffB2 + r], &hi, &lo);
+      Op16<F16>::split(P[kOffB2 + r], &hi, &lo);
       v = k == kColB2 ? hi : lo;
     } else if (r < kH3 && (k == kColB3 || k == kColB3 + 1)) {
-      split_f16(P[kOffB3 + r], &hi, &lo);
+      Op16<F16>::split(P[kOffB3 + r], &hi, &lo);
       v = k == kColB3 ? hi : lo;
     }
-    *reinterpret_cast<uint16_t*>(sW1 + umma::sw128_offset(128, r, k)) = to_f16(v);
-    *reinterpret_cast<uint16_t*>(sOne + umma::sw128_offset(128, r, k)) = to_f16(k < 2 ? 1.0f : 0.0f);
+    *reinterpret_cast<uint16_t*>(sW1 + umma::sw128_offset(128, r, k)) = Op16<F16>::bits(v);
+    *reinterpret_cast<uint16_t*>(sOne + umma::sw128_offset(128, r, k)) = Op16<F16>::bits(k < 2 ? 1.0f : 0.0f);
   }
   for (int q = threadIdx.x; q < 128 * 128; q += blockDim.x) {
     const int r = q >> 7, k = q & 127;
-    *reinterpret_cast<uint16_t*>(sW2 + umma::sw128_offset(128, r, k)) = to_f16(P[kOffW2 + q]);
+    *reinterpret_cast<uint16_t*>(sW2 + umma::sw128_offset(128, r, k)) = Op16<F16>::bits(P[kOffW2 + q]);
   }
   for (int q = threadIdx.x; q < 64 * 128; q += blockDim.x) {
     const int r = q >> 7, k = q & 127;
-    *reinterpret_cast<uint16_t*>(sW3 + umma::sw128_offset(64, r, k)) = to_f16(P[kOffW3 + q]);
+    *reinterpret_cast<uint16_t*>(sW3 + umma::sw128_offset(64, r, k)) = Op16<F16>::bits(P[kOffW3 + q]);
   }
   for (int q = threadIdx.x; q < 16 * 64; q += blockDim.x) {
     const int r = q >> 6, k = q & 63;
     float hi, lo;
-    split_f16(P[kOffW4 + k], &hi, &lo);
-    *reinterpret_cast<uint16_t*>(sW4 + umma::sw128_offset(16, r, k)) = to_f16(r == 0 ? hi : r == 1 ? lo : 0.0f);
+    Op16<F16>::split(P[kOffW4 + k], &hi, &lo);
+    *reinterpret_cast<uint16_t*>(sW4 + umma::sw128_offset(16, r, k)) = Op16<F16>::bits(r == 0 ? hi : r == 1 ? lo : 0.0f);
   }
 }
 
@@ -185,15 +231,15 @@ __device__ __forceinline__ uint4* tile_chunk(unsigned char* rowp, int r7s, int a
 
 // The activation of 16 loaded accumulator columns c .. c+15 -> the
 // activation tile (two 16-byte stores)
-template <int ACT>
+template <int ACT, bool F16>
 __device__ __forceinline__ void act_store16(unsigned char* rowp, int r7s, int c, const uint32_t* v) {
   uint32_t h[8];
 #pragma unroll
   for (int i = 0; i < 8; i++) {
     if constexpr (ACT == CBMV_ACT_GELU)
-      h[i] = gelu_f16x2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
+      h[i] = Op16<F16>::gelu(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
     else
-      h[i] = relu_f16x2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
+      h[i] = Op16<F16>::relu(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1]));
   }
 #pragma unroll
   for (int q = 0; q < 2; q++)
@@ -204,7 +250,7 @@ __device__ __forceinline__ void act_store16(unsigned char* rowp, int r7s, int c,
 // activation-tile columns alike; C0 a multiple of 64), 16 columns per
 // tensor-memory load, the next load in flight while the current columns
 // are computed.
-template <int C0, int NC, int ACT>
+template <int C0, int NC, int ACT, bool F16>
 __device__ __forceinline__ void epilogue_hidden(uint32_t tlane, unsigned char* rowp, int r7s) {
   uint32_t ga[16], gb[16];
   umma::tmem_ld16_issue(tlane + C0, ga);
@@ -212,10 +258,10 @@ __device__ __forceinline__ void epilogue_hidden(uint32_t tlane, unsigned char* r
 #pragma unroll
   for (int c = C0; c < C0 + NC; c += 32) {
     umma::tmem_ld16_issue(tlane + c + 16, gb);
-    act_store16<ACT>(rowp, r7s, c, ga);
+    act_store16<ACT, F16>(rowp, r7s, c, ga);
     umma::tmem_ld16_wait(gb);
     if (c + 32 < C0 + NC) umma::tmem_ld16_issue(tlane + c + 32, ga);
-    act_store16<ACT>(rowp, r7s, c + 16, gb);
+    act_store16<ACT, F16>(rowp, r7s, c + 16, gb);
     if (c + 32 < C0 + NC) umma::tmem_ld16_wait(ga);
   }
 }
@@ -272,7 +318,7 @@ __global__ void features_f32_gather_kernel(FeatVolsF fv, const float2* __restric
   }
 }
 
-template <int ACT>
+template <int ACT, bool F16>
 __global__ void __launch_bounds__(kInfThreads, 1)
     features_mlp_kernel(FeatVolsF fv, const float2* __restrict__ statsf, int64_t H, int64_t W, int D,
                         const float* __restrict__ P, float* __restrict__ prob0, int* __restrict__ status) {
@@ -292,7 +338,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
 
   if (tid < 32) umma::tmem_alloc(&tmem_base, 128 * kGroups);
   if (tid < kGroups) umma::mbar_init(&bars[tid], 1);
-  stage_inference_weights(P, sW1, sW2, sW3, sW4, sOne);
+  stage_inference_weights<F16>(P, sW1, sW2, sW3, sW4, sOne);
   for (int i = tid; i < kF; i += kInfThreads) s_nrm[i] = make_float4(P[i], P[kF + i], P[2 * kF + i], 0.0f);
   if (tid == 0) s_b4 = P[kOffB4];
   umma::fence_async_smem();
@@ -307,8 +353,8 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   const uint32_t tacc = tmem_base + (uint32_t)(g * 128);
   const uint32_t tlane = tacc + ((uint32_t)(wq * 32) << 16);
   const bool leader = row == 0;
-  constexpr uint32_t id128 = umma::idesc_f16(128, 128), id64 = umma::idesc_f16(128, 64),
-                     id16 = umma::idesc_f16(128, 16);
+  constexpr uint32_t id128 = Op16<F16>::idesc(128, 128), id64 = Op16<F16>::idesc(128, 64),
+                     id16 = Op16<F16>::idesc(128, 16);
   // operand descriptors, formed where the leader issues (keeps them out of the other threads' registers)
 #define DESC(ptr) umma::sw128_desc(umma::smem_u32(ptr))
 
@@ -355,11 +401,11 @@ __global__ void __launch_bounds__(kInfThreads, 1)
 #pragma unroll
       for (int k = 0; k < 20; k += 2) {
         const float4 na = s_nrm[k], nb = s_nrm[k + 1];
-        u[k >> 1] = pack_f16x2((fminf(f[k], na.x) - na.y) * na.z, (fminf(f[k + 1], nb.x) - nb.y) * nb.z);
+        u[k >> 1] = Op16<F16>::pack((fminf(f[k], na.x) - na.y) * na.z, (fminf(f[k + 1], nb.x) - nb.y) * nb.z);
       }
       *tile_chunk(rowp, r7s, 1, 0) = make_uint4(u[0], u[1], u[2], u[3]);
       *tile_chunk(rowp, r7s, 1, 1) = make_uint4(u[4], u[5], u[6], u[7]);
-      *tile_chunk(rowp, r7s, 1, 2) = make_uint4(u[8], u[9], kF16OneOne, 0u);
+      *tile_chunk(rowp, r7s, 1, 2) = make_uint4(u[8], u[9], Op16<F16>::kOneOne, 0u);
       *tile_chunk(rowp, r7s, 1, 3) = make_uint4(0u, 0u, 0u, 0u);
     }
     // advance to this thread's next sample (tile + tstride) and load its
@@ -385,7 +431,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       umma::mma_commit(bar0);
     }
     if (!(ok = wait(bar0, ph0))) break;
-    epilogue_hidden<0, 128, ACT>(tlane, rowp, r7s);
+    epilogue_hidden<0, 128, ACT, F16>(tlane, rowp, r7s);
     handoff();
     // 3. layer 2 (K = 128) onto the bias b2
     if (leader) {
@@ -398,7 +444,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       umma::mma_commit(bar0);
     }
     if (!(ok = wait(bar0, ph0))) break;
-    epilogue_hidden<0, 128, ACT>(tlane, rowp, r7s);
+    epilogue_hidden<0, 128, ACT, F16>(tlane, rowp, r7s);
     handoff();
     // 4. layer 3 (N = 64) onto the bias b3
     if (leader) {
@@ -411,7 +457,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       umma::mma_commit(bar0);
     }
     if (!(ok = wait(bar0, ph0))) break;
-    epilogue_hidden<0, 64, ACT>(tlane, rowp, r7s);
+    epilogue_hidden<0, 64, ACT, F16>(tlane, rowp, r7s);
     handoff();
     // 5. output layer (N = 16, rows 0/1 = high/low parts of w4) -> columns 64..79
     if (leader) {
@@ -455,18 +501,18 @@ inline int features_mlp_grid(int64_t H, int64_t W, int D, int max_ctas, int sms)
   return (int)(need < cap ? need : cap);
 }
 
-template <int ACT>
+template <int ACT, bool F16>
 int launch_features_mlp_act(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
                             const cbmv_mlp* m, float* prob0, cudaStream_t st, int max_ctas) {
   int dev = 0, sms = 0;
   CBMV_CUDA(cudaGetDevice(&dev));
   CBMV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  CBMV_CUDA(cudaFuncSetAttribute(features_mlp_kernel<ACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  CBMV_CUDA(cudaFuncSetAttribute(features_mlp_kernel<ACT, F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSmInf));
   CBMV_REQUIRE(((uintptr_t)statsf & 7) == 0, CBMV_EINVAL, "feature statistics must be 8-byte aligned");
   const int grid = features_mlp_grid(H, W, D, max_ctas, sms);
   FeatVolsF fv = {{vols[0], vols[1], vols[2], vols[3]}};
-  features_mlp_kernel<ACT><<<grid, kInfThreads, kSmInf, st>>>(fv, statsf, H, W, D, m->P, prob0, m->status);
+  features_mlp_kernel<ACT, F16><<<grid, kInfThreads, kSmInf, st>>>(fv, statsf, H, W, D, m->P, prob0, m->status);
   return check_launch("features_mlp");
 }
 

@@ -1,12 +1,18 @@
-// The fused features + network kernel with ReLU hidden layers, the
-// learned path's feature read-back (cbmv_ctx_features_f32_at) and the
-// dispatch on the network's activation.
+// The fused features + network kernel with ReLU hidden layers and f16
+// operands, the learned path's feature read-back (cbmv_ctx_features_f32_at)
+// and the dispatch on the network's activation and precision (one
+// instantiation per translation unit, so that none changes how the
+// compiler allocates another's registers).
 #include "mlp_infer.cuh"
 
 namespace cbmv {
 
 int launch_features_mlp_gelu(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
                              const cbmv_mlp* m, float* prob0, cudaStream_t st, int max_ctas);
+int launch_features_mlp_gelu_bf16(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
+                                  const cbmv_mlp* m, float* prob0, cudaStream_t st, int max_ctas);
+int launch_features_mlp_relu_bf16(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
+                                  const cbmv_mlp* m, float* prob0, cudaStream_t st, int max_ctas);
 
 int launch_features_f32_gather(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
                                const int64_t* idx, int64_t n, float* out, cudaStream_t st) {
@@ -19,8 +25,13 @@ int launch_features_f32_gather(const float* const* vols, const float2* statsf, i
 
 int launch_features_mlp(const float* const* vols, const float2* statsf, int64_t H, int64_t W, int D,
                         const cbmv_mlp* m, float* prob0, cudaStream_t st, int max_ctas) {
+  if (m->prec == CBMV_PREC_BF16) {
+    if (m->act == CBMV_ACT_GELU)
+      return launch_features_mlp_gelu_bf16(vols, statsf, H, W, D, m, prob0, st, max_ctas);
+    return launch_features_mlp_relu_bf16(vols, statsf, H, W, D, m, prob0, st, max_ctas);
+  }
   if (m->act == CBMV_ACT_GELU) return launch_features_mlp_gelu(vols, statsf, H, W, D, m, prob0, st, max_ctas);
-  return launch_features_mlp_act<CBMV_ACT_RELU>(vols, statsf, H, W, D, m, prob0, st, max_ctas);
+  return launch_features_mlp_act<CBMV_ACT_RELU, true>(vols, statsf, H, W, D, m, prob0, st, max_ctas);
 }
 
 }  // namespace cbmv

@@ -47,6 +47,14 @@ constexpr uint16_t kG0Bits = 0x35fe, kG1Bits = 0xa977, kG2Bits = 0x18a7;  // 0.3
 
 __device__ __forceinline__ __half f16_bits(uint16_t b) { return __ushort_as_half(b); }
 
+// The same form evaluated in bfloat16 operations, for the fused inference
+// with bf16 operands (cbmv_mlp_set_precision): x <- bf16(x); u = x * x;
+// p = G2 u + G1; p = p u + G0; q = min(max(x p + 0.5, 0), 1); x * q, every
+// operation one bf16 rounding, with coefficients searched for this bf16
+// evaluation: within 1.21e-2 of x * Phi(x) on every bf16 x.
+constexpr uint16_t kGB0Bits = 0x3ebf, kGB1Bits = 0xbd30, kGB2Bits = 0x3b1c;  // 0.373046875, -0.04296875, 0.00238037109375
+__device__ __forceinline__ __nv_bfloat16 bf16_bits(uint16_t b) { return __ushort_as_bfloat16(b); }
+
 // GELU of x (float32 in, its f16 rounding used) and, for the backward pass,
 // the derivative of the smooth function it approximates at that point:
 // q + x (p + 2 u p'(u)) where 0 < x p + 0.5 < 1, else q (0 or 1), in float32.
@@ -95,5 +103,6 @@ struct cbmv_mlp {
   float *dW1, *dW2, *dW3T, *db1, *db2, *db3, *dw4, *db4, *loss;
   int* status;
   int step = 0;
-  int act = CBMV_ACT_RELU;  // hidden-layer activation
+  int act = CBMV_ACT_RELU;    // hidden-layer activation
+  int prec = CBMV_PREC_F16;   // 16-bit operand type of the fused inference
 };

@@ -1,5 +1,5 @@
-"""The learned classifier: a 16-bit MLP (bf16 training, f16 fused inference)
-standing in for the reference's random
+"""The learned classifier: a 16-bit MLP (bf16 training; f16 or bf16 fused
+inference) standing in for the reference's random
 forest (test.py:603-620) as the per-(pixel, d) matching-probability model.
 
     net = MlpParams.init(seed, stats)        # fresh weights + input transform
@@ -22,6 +22,7 @@ from . import _dev, _lib
 F = 20
 LAYERS = [(128, F), (128, 128), (64, 128)]
 ACTIVATIONS = {"relu": 0, "gelu": 1}  # CBMV_ACT_RELU, CBMV_ACT_GELU
+PRECISIONS = {"f16": 0, "bf16": 1}  # CBMV_PREC_F16, CBMV_PREC_BF16
 
 
 def num_params():
@@ -139,9 +140,12 @@ class MlpTrainer:
 
 
 class GpuMlp:
-    """A trained network uploaded for inference (cbmv_run_mlp)."""
+    """A trained network uploaded for inference (cbmv_run_mlp).
 
-    def __init__(self, params):
+    precision: operand type of the fused inference, "f16" (the default:
+    the faster and the more precise of the two) or "bf16"."""
+
+    def __init__(self, params, precision="f16"):
         _dev.require_cuda()
         h = ctypes.c_void_p()
         _lib.call("cbmv_mlp_create", 128, ctypes.byref(h))
@@ -149,10 +153,17 @@ class GpuMlp:
         _lib.call("cbmv_mlp_set_params", self.h, params.vec.ctypes.data)
         _lib.call("cbmv_mlp_set_activation", self.h, ACTIVATIONS[params.activation])
         self.activation = params.activation
+        self.set_precision(precision)
 
     @classmethod
-    def load(cls, path):
-        return cls(MlpParams.load(path))
+    def load(cls, path, precision="f16"):
+        return cls(MlpParams.load(path), precision)
+
+    def set_precision(self, precision):
+        if precision not in PRECISIONS:
+            raise ValueError("precision must be one of %s" % sorted(PRECISIONS))
+        _lib.call("cbmv_mlp_set_precision", self.h, PRECISIONS[precision])
+        self.precision = precision
 
     def status(self):
         s = ctypes.c_int()

@@ -27,11 +27,14 @@ def relu(x):
 
 def bf16_rn(x):
     """Round float64 values to bfloat16 directly (round to nearest even), as
-    one bf16 operation rounds its exact result."""
+    one bf16 operation rounds its exact result; below 2^-126 onto the
+    subnormal grid of 2^-133."""
     a = np.ascontiguousarray(np.asarray(x, np.float64))
     u = a.view(np.uint64)
-    r = ((u + np.uint64(0xFFFFFFFFFFF) + ((u >> np.uint64(45)) & np.uint64(1))) >> np.uint64(45)) << np.uint64(45)
-    return r.view(np.float64)
+    r = (((u + np.uint64(0xFFFFFFFFFFF) + ((u >> np.uint64(45)) & np.uint64(1))) >> np.uint64(45))
+         << np.uint64(45)).view(np.float64)
+    tiny = np.abs(a) < 2.0 ** -126
+    return np.where(tiny, np.round(a * 2.0 ** 133) * 2.0 ** -133, r)
 
 
 def f16(x):
@@ -85,6 +88,24 @@ def gelu(x):
     dq = p + 2 * u * (2 * G[2] * u + G[1])
     d = np.where(qr <= 0, 0.0, np.where(qr >= 1, 1.0, qr + xb * dq))
     return g, d
+
+
+# the bf16 form's GELU coefficients (cbmv_b200/csrc/mlp_net.cuh, kGB*Bits), bf16 values
+GB = np.array([0.373046875, -0.04296875, 0.00238037109375])
+
+
+def gelu_bf16(x):
+    """The GELU of the fused kernel's bf16 form: x rounded from float32 to
+    bf16, then u = x*x, p = GB2 u + GB1, p = p u + GB0, q = max(x p + 0.5,
+    0) (a `.relu` FMA), q = min(q, 1), x*q, each operation rounded once to
+    bf16 (mlp_infer.cuh, Op16<false>::gelu)."""
+    xb = bf16(x)
+    u = bf16_rn(xb * xb)
+    p = bf16_rn(GB[2] * u + GB[1])
+    p = bf16_rn(p * u + GB[0])
+    q = np.maximum(bf16_rn(xb * p + 0.5), 0.0)
+    q = np.minimum(q, 1.0)
+    return bf16_rn(xb * q)
 
 
 ACT = {"relu": relu, "gelu": gelu}
@@ -153,26 +174,41 @@ def split_f16(x):
     return hi, f16_sat(x - np.float32(hi))
 
 
-def forward_fused(vec, X, act="relu"):
+def split_bf16(x):
+    """bf16 high part of float32 x and the bf16 rounding of the rest (the
+    rest formed in float32)."""
+    x = np.asarray(x, np.float32)
+    hi = bf16(x)
+    return hi, bf16(x - np.float32(hi))
+
+
+def forward_fused(vec, X, act="relu", prec="f16"):
     """The network as the fused inference kernel evaluates it (test
-    infrastructure): f16 operands throughout -- the normalised inputs, the
+    infrastructure), in its f16 form (prec="f16") or its bf16 form
+    (prec="bf16"): 16-bit operands throughout -- the normalised inputs, the
     weights, the hidden activations (ReLU of the float32 accumulator rounded
-    to f16, or the f16 GELU of it) -- every bias (and w4) as its f16 high +
-    low parts; the output layer runs on those f16 activations.  Returns z."""
+    to the 16-bit type, or that form's GELU of it) -- every bias (and w4) as
+    its 16-bit high + low parts; the output layer runs on those 16-bit
+    activations.  Returns z."""
+    if prec == "f16":
+        r16, split, g16 = f16_sat, split_f16, gelu_f16
+    elif prec == "bf16":
+        r16, split, g16 = bf16, split_bf16, gelu_bf16
+    else:
+        raise ValueError("prec must be 'f16' or 'bf16'")
     if act == "gelu":
-        def h(s):
-            return gelu_f16(s)
+        h = g16
     else:
         def h(s):
-            return f16_sat(np.maximum(np.asarray(s, np.float32), 0))
+            return r16(np.maximum(np.asarray(s, np.float32), 0))
     p = unpack(vec)
     c32, m32, s32 = (np.float32(p[k]) for k in ("cap", "mu", "inv_sd"))
-    X0 = f16_sat((np.minimum(np.asarray(X, np.float32), c32) - m32) * s32)
-    b1h, b1l = split_f16(p["b1"])
-    b2h, b2l = split_f16(p["b2"])
-    b3h, b3l = split_f16(p["b3"])
-    wh, wl = split_f16(p["w4"])
-    A1 = h(X0 @ f16_sat(np.float32(p["W1"])).T + (b1h + b1l))
-    A2 = h(A1 @ f16_sat(np.float32(p["W2"])).T + (b2h + b2l))
-    A3 = h(A2 @ f16_sat(np.float32(p["W3"])).T + (b3h + b3l))
+    X0 = r16((np.minimum(np.asarray(X, np.float32), c32) - m32) * s32)
+    b1h, b1l = split(p["b1"])
+    b2h, b2l = split(p["b2"])
+    b3h, b3l = split(p["b3"])
+    wh, wl = split(p["w4"])
+    A1 = h(X0 @ r16(np.float32(p["W1"])).T + (b1h + b1l))
+    A2 = h(A1 @ r16(np.float32(p["W2"])).T + (b2h + b2l))
+    A3 = h(A2 @ r16(np.float32(p["W3"])).T + (b3h + b3l))
     return A3 @ (wh + wl) + p["b4"][0]

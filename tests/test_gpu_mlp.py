@@ -78,15 +78,16 @@ def test_mlp_training_reduces_loss(gpu, act):
     assert np.mean(losses[-8:]) < 0.5 * np.mean(losses[:4]), losses
 
 
+@pytest.mark.parametrize("prec", ["f16", "bf16"])
 @pytest.mark.parametrize("act", ["relu", "gelu"])
-def test_fused_inference_matches_oracle_forward(gpu, small_pair, act):
+def test_fused_inference_matches_oracle_forward(gpu, small_pair, act, prec):
     """cbmv_run_mlp's matching cost (float32 features + four tcgen05 layers
-    fused on f16 operands, f16 ReLU or GELU activations, biases as f16 high
-    + low parts) against (a) the oracle's model of the same arithmetic: max
-    5e-3, mean 3e-4 on P -- the kernel's float32 features and accumulation
-    order move an f16 rounding of an input or activation here and there;
-    (b) the float64 network on the same features: max 3e-2, mean 2e-3 --
-    the cost of 16-bit activations."""
+    fused on f16 or bf16 operands, 16-bit ReLU or GELU activations, biases
+    as 16-bit high + low parts) against (a) the oracle's model of the same
+    arithmetic: max 5e-3, mean 3e-4 on P -- the kernel's float32 features
+    and accumulation order move a 16-bit rounding of an input or activation
+    here and there; (b) the float64 network on the same features: max
+    3e-2, mean 2e-3 -- the cost of 16-bit activations."""
     from cbmv_b200.mlp import GpuMlp, MlpParams, input_stats
     from cbmv_b200.pipeline import StereoPipeline
     from oracle import mlp_ref
@@ -103,17 +104,17 @@ def test_fused_inference_matches_oracle_forward(gpu, small_pair, act):
     v["b2"][:] = np.linspace(-0.2, 0.2, 128)
     v["b3"][:] = -0.1
     v["b4"][:] = 0.2
-    g = GpuMlp(net)
+    g = GpuMlp(net, prec)
     prob = torch.empty((H, W, D), device="cuda")
     pipe.run_mlp(g, L, R, D, prob_out=prob)
     torch.cuda.synchronize()
     assert g.status() == 0
     got = prob.cpu().numpy().reshape(-1)
-    model = 1.0 / (1.0 + np.exp(mlp_ref.forward_fused(net.vec, X, act)))
+    model = 1.0 / (1.0 + np.exp(mlp_ref.forward_fused(net.vec, X, act, prec)))
     exact = 1.0 / (1.0 + np.exp(mlp_ref.forward(net.vec, X, act)["z"]))
     e_model, e_exact = np.abs(got - model), np.abs(got - exact)
-    print("%s fused vs model: max %.2e mean %.2e; vs float64 network: max %.2e mean %.2e"
-          % (act, e_model.max(), e_model.mean(), e_exact.max(), e_exact.mean()))
+    print("%s %s fused vs model: max %.2e mean %.2e; vs float64 network: max %.2e mean %.2e"
+          % (act, prec, e_model.max(), e_model.mean(), e_exact.max(), e_exact.mean()))
     assert e_model.max() < 5e-3 and e_model.mean() < 3e-4, (e_model.max(), e_model.mean())
     assert e_exact.max() < 3e-2 and e_exact.mean() < 2e-3, (e_exact.max(), e_exact.mean())
 

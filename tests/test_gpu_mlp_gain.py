@@ -12,7 +12,9 @@ features, classifier, MC-CNN `_mem` post) is run three ways:
   cost, the best single matcher (test.py:341-449 driven with that volume),
   i.e. MC-CNN's pipeline on a hand-made cost.
 
-The trained network must beat both by a clear margin on bad-2.0.
+The trained network must beat both by a clear margin on bad-2.0, and its
+bf16 form of the fused inference (cbmv_mlp_set_precision) must stay within
+0.5 percentage points of the f16 form it runs in by default.
 """
 import os
 
@@ -46,7 +48,7 @@ def test_trained_mlp_beats_untrained_and_no_classifier(gpu):
     trained = MlpParams.load(MLP)
     v = trained.views()
     untrained = MlpParams.init(0, v["cap"].copy(), v["mu"].copy(), 1.0 / v["inv_sd"], trained.activation)
-    net_t, net_u = GpuMlp(trained), GpuMlp(untrained)
+    net_t, net_u, net_b = GpuMlp(trained), GpuMlp(untrained), GpuMlp(trained, "bf16")
     pipe = StereoPipeline()
     rows = []
     for s in SEEDS:
@@ -54,11 +56,13 @@ def test_trained_mlp_beats_untrained_and_no_classifier(gpu):
         l, r = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
         bt = bad_x(pipe.run_mlp(net_t, l, r, 128).cpu().numpy(), gt, nonocc)
         bu = bad_x(pipe.run_mlp(net_u, l, r, 128).cpu().numpy(), gt, nonocc)
+        bb = bad_x(pipe.run_mlp(net_b, l, r, 128).cpu().numpy(), gt, nonocc)
         bc = _census_only(L, R, nonocc, gt)
-        rows.append((bt, bu, bc))
-    assert net_t.status() == 0 and net_u.status() == 0
-    bt, bu, bc = (float(np.mean(c)) for c in zip(*rows))
-    print("bad-2.0 trained %.4f untrained %.4f census-only %.4f" % (bt, bu, bc))
+        rows.append((bt, bu, bc, bb))
+    assert net_t.status() == 0 and net_u.status() == 0 and net_b.status() == 0
+    bt, bu, bc, bb = (float(np.mean(c)) for c in zip(*rows))
+    print("bad-2.0 trained %.4f (bf16 form %.4f) untrained %.4f census-only %.4f" % (bt, bb, bu, bc))
+    assert abs(bb - bt) < 0.005, (bb, bt)
     assert bt < 0.06, bt
     assert bt < bu - 0.05, (bt, bu)      # training, not the architecture, makes the classifier
     assert bt < 0.8 * bc, (bt, bc)       # the learned classifier over the best single matcher

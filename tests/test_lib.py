@@ -92,6 +92,9 @@ def test_argument_checks_of_the_fused_entry_points():
     prm = _lib.default_params(sgm_prefetch=3)
     assert L.cbmv_run_mlp(buf, buf, ctypes.byref(prm), buf, buf, 64, 64, 32, buf, None) != 0
     assert b"sgm_prefetch" in L.cbmv_last_error()
+    prec = ctypes.c_int()
+    assert L.cbmv_mlp_set_precision(None, 1) == -1
+    assert L.cbmv_mlp_get_precision(None, ctypes.byref(prec)) == -1
 
 
 def test_forest_upload_validation():
