@@ -362,7 +362,13 @@ __global__ void __launch_bounds__(128) matcher_strip_kernel(
         for (int k = 0; k < WIN; k++)
 #pragma unroll
           for (int wh = 0; wh < WIN; wh++) acc = __sad(dif[MODE == kStripZsad ? (s + k) % WIN : 0][wh], m, acc);
-        v = (float)((double)acc / (double)(WIN * WIN));
+        // acc < 2^24 (WIN^2 terms of at most 2 WIN^2 255) is exact in
+        // float32, and acc / WIN^2 is either an integer or more than 2^-29
+        // (relative) away from every float32 rounding midpoint, so one
+        // correctly rounded float32 division gives the float32 rounding of
+        // the exact quotient -- what rounding a float64 quotient would give
+        static_assert(WIN * WIN * WIN * WIN * 510 < (1 << 24), "ZSAD window sum exact in float32");
+        v = __fdiv_rn((float)acc, (float)(WIN * WIN));
       } else {
         const int64_t pl = y * W + x, pr = pl - d;
         unsigned acc = 0;
