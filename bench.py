@@ -23,8 +23,8 @@ gathered on rank 0.
 
 `value` is device time with the images resident in HBM and L2 flushed
 between steps; `e2e` is the same metric through the public call with pinned
-host buffers (H2D of both images and D2H of the disparity inside the timed
-region).  `--impl reference` times the reference's own implementation of the
+host buffers, i.e. the C ABI's host-buffer entry point cbmv_run_mlp_host
+(H2D of both images and D2H of the disparity inside the timed region).  `--impl reference` times the reference's own implementation of the
 path on whole pairs: its C++ matchers and feature extraction compiled
 unmodified (oracle/_ref) and batched as its test.py does, scikit-learn's
 predict_proba on the same forest, and its post.cu on the GPU (as shipped;
@@ -188,8 +188,10 @@ def _time_path(run, a, ws, flush, st, pipe):
 
 
 def _time_e2e(run_host, a, ws, flush, st):
-    """Wall time of the public call with pinned host images (H2D, whole
-    path, D2H of the disparity map inside the timed region)."""
+    """Wall time of the public call with pinned host buffers, which goes
+    through the C ABI's host-buffer entry point (cbmv_run_mlp_host /
+    cbmv_run_rf_host: H2D of both images, the whole path, D2H of the
+    disparity map and the stream synchronisation inside the timed region)."""
     for _ in range(2):
         run_host()
     barrier(ws)
@@ -268,15 +270,16 @@ def run_cbmv(a, ws, rank, local):
     st = torch.cuda.current_stream()
     Lh = torch.from_numpy(L).pin_memory()
     Rh = torch.from_numpy(R).pin_memory()
+    Dh = torch.empty(L.shape, dtype=torch.float32).pin_memory()
 
     if a.classifier == "mlp" and net is None:
         raise SystemExit("MLP parameters missing: %s (python -m cbmv_b200.train_mlp)" % a.mlp)
     paths = {}
     if a.classifier in ("both", "rf"):
-        paths["rf"] = (lambda: pipe.run_rf(l, r, D0, disp_out=disp), lambda: pipe.run_rf(Lh, Rh, D0))
+        paths["rf"] = (lambda: pipe.run_rf(l, r, D0, disp_out=disp), lambda: pipe.run_rf(Lh, Rh, D0, disp_out=Dh))
     if a.classifier in ("both", "mlp") and net is not None:
         paths["mlp"] = (lambda: pipe.run_mlp(net, l, r, D0, disp_out=disp),
-                        lambda: pipe.run_mlp(net, Lh, Rh, D0))
+                        lambda: pipe.run_mlp(net, Lh, Rh, D0, disp_out=Dh))
     res = {}
     relu = bf16v = None
     with Clocks(local) as clk:

@@ -36,6 +36,30 @@ def to_device(a, dtype):
     return t.to("cuda", non_blocking=False).contiguous(), True
 
 
+def is_host(a):
+    """True for numpy arrays and CPU tensors (pinned or not)."""
+    return isinstance(a, np.ndarray) or (isinstance(a, torch.Tensor) and not a.is_cuda)
+
+
+def host_array(a, dtype):
+    """`a` as C-contiguous host memory of `dtype`: a numpy array, or a CPU
+    tensor (kept as it is, pinned memory included, when it already is)."""
+    if isinstance(a, torch.Tensor):
+        return a.to(dtype=_NP2T[np.dtype(dtype)]).contiguous()
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def host_f32_buffer(a, shape):
+    """True when `a` can receive float32 [shape] results in place."""
+    if isinstance(a, torch.Tensor):
+        return a.dtype == torch.float32 and tuple(a.shape) == shape and a.is_contiguous()
+    return a.dtype == np.float32 and a.shape == shape and a.flags.c_contiguous and a.flags.writeable
+
+
+def host_ptr(a):
+    return a.data_ptr() if isinstance(a, torch.Tensor) else a.ctypes.data
+
+
 def empty(shape, dtype):
     require_cuda()
     return torch.empty(tuple(int(s) for s in shape), dtype=_NP2T[np.dtype(dtype)], device="cuda")

@@ -100,6 +100,8 @@ SIGNATURES = {
     "cbmv_ctx_timings": [_vp, ctypes.POINTER(_flt)],
     "cbmv_run_rf": [_vp, _vp, ctypes.POINTER(cbmv_params), _vp, _vp, _i64, _i64, _int, _vp, _vp],
     "cbmv_run_mlp": [_vp, _vp, ctypes.POINTER(cbmv_params), _vp, _vp, _i64, _i64, _int, _vp, _vp],
+    "cbmv_run_rf_host": [_vp, _vp, ctypes.POINTER(cbmv_params), _vp, _vp, _i64, _i64, _int, _vp],
+    "cbmv_run_mlp_host": [_vp, _vp, ctypes.POINTER(cbmv_params), _vp, _vp, _i64, _i64, _int, _vp],
     "cbmv_ctx_features_at": [_vp, ctypes.POINTER(cbmv_params), _vp, _vp, _i64, _i64, _int, _vp, _i64, _vp],
     "cbmv_ctx_features_f32_at": [_vp, ctypes.POINTER(cbmv_params), _vp, _vp, _i64, _i64, _int, _vp, _i64, _vp],
     "cbmv_ctx_volumes_f32": [_vp, ctypes.POINTER(cbmv_params), _vp, _vp, _i64, _i64, _int, _vp],

@@ -70,6 +70,8 @@ struct cbmv_ctx {
   float* gauss = nullptr;  // device copy of the mean2d kernel
   int gauss_ks = 0;
   float gauss_sigma = -1.0f;
+  void* io = nullptr;  // device copies of a host-buffer call's images and disparity
+  size_t io_bytes = 0;
 };
 
 namespace {
@@ -209,6 +211,7 @@ extern "C" int cbmv_ctx_destroy(cbmv_ctx* c) {
   if (c->side) cudaStreamSynchronize(c->side);
   if (c->ws) cudaFree(c->ws);
   if (c->gauss) cudaFree(c->gauss);
+  if (c->io) cudaFree(c->io);
   for (int i = 0; i < 6; i++)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->fork_ev) cudaEventDestroy(c->fork_ev);
@@ -494,6 +497,54 @@ extern "C" int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p
   RC(run_post(c, p, L, R, H, W, D, w, disp));
   CBMV_CUDA(cudaEventRecord(c->ev[4], st));
   return CBMV_OK;
+}
+
+// The host-buffer forms: the images are copied into the context's device
+// buffers (grown on demand; the previous host-buffer call synchronised the
+// stream, so nothing still uses them), the path runs on the context's
+// stream, the disparity is copied back and the stream synchronised.
+template <class Run>
+static int run_host_buffers(cbmv_ctx* c, const uint8_t* L, const uint8_t* R, int64_t H, int64_t W, float* disp,
+                            Run run) {
+  CBMV_REQUIRE(c && L && R && disp, CBMV_EINVAL, "null pointer argument");
+  CBMV_REQUIRE(H > 0 && W > 0, CBMV_EINVAL, "bad size H=%lld W=%lld", (long long)H, (long long)W);
+  CBMV_REQUIRE(H <= 65535 && W <= (int64_t(1) << 24), CBMV_ERANGE, "image %lldx%lld: W must be <= 2^24 and H <= 65535",
+               (long long)W, (long long)H);
+  const size_t HW = (size_t)H * (size_t)W, img = (HW + 255) & ~(size_t)255;
+  const size_t need = 2 * img + HW * sizeof(float);
+  if (need > c->io_bytes) {
+    if (c->io) CBMV_CUDA(cudaFree(c->io));
+    c->io = nullptr;
+    c->io_bytes = 0;
+    CBMV_CUDA(cudaMalloc(&c->io, need));
+    c->io_bytes = need;
+  }
+  uint8_t* dL = static_cast<uint8_t*>(c->io);
+  uint8_t* dR = dL + img;
+  float* dD = reinterpret_cast<float*>(dR + img);
+  cudaStream_t st = c->stream;
+  CBMV_CUDA(cudaMemcpyAsync(dL, L, HW, cudaMemcpyHostToDevice, st));
+  CBMV_CUDA(cudaMemcpyAsync(dR, R, HW, cudaMemcpyHostToDevice, st));
+  const int rc = run(dL, dR, dD);
+  if (rc == CBMV_OK) CBMV_CUDA(cudaMemcpyAsync(disp, dD, HW * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CBMV_CUDA(cudaStreamSynchronize(st));
+  return rc;
+}
+
+extern "C" int cbmv_run_rf_host(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params* p, const uint8_t* L,
+                                const uint8_t* R, int64_t H, int64_t W, int D, float* disp) {
+  CBMV_REQUIRE(f, CBMV_EINVAL, "null pointer argument");
+  return run_host_buffers(c, L, R, H, W, disp, [&](const uint8_t* dL, const uint8_t* dR, float* dD) {
+    return cbmv_run_rf(c, f, p, dL, dR, H, W, D, dD, nullptr);
+  });
+}
+
+extern "C" int cbmv_run_mlp_host(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p, const uint8_t* L,
+                                 const uint8_t* R, int64_t H, int64_t W, int D, float* disp) {
+  CBMV_REQUIRE(m, CBMV_EINVAL, "null pointer argument");
+  return run_host_buffers(c, L, R, H, W, disp, [&](const uint8_t* dL, const uint8_t* dR, float* dD) {
+    return cbmv_run_mlp(c, m, p, dL, dR, H, W, D, dD, nullptr);
+  });
 }
 
 extern "C" int cbmv_run_post(cbmv_ctx* c, const cbmv_params* p, const uint8_t* L, const uint8_t* R, int64_t H,

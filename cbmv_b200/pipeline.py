@@ -3,8 +3,11 @@
 StereoPipeline.run_rf(L, R, D) does on the device what the reference's
 main.py:53-70 does on the host (matchers, features, random forest, then
 eval_prob with the `_mem` post-processing) and returns the disparity map.
-Inputs may be numpy uint8 [H,W] (copied in, result copied out) or torch
-CUDA uint8 tensors (result stays on the device).
+Inputs may be host memory -- numpy uint8 [H,W] or CPU tensors, pinned or
+not -- (the host-buffer entry points cbmv_run_rf_host / cbmv_run_mlp_host
+copy them in and the disparity out; the result is a numpy array, or
+`disp_out` when that is a host buffer) or torch CUDA uint8 tensors (result
+stays on the device).
 """
 import ctypes
 
@@ -34,7 +37,29 @@ class StereoPipeline:
         except Exception:
             pass
 
+    def _host_call(self, left, right, disp_out, prob_out):
+        """True when the call goes through a host-buffer entry point: both
+        images and the output (if given) in host memory, no cost volume
+        requested."""
+        return (prob_out is None and _dev.is_host(left) and _dev.is_host(right)
+                and (disp_out is None or _dev.is_host(disp_out)))
+
+    def _run_host(self, fn, model, left, right, ndisp, disp_out):
+        l = _dev.host_array(left, np.uint8)
+        r = _dev.host_array(right, np.uint8)
+        if l.ndim != 2 or tuple(r.shape) != tuple(l.shape):
+            raise ValueError("left and right must be [H,W] images of one shape")
+        H, W = l.shape
+        out = disp_out if disp_out is not None else np.empty((H, W), np.float32)
+        if not _dev.host_f32_buffer(out, (H, W)):
+            raise ValueError("disp_out must be a writable C-contiguous float32 [H,W] host buffer")
+        _lib.call(fn, self.ctx, model, ctypes.byref(self.params), _dev.host_ptr(l), _dev.host_ptr(r), H, W,
+                  int(ndisp), _dev.host_ptr(out))
+        return out
+
     def run_rf(self, left, right, ndisp, disp_out=None, prob_out=None):
+        if self._host_call(left, right, disp_out, prob_out):
+            return self._run_host("cbmv_run_rf_host", self.forest.handle, left, right, ndisp, disp_out)
         l, host = _dev.to_device(left, np.uint8)
         r, _ = _dev.to_device(right, np.uint8)
         H, W = l.shape
@@ -46,6 +71,8 @@ class StereoPipeline:
 
     def run_mlp(self, net, left, right, ndisp, disp_out=None, prob_out=None):
         """The same path with the learned classifier (cbmv_b200.mlp.GpuMlp)."""
+        if self._host_call(left, right, disp_out, prob_out):
+            return self._run_host("cbmv_run_mlp_host", net.h, left, right, ndisp, disp_out)
         l, host = _dev.to_device(left, np.uint8)
         r, _ = _dev.to_device(right, np.uint8)
         H, W = l.shape

@@ -375,6 +375,20 @@ int cbmv_run_rf(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params* p, const u
 int cbmv_run_mlp(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p, const uint8_t* L,
                  const uint8_t* R, int64_t H, int64_t W, int D, float* disp, float* prob0);
 
+/* cbmv_run_rf / cbmv_run_mlp with HOST buffers, the form a driver holding
+ * its images in host memory binds (the reference's drivers pass numpy
+ * arrays to its modules and read the disparity on the host,
+ * test.py:143-149, 408-409): L, R uint8 [H,W] and disp float32 [H,W] in
+ * host memory, pinned or pageable.  The images are copied into device
+ * buffers the context owns (grown on demand, freed with it), the path
+ * runs on the context's stream, the disparity is copied back, and the
+ * call returns once it is in `disp` (the stream is synchronised).  Errors
+ * as the device-pointer forms; W <= 2^24. */
+int cbmv_run_rf_host(cbmv_ctx* c, const cbmv_forest* f, const cbmv_params* p, const uint8_t* L,
+                     const uint8_t* R, int64_t H, int64_t W, int D, float* disp);
+int cbmv_run_mlp_host(cbmv_ctx* c, const cbmv_mlp* m, const cbmv_params* p, const uint8_t* L,
+                      const uint8_t* R, int64_t H, int64_t W, int D, float* disp);
+
 /* The post-processing alone (Testing.eval_prob with the _mem chain,
  * test.py:143-149, 341-449) on a given matching cost: cost float32 [H,W,D]
  * (low = good, e.g. a saved P(class 0) volume, main.py:56-67), the images L,

@@ -103,6 +103,33 @@ def test_pipeline_repeatable_and_device_io(gpu, small_pair, forest):
     assert np.array_equal(a, b.cpu().numpy())  # deterministic
 
 
+def test_host_buffer_entry_points_equal_device_ones(gpu, small_pair, forest):
+    """cbmv_run_rf_host / cbmv_run_mlp_host (images in host memory, the
+    disparity written to host memory; pageable numpy arrays and pinned
+    tensors) give the device-pointer forms' disparity bit for bit, on
+    repeated calls and after a larger pair has grown the context's device
+    copies."""
+    import os
+    from cbmv_b200 import synth
+    from cbmv_b200.forest_gpu import GpuForest
+    from cbmv_b200.mlp import GpuMlp
+    from cbmv_b200.pipeline import StereoPipeline
+    net = GpuMlp.load(os.path.join(os.path.dirname(__file__), "golden", "mlp_gelu_694x554.npz"))
+    pipe = StereoPipeline(GpuForest(forest))
+    L2, R2, _, _ = synth.make_pair(seed=12, width=130, height=70, ndisp=32, planes=4, dmin=2, dmax=28)
+    for (L, R), D in (((small_pair[0], small_pair[1]), 24), ((L2, R2), 32), ((small_pair[0], small_pair[1]), 24)):
+        l, r = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
+        Lp, Rp = torch.from_numpy(L).pin_memory(), torch.from_numpy(R).pin_memory()
+        out = torch.empty(L.shape, dtype=torch.float32).pin_memory()
+        for run in (lambda *a, **k: pipe.run_rf(*a, **k), lambda *a, **k: pipe.run_mlp(net, *a, **k)):
+            want = run(l, r, D).cpu().numpy()
+            for _ in range(2):
+                got = run(L, R, D)
+                assert isinstance(got, np.ndarray) and np.array_equal(got, want)
+                assert run(Lp, Rp, D, disp_out=out) is out
+                assert np.array_equal(out.numpy(), want)
+
+
 def test_saved_cost_volume_gives_the_same_disparity(gpu, small_pair, tmp_path):
     """--saveCostVolume then --loadCostVolume (main.py:56-67): the post run on
     the reloaded cost reproduces the fused path's disparity bit for bit."""

@@ -92,6 +92,13 @@ def test_argument_checks_of_the_fused_entry_points():
     prm = _lib.default_params(sgm_prefetch=3)
     assert L.cbmv_run_mlp(buf, buf, ctypes.byref(prm), buf, buf, 64, 64, 32, buf, None) != 0
     assert b"sgm_prefetch" in L.cbmv_last_error()
+    # the host-buffer forms check their pointers and sizes before touching the context
+    assert L.cbmv_run_mlp_host(None, buf, None, buf, buf, 64, 64, 32, buf) == -1
+    assert L.cbmv_run_mlp_host(buf, None, None, buf, buf, 64, 64, 32, buf) == -1
+    assert L.cbmv_run_rf_host(buf, buf, None, buf, None, 64, 64, 32, buf) == -1
+    assert L.cbmv_run_rf_host(buf, buf, None, buf, buf, 0, 64, 32, buf) == -1
+    assert L.cbmv_run_mlp_host(buf, buf, None, buf, buf, 70000, 64, 32, buf) == -4
+    assert b"65535" in L.cbmv_last_error()
     prec = ctypes.c_int()
     assert L.cbmv_mlp_set_precision(None, 1) == -1
     assert L.cbmv_mlp_get_precision(None, ctypes.byref(prec)) == -1
