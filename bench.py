@@ -378,6 +378,19 @@ def run_cbmv(a, ws, rank, local):
                                            "included) at the measured peak"},
                     "note": "dense flops of 20-128-128-64-1 per (pixel,d); the kernel also builds "
                             "the 20 features from the four float32 cost volumes"}
+        ipu = traffic.get("features_mlp_kernel_warp_inst_per_unit")
+        if ipu:
+            # the bound the kernel actually meets: instruction issue (one warp
+            # instruction per clock per SM sub-partition); the GELU epilogues
+            # and the features are CUDA-core work beside the MMAs
+            sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
+            issue_peak = sm_count * 4 * clk_max_mhz() * 1e6
+            issue_achieved = ipu * units / (t_cls / 1e3)
+            roof_mlp["issue"] = {"warp_inst_per_unit": ipu, "achieved": issue_achieved, "peak": issue_peak,
+                                 "unit": "warp instructions/s", "frac": issue_achieved / issue_peak,
+                                 "note": "warp instructions per (pixel,d) from the committed ncu capture "
+                                         "(profiles/traffic.json); peak = SMs x 4 sub-partitions x max SM "
+                                         "clock"}
         res["mlp"]["roofline"] = roof_mlp
     roof = res[head]["roofline"]
 
