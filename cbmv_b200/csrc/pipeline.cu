@@ -513,9 +513,10 @@ static int run_host_buffers(cbmv_ctx* c, const uint8_t* L, const uint8_t* R, int
   const size_t HW = (size_t)H * (size_t)W, img = (HW + 255) & ~(size_t)255;
   const size_t need = 2 * img + HW * sizeof(float);
   if (need > c->io_bytes) {
-    if (c->io) CBMV_CUDA(cudaFree(c->io));
+    void* old = c->io;  // forgotten first, so that no error path frees it twice
     c->io = nullptr;
     c->io_bytes = 0;
+    if (old) CBMV_CUDA(cudaFree(old));
     CBMV_CUDA(cudaMalloc(&c->io, need));
     c->io_bytes = need;
   }
