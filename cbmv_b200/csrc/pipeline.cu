@@ -517,7 +517,9 @@ static int run_host_buffers(cbmv_ctx* c, const uint8_t* L, const uint8_t* R, int
     c->io = nullptr;
     c->io_bytes = 0;
     if (old) CBMV_CUDA(cudaFree(old));
-    CBMV_CUDA(cudaMalloc(&c->io, need));
+    void* fresh = nullptr;
+    CBMV_CUDA(cudaMalloc(&fresh, need));
+    c->io = fresh;
     c->io_bytes = need;
   }
   uint8_t* dL = static_cast<uint8_t*>(c->io);
