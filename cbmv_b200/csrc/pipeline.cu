@@ -236,9 +236,11 @@ static int ensure_workspace(cbmv_ctx* c, size_t bytes) {
   if (c->ws) cudaFree(c->ws);
   c->ws = nullptr;
   c->ws_bytes = 0;
-  cudaError_t e = cudaMalloc(&c->ws, bytes);
+  void* fresh = nullptr;
+  cudaError_t e = cudaMalloc(&fresh, bytes);
   if (e != cudaSuccess)
     return set_error(CBMV_ENOMEM, "workspace of %zu bytes: %s", bytes, cudaGetErrorString(e));
+  c->ws = fresh;
   c->ws_bytes = bytes;
   return CBMV_OK;
 }
@@ -252,7 +254,10 @@ static int ensure_gaussian(cbmv_ctx* c, float sigma) {
     cudaFree(c->gauss);
     c->gauss = nullptr;
   }
-  CBMV_CUDA(cudaMalloc(&c->gauss, k.size() * sizeof(float)));
+  float* fresh = nullptr;
+  CBMV_CUDA(cudaMalloc(&fresh, k.size() * sizeof(float)));
+  c->gauss = fresh;
+  c->gauss_sigma = -1.0f;  // valid once the copy below succeeded
   CBMV_CUDA(cudaMemcpy(c->gauss, k.data(), k.size() * sizeof(float), cudaMemcpyHostToDevice));
   c->gauss_ks = ks;
   c->gauss_sigma = sigma;
