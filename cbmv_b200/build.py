@@ -18,8 +18,10 @@ OUT = os.path.join(HERE, "libcbmv.so")
 BUILD = os.path.join(CSRC, "_build")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
-         "-Xptxas", "-warn-spills"]
+# hidden visibility: only the C ABI of include/cbmv.h (default visibility
+# there) is exported, no C++ internals or kernel stubs
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+         "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 
 
 def _headers():

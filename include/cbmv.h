@@ -37,6 +37,12 @@
 extern "C" {
 #endif
 
+/* libcbmv.so is built with hidden visibility: the declarations of this
+ * header are its only exported symbols. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
 enum cbmv_status {
   CBMV_OK = 0,
   CBMV_EINVAL = -1,  /* bad argument (null pointer, size, window, dtype ...) */
@@ -449,6 +455,10 @@ int cbmv_batch_timings(cbmv_batch* b, float* pair_ms, float* done_ms, float* tot
  * [0] matchers, [1] feature statistics, [2] features+classifier, [3] post,
  * [4] total.  Valid after the stream has been synchronised. */
 int cbmv_ctx_timings(cbmv_ctx* c, float* ms5);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
 
 #ifdef __cplusplus
 }

@@ -27,6 +27,24 @@ def test_library_exports_every_declared_symbol():
     assert not [n for n in names if n not in _lib.SIGNATURES], "unbound entry points"
 
 
+def test_library_exports_nothing_else():
+    """Hidden visibility: the dynamic symbol table holds the C ABI of
+    include/cbmv.h and no C++ internals of the library (kernel stubs,
+    cbmv:: functions) that could clash with a host process's own."""
+    import shutil
+    import subprocess
+    from cbmv_b200 import _lib
+    nm = shutil.which("nm")
+    if nm is None:
+        pytest.skip("nm not installed")
+    out = subprocess.run([nm, "-D", "--defined-only", _lib.lib()._name], capture_output=True, text=True,
+                         check=True).stdout
+    syms = [ln.split()[-1] for ln in out.splitlines() if ln.split() and ln.split()[-2] in "TDBR"]
+    ours = sorted(s for s in syms if s.startswith("cbmv_"))
+    assert ours == _declared()
+    assert not [s for s in syms if "cbmv" in s and not s.startswith("cbmv_")], "C++ internals exported"
+
+
 def test_host_side_argument_checks():
     from cbmv_b200 import _lib
     L = _lib.lib()
