@@ -18,8 +18,12 @@ HELD_OUT = list(range(3000, 3020))
 
 
 def bad_x(disp, gt, mask, thr=2.0):
+    """1 - (pixels of the mask with |disp - gt| <= thr) / (pixels of the
+    mask), as Evaluator.h:196-211 counts it (errorMap = |disp - dispGT| <=
+    threshold), so a NaN disparity counts as an error; ground-truth pixels
+    that are not finite are outside the mask (the reference's validMask)."""
     m = mask & np.isfinite(gt)
-    return float(np.mean(np.abs(disp[m] - gt[m]) > thr))
+    return float(1.0 - np.mean(np.abs(disp[m] - gt[m]) <= thr))
 
 
 def compare(forest_path, mlp_path, seeds=HELD_OUT, ndisp=128):

@@ -35,3 +35,17 @@ def test_calib(tmp_path):
     p = tmp_path / "calib.txt"
     p.write_text("cam0=[1 0 0]\ndoffs=0\nbaseline=193\nwidth=694\nheight=554\nndisp=128\nvmin=1\n")
     assert read_calib(str(p)) == (694, 554, 128)
+
+
+def test_bad_x_counts_as_the_reference_evaluator():
+    """bad-x as Evaluator.h:196-211: 1 - |{|d - gt| <= thr} & mask| / |mask|;
+    a NaN disparity is an error, an infinite ground truth is outside the
+    mask, the threshold itself is not an error."""
+    from cbmv_b200.evaluate import bad_x
+    gt = np.array([[10.0, 10.0, 10.0], [10.0, np.inf, 10.0]], np.float32)
+    disp = np.array([[12.0, 12.5, np.nan], [10.0, 99.0, 7.0]], np.float32)
+    mask = np.array([[True, True, True], [True, True, False]])
+    # in the mask with a finite gt: 12 (|2| <= 2, good), 12.5 (bad), NaN (bad), 10 (good)
+    assert bad_x(disp, gt, mask) == 0.5
+    assert bad_x(disp, gt, mask, thr=3.0) == 0.25
+    assert bad_x(disp, gt, np.ones_like(mask)) == 0.6  # + 7 vs 10 (bad); the inf pixel stays out
