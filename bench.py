@@ -131,10 +131,14 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def env_ranks():
+    """(world size, rank, local rank) as torchrun sets them."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
 def dist_init():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    ws, rank, local = env_ranks()
     if ws > 1:
         import datetime
         import torch
@@ -708,11 +712,17 @@ def main():
     ap.add_argument("--height", type=int, default=H0,
                     help="rows of the pair (smaller cases for profiler captures; default 554)")
     a = ap.parse_args()
-    ws, rank, local = dist_init()
     if a.impl == "reference":
+        # rank 0 alone runs the reference and no rank exchanges anything, so
+        # no process group is opened (the other ranks exit at once)
+        ws, rank, local = env_ranks()
         with native_stdout_to_stderr():
             line = run_reference(a, ws, rank, local)
-    elif a.batch:
+        if rank == 0 and line is not None:
+            print(json.dumps(line))
+        return
+    ws, rank, local = dist_init()
+    if a.batch:
         line = run_batch(a, ws, rank, local)
     else:
         line = run_cbmv(a, ws, rank, local)
