@@ -230,19 +230,30 @@ def forest_visits_per_unit(pipe, gf, flat, l, r, n=65536):
     return float(depth[flat.roots[None, :].astype(np.int64) + leaves].sum(axis=1).mean())
 
 
-def launches_per_pair(prm):
-    """Kernel launches of one cbmv_run_mlp call (pipeline.cu) for parameters
-    prm: 6 per-pixel terms (census descriptors, NCC sums, Sobel; both
-    images; the ZSAD strip kernel of window 5 forms its window means itself,
-    another window adds their 2 launches), 4 cost volumes, 2 row
-    statistics, 1 features+classifier; post: 4 image normalisation, 2
-    cross, 2 SGM neighbour differences (one per image), 2 per SGM
-    iteration, 1 CBCA support build and 1 per CBCA pass, WTA+subpixel,
-    median per iteration, mean2d (33 with the defaults, as an ncu launch
-    list of the headline step counts them per pass)."""
-    post = 4 + 2 + (2 + 2 * prm.sgm_i if prm.sgm_i else 0) + (1 + prm.cbca_i2 if prm.cbca_i2 else 0) \
-        + (1 + prm.cbca_i1 if prm.cbca_i1 else 0) + 1 + prm.median_i + 1
-    return (6 if prm.sadw == 5 else 8) + 4 + 2 + 1 + post
+def launches_per_pair(prm, classifier="mlp"):
+    """Kernel launches of one cbmv_run_mlp / cbmv_run_rf call (pipeline.cu)
+    for parameters prm.  Front end: census descriptors, NCC sums and Sobel of
+    both images (6) plus the ZSAD window means (2) except on the learned path
+    with window 5, whose strip kernel forms them itself; 4 cost volumes; the
+    row statistics (learned path 2, forest path one per volume, 4); 1
+    features + classifier.  Post: image normalisation (4), cross arms (2),
+    the SGM neighbour differences (2, with any SGM iteration); per cost
+    chain one CBCA support build (when the passes read precomputed
+    supports, L1 <= 6 and not exact_cbca) and one launch per CBCA pass, 2
+    per SGM iteration; WTA + subpixel; with interpolate the right view's
+    cost (1), its chain and its WTA (1), and the left-right check and fills
+    (3); median per iteration; mean2d.  33 (learned) and 37 (forest) with
+    the defaults, as the ncu launch lists of the headline step count them
+    per pass."""
+    f32 = classifier == "mlp"
+    front = 6 + (0 if (f32 and prm.sadw == 5) else 2) + 4 + (2 if f32 else 4) + 1
+    masked = not prm.exact_cbca and prm.L1 - 1 <= 5
+    passes = prm.cbca_i1 + prm.cbca_i2
+    chain = (1 if masked and passes else 0) + passes + 2 * prm.sgm_i
+    post = 4 + 2 + (2 if prm.sgm_i else 0) + chain + 1 + prm.median_i + 1
+    if prm.interpolate:
+        post += 1 + chain + 1 + 3
+    return front + post
 
 
 def run_cbmv(a, ws, rank, local):
@@ -342,7 +353,7 @@ def run_cbmv(a, ws, rank, local):
         head = a.classifier
     h = res[head]
 
-    launches = launches_per_pair(pipe.params)
+    launches = launches_per_pair(pipe.params, head)
 
     hbm, hbm_kind = peaks()
     tc, tc_kind = tensor_peak()

@@ -18,13 +18,26 @@ def test_launch_count_matches_the_committed_launch_list():
     shows per pass."""
     from cbmv_b200 import _lib
     b = _bench()
-    assert b.launches_per_pair(_lib.default_params()) == 33
+    dp = _lib.default_params
+    assert b.launches_per_pair(dp(), "mlp") == 33
     text = open(os.path.join(ROOT, "profiles", "launches_694x554_mlp.md")).read()
     m = re.search(r"Per pass: (\d+) launches", text)
     assert m and int(m.group(1)) == 33
-    # every SGM iteration adds its scan and its combine, every CBCA pass one launch
-    assert b.launches_per_pair(_lib.default_params(sgm_i=1)) == 31
-    assert b.launches_per_pair(_lib.default_params(cbca_i2=2)) == 31
+    # the forest path: ZSAD window means and four float64 statistics launches
+    assert b.launches_per_pair(dp(), "rf") == 37
+    text = open(os.path.join(ROOT, "profiles", "launches_694x554_rf.md")).read()
+    m = re.search(r"Per pass (\d+) launches", text)
+    assert m and int(m.group(1)) == 37
+    # every SGM iteration adds its scan and its combine, every CBCA pass one
+    # launch; one support build per chain, none when the passes build their
+    # own supports (L1 > 6 or the reference's summation order)
+    assert b.launches_per_pair(dp(sgm_i=1)) == 31
+    assert b.launches_per_pair(dp(cbca_i2=2)) == 31
+    assert b.launches_per_pair(dp(cbca_i1=1, cbca_i2=1)) == 31
+    assert b.launches_per_pair(dp(L1=9)) == 32
+    assert b.launches_per_pair(dp(exact_cbca=1)) == 32
+    # _interp: the right view's cost, chain and WTA, then the check and fills
+    assert b.launches_per_pair(dp(interpolate=1)) == 33 + 1 + 9 + 1 + 3
 
 
 def test_algorithmic_figures():
