@@ -670,7 +670,11 @@ def run_batch(a, ws, rank, local):
                                "(means over the timed steps)"},
         "sequential_ms": seq_ms, "sequential_value": units / (seq_ms / 1e3),
         "identical_to_sequential": bool(same), "bad2_nonocc_mean": float(np.mean(bad)),
-        "gpu_launches": "1 graph launch per step per GPU", "clocks": clk.summary(),
+        "gpu_launches": a.steps * len(all_shapes) * launches_per_pair(_lib.default_params(), "mlp"),
+        "gpu_launches_note": "this package's kernels inside the graphs over the timed steps: %d per pair "
+                             "x %d pairs per step, one graph launch per step per GPU"
+                             % (launches_per_pair(_lib.default_params(), "mlp"), len(all_shapes)),
+        "clocks": clk.summary(),
     }
 
 
