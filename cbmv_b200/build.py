@@ -28,9 +28,10 @@ def _headers():
     return glob.glob(os.path.join(CSRC, "*.cuh")) + [os.path.join(os.path.dirname(HERE), "include", "cbmv.h")]
 
 
-def _compile(src, newest_header):
+def _compile(src, newest_header, flags_changed):
     obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
-    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), newest_header):
+    if not flags_changed and os.path.exists(obj) and \
+            os.path.getmtime(obj) >= max(os.path.getmtime(src), newest_header):
         return obj, ""
     cmd = [NVCC] + ARCH + FLAGS + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -43,13 +44,19 @@ def build(verbose=False):
     os.makedirs(BUILD, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     newest = max(os.path.getmtime(h) for h in _headers())
+    # objects compiled with other flags are stale too
+    stamp = os.path.join(BUILD, "flags.txt")
+    flags = " ".join([NVCC] + ARCH + FLAGS)
+    changed = not os.path.exists(stamp) or open(stamp).read() != flags
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
-        results = list(ex.map(lambda s: _compile(s, newest), srcs))
+        results = list(ex.map(lambda s: _compile(s, newest, changed), srcs))
+    with open(stamp, "w") as f:
+        f.write(flags)
     objs = [o for o, _ in results]
     for o, msg in results:
         if msg and verbose:
             print(msg, file=sys.stderr)
-    if not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(o) for o in objs):
+    if changed or not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(o) for o in objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
