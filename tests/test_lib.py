@@ -179,3 +179,27 @@ def test_learned_classifier_falls_back_to_the_forest():
     with pytest.raises(RuntimeError):
         p.run_classified(None, None, 8, net=Net(0))
     p.ctx = None  # nothing to release
+
+
+def test_product_never_imports_the_oracle():
+    """The oracle is the checker only: no module of the package imports it,
+    and the library's sources include nothing from it."""
+    import ast
+    pkg = os.path.join(ROOT, "cbmv_b200")
+    for name in sorted(os.listdir(pkg)):
+        if not name.endswith(".py"):
+            continue
+        tree = ast.parse(open(os.path.join(pkg, name)).read())
+        for node in ast.walk(tree):
+            mods = []
+            if isinstance(node, ast.Import):
+                mods = [a.name for a in node.names]
+            elif isinstance(node, ast.ImportFrom):
+                mods = [node.module or ""]
+            assert not [m for m in mods if m == "oracle" or m.startswith("oracle.")], (name, mods)
+    csrc = os.path.join(pkg, "csrc")
+    for name in sorted(os.listdir(csrc)):
+        if name.endswith((".cu", ".cuh", ".h")):
+            for line in open(os.path.join(csrc, name)):
+                if line.lstrip().startswith("#include"):
+                    assert "oracle" not in line, (name, line)
