@@ -21,6 +21,9 @@ gathered on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cbmv|reference]
 
+(started directly with --gpus N > 1 it relaunches itself under torchrun, one
+process per GPU; under torchrun --gpus must equal WORLD_SIZE)
+
 `value` is device time with the images resident in HBM and L2 flushed
 between steps; `e2e` is the same metric through the public call with pinned
 host buffers, i.e. the C ABI's host-buffer entry point cbmv_run_mlp_host
@@ -727,6 +730,15 @@ def main():
     ap.add_argument("--height", type=int, default=H0,
                     help="rows of the pair (smaller cases for profiler captures; default 554)")
     a = ap.parse_args()
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # started directly with --gpus N: one process per GPU under torchrun
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(a.gpus),
+               "--master-addr", "127.0.0.1", "--master-port", os.environ.get("MASTER_PORT", "29517"),
+               os.path.abspath(__file__)] + sys.argv[1:]
+        os.execv(sys.executable, cmd)
+    if a.gpus != env_ranks()[0]:
+        raise SystemExit("--gpus %d but WORLD_SIZE=%d: launch with torchrun --nproc-per-node %d"
+                         % (a.gpus, env_ranks()[0], a.gpus))
     if a.impl == "reference":
         # rank 0 alone runs the reference and no rank exchanges anything, so
         # no process group is opened (the other ranks exit at once)
