@@ -203,3 +203,30 @@ def test_product_never_imports_the_oracle():
             for line in open(os.path.join(csrc, name)):
                 if line.lstrip().startswith("#include"):
                     assert "oracle" not in line, (name, line)
+
+
+def test_header_is_plain_c_and_links(tmp_path):
+    """include/cbmv.h compiles as pedantic C99 (cgo, JNI and other FFIs bind
+    it from C), and a C program links against libcbmv.so and calls it."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not installed")
+    src = tmp_path / "t.c"
+    src.write_text('#include "cbmv.h"\n#include <stdio.h>\n'
+                   "int main(void) { cbmv_params p; cbmv_params_default(&p);\n"
+                   '  printf("%d %d %s\\n", p.censw, p.sgm_i, cbmv_version()); return 0; }\n')
+    exe = tmp_path / "t"
+    lib_dir = os.path.join(ROOT, "cbmv_b200")
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", str(exe), "-L" + lib_dir, "-lcbmv", "-Wl,-rpath," + lib_dir,
+                    "-Wl,--unresolved-symbols=ignore-in-shared-libs"], check=True, capture_output=True)
+    env = dict(os.environ)
+    try:
+        import nvidia.cuda_runtime as cr  # the CUDA runtime the library was linked against
+        env["LD_LIBRARY_PATH"] = os.path.join(cr.__path__[0], "lib") + ":" + env.get("LD_LIBRARY_PATH", "")
+    except ImportError:
+        pass
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True, env=env).stdout.split()
+    assert out[:2] == ["11", "2"] and out[2].startswith("cbmv-b200")
